@@ -1,0 +1,183 @@
+/*
+ * rmetis-b200: B200-native multilevel k-way partitioning behind the C ABI of
+ * javagg/rmetis.
+ *
+ * Drop-in entry points (same names, argument meaning, ownership and return
+ * codes as the reference's C ABI, src/ffi/c_api.rs):
+ *   RMETIS_SetDefaultOptions   replaces src/ffi/c_api.rs:15-23
+ *   RMETIS_PartGraphKway       replaces src/ffi/c_api.rs:56-81 (+ c_partition_impl :140-209,
+ *                              parse_options :211-222)
+ *
+ * The k-way path computes on the GPU (CType Shem/Rm, IpType Grow/Random/MetisRb,
+ * RType Greedy). RType Fm (the reference's default) is not on this path: such a
+ * call returns METIS_ERROR_INPUT instead of silently running another
+ * algorithm. Callers select Greedy with options[METIS_OPTION_PTYPE] != -1 and
+ * options[METIS_OPTION_RTYPE] = 1, exactly as the reference's from_raw
+ * (src/types.rs:190-224) decodes them.
+ *
+ * Everything after the drop-in section is additive: a device-pointer variant,
+ * stream/tuning/profiling controls, and one entry point per reference function
+ * of the hot path (used by the parity tests and available to users).
+ *
+ * Types follow the reference: idx_t = int32_t (src/types.rs:4), real_t = float
+ * (src/types.rs:6). Return codes (src/types.rs:164-167): METIS_OK 1,
+ * METIS_ERROR_INPUT -2, METIS_ERROR_MEMORY -3, METIS_ERROR -4.
+ */
+#ifndef RMETIS_B200_H
+#define RMETIS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t idx_t;
+typedef float real_t;
+
+#if defined(__GNUC__)
+#define RMETIS_API __attribute__((visibility("default")))
+#else
+#define RMETIS_API
+#endif
+
+#define METIS_OK 1
+#define METIS_ERROR_INPUT (-2)
+#define METIS_ERROR_MEMORY (-3)
+#define METIS_ERROR (-4)
+
+#define METIS_NOPTIONS 40
+#define METIS_OPTION_PTYPE 0
+#define METIS_OPTION_OBJTYPE 1
+#define METIS_OPTION_CTYPE 2
+#define METIS_OPTION_IPTYPE 3
+#define METIS_OPTION_RTYPE 4
+#define METIS_OPTION_DBGLVL 5
+#define METIS_OPTION_NITER 6
+#define METIS_OPTION_NCUTS 7
+#define METIS_OPTION_SEED 8
+#define METIS_OPTION_NO2HOP 9
+#define METIS_OPTION_MINCONN 10
+#define METIS_OPTION_CONTIG 11
+#define METIS_OPTION_UFACTOR 16
+#define METIS_OPTION_NUMBERING 17
+
+/* ---- drop-in ---------------------------------------------------------- */
+
+/* Fills options[0..40) with the reference's Options::default().to_raw()
+ * (src/types.rs:77-95, :227-245). options[0] stays -1, which the partitioner
+ * reads as "all defaults". NULL -> METIS_ERROR_INPUT. */
+RMETIS_API int RMETIS_SetDefaultOptions(idx_t *options);
+
+/* Multilevel k-way partition (src/ffi/c_api.rs:56-81). Host pointers.
+ * Required: nvtxs, ncon, xadj[n+1], adjncy[xadj[n]], nparts, part[n].
+ * Optional (NULL = default): vwgt[n*ncon] (unit), vsize (ignored, as in the
+ * reference), adjwgt[xadj[n]] (unit), tpwgts[nparts*ncon] (1/nparts),
+ * ubvec[ncon] (1 + ufactor/1000), options (defaults), objval (not written).
+ * The caller owns all buffers; the library copies the inputs and writes only
+ * part[0..n) and *objval. */
+RMETIS_API int RMETIS_PartGraphKway(const idx_t *nvtxs, const idx_t *ncon, const idx_t *xadj, const idx_t *adjncy,
+                         const idx_t *vwgt, const idx_t *vsize, const idx_t *adjwgt, const idx_t *nparts,
+                         const real_t *tpwgts, const real_t *ubvec, const idx_t *options, idx_t *objval,
+                         idx_t *part);
+
+/* ---- GPU extensions ---------------------------------------------------- */
+
+/* Same contract as RMETIS_PartGraphKway, but xadj, adjncy, vwgt, adjwgt and part
+ * are device pointers (current device). Scalars, tpwgts, ubvec, options and
+ * objval stay on the host. No reference counterpart (additive). */
+RMETIS_API int RMETIS_GPU_PartGraphKwayDevice(const idx_t *nvtxs, const idx_t *ncon, const idx_t *d_xadj,
+                                   const idx_t *d_adjncy, const idx_t *d_vwgt, const idx_t *d_adjwgt,
+                                   const idx_t *nparts, const real_t *tpwgts, const real_t *ubvec,
+                                   const idx_t *options, idx_t *objval, idx_t *d_part);
+
+/* Runs the engine of the current device on `stream` (a cudaStream_t; NULL =
+ * the engine's own stream). */
+RMETIS_API int RMETIS_GPU_SetStream(void *stream);
+
+/* Engine knobs without a METIS option slot: grown partitions per attempt
+ * (lowest cut kept), matching rounds per level, and whether a graph without
+ * vertex weights gets summed coarse weights (1) or the reference's unit coarse
+ * weights (0, default). Values < 0 leave a knob unchanged. */
+RMETIS_API int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weights);
+
+/* Per-launch CUDA-event timing of the hot kernels (off by default).
+ * RMETIS_GPU_GetProfile fills, per kernel id (0 gain, 1 decide, 2 propose,
+ * 3 contract, 4 cut, 5 grow), launches[i], ms[i] (summed device time) and
+ * bytes[i] (summed algorithmic bytes); returns the number of ids. With
+ * max_ids above that number, launches[ids] receives the count of all kernel
+ * launches made by this library in the process so far. */
+RMETIS_API int RMETIS_GPU_SetProfiling(int on);
+RMETIS_API int RMETIS_GPU_GetProfile(int64_t *launches, double *ms, double *bytes, int max_ids);
+
+/* Like RMETIS_PartGraphKway, and also returns the random choices of the kept
+ * attempt: the matching of every coarsening level (concatenated into
+ * matchings, level offsets in level_off[0..nlevels]) and the nparts grow seeds.
+ * matchings_cap / level_off_cap are the capacities of those arrays; a trace
+ * that does not fit returns METIS_ERROR_MEMORY. stats (optional, 3 entries):
+ * refinement passes, moves, decision rounds of the kept attempt. */
+RMETIS_API int RMETIS_GPU_PartGraphKwayTrace(const idx_t *nvtxs, const idx_t *ncon, const idx_t *xadj, const idx_t *adjncy,
+                                  const idx_t *vwgt, const idx_t *adjwgt, const idx_t *nparts,
+                                  const real_t *tpwgts, const real_t *ubvec, const idx_t *options, idx_t *objval,
+                                  idx_t *part, idx_t *matchings, int64_t matchings_cap, int64_t *level_off,
+                                  int64_t level_off_cap, int64_t *nlevels, idx_t *grow_seeds, int64_t *stats);
+
+/* ---- hot-path functions (host pointers; one call = upload, kernels, download) */
+
+/* Graph::edge_cut (src/graph/mod.rs:123-137). adjwgt may be NULL. */
+RMETIS_API int RMETIS_GPU_EdgeCut(idx_t n, const idx_t *xadj, const idx_t *adjncy, const idx_t *adjwgt, const idx_t *part,
+                       idx_t *cut);
+
+/* Graph::partition_weights (src/graph/mod.rs:140-149): pw[nparts*ncon]. */
+RMETIS_API int RMETIS_GPU_PartitionWeights(idx_t n, idx_t ncon, const idx_t *vwgt, const idx_t *part, idx_t nparts,
+                                idx_t *pw);
+
+/* Graph::build_coarse_graph (src/graph/mod.rs:284-384) for a given matching
+ * (an involution; match[v] == v means unmatched). Outputs cmap[n],
+ * cxadj[n+1], cadjncy/cadjwgt[xadj[n]] capacity, cvwgt[n*ncon] (written when
+ * vwgt != NULL), *cn. Coarse edge weights are always returned (1 where the
+ * reference keeps no coarse adjwgt). */
+RMETIS_API int RMETIS_GPU_BuildCoarseGraph(idx_t n, idx_t ncon, const idx_t *xadj, const idx_t *adjncy, const idx_t *vwgt,
+                                const idx_t *adjwgt, const idx_t *match, idx_t *cn, idx_t *cmap, idx_t *cxadj,
+                                idx_t *cadjncy, idx_t *cadjwgt, idx_t *cvwgt);
+
+/* Projection fine[v] = coarse[cmap[v]] (src/partition/kway.rs:81-84). */
+RMETIS_API int RMETIS_GPU_Project(idx_t n_fine, const idx_t *cmap, idx_t n_coarse, const idx_t *coarse_part,
+                       idx_t *fine_part);
+
+/* Gain table of a partition (boundary_vertices src/graph/mod.rs:164-171 and
+ * compute_move_gain src/refine/greedy.rs:197-218): boundary[n] flags,
+ * wfrom[n], ncand[n] and, at cand_part/cand_gain[xadj[v]..], the parts with
+ * nonzero connection weight sorted by (gain desc, part asc). For any other
+ * part p != part[v], gain(v, p) = -wfrom[v]. */
+RMETIS_API int RMETIS_GPU_GainTable(idx_t n, const idx_t *xadj, const idx_t *adjncy, const idx_t *adjwgt, const idx_t *part,
+                         idx_t nparts, idx_t *boundary, idx_t *ncand, idx_t *wfrom, idx_t *cand_part,
+                         idx_t *cand_gain);
+
+/* Parallel matching replacing shem_matching / random_matching
+ * (src/coarsen/shem.rs:13-56, src/coarsen/rm.rs:13-43): mode 1 = heavy
+ * edge, 0 = random. match[n] is an involution. */
+RMETIS_API int RMETIS_GPU_Match(idx_t n, const idx_t *xadj, const idx_t *adjncy, const idx_t *adjwgt, int mode, uint64_t seed,
+                     int rounds, idx_t *match);
+
+/* grow_partition (src/initial/grow.rs:12-103) for ntrials seed sets
+ * seeds[ntrials*nparts]; targets[nparts*ncon] are the f64 targets the
+ * reference passes in (compute_target_weights). parts[ntrials*n], cuts[ntrials]
+ * (sum over both directions). */
+RMETIS_API int RMETIS_GPU_GrowPartition(idx_t n, idx_t ncon, const idx_t *xadj, const idx_t *adjncy, const idx_t *vwgt,
+                             const idx_t *adjwgt, idx_t nparts, const double *targets, idx_t ntrials,
+                             const idx_t *seeds, idx_t *parts, int64_t *cuts);
+
+/* greedy_refine (src/refine/greedy.rs:12-22, :36-193): part updated in place;
+ * targets[nparts*ncon] and ubvec[ncon] in f64 as the reference passes them.
+ * *cut receives the edge cut afterwards; stats (optional, 4 entries): passes,
+ * moves, decision rounds, movers. */
+RMETIS_API int RMETIS_GPU_GreedyRefine(idx_t n, idx_t ncon, const idx_t *xadj, const idx_t *adjncy, const idx_t *vwgt,
+                            const idx_t *adjwgt, idx_t *part, idx_t nparts, const double *targets,
+                            const double *ubvec, idx_t niter, idx_t *cut, int64_t *stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RMETIS_B200_H */

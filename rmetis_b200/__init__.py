@@ -1,0 +1,365 @@
+"""rmetis_b200 — B200-native multilevel k-way graph partitioning.
+
+A Python mirror of the reference's public k-way API (javagg/rmetis:
+`Graph` src/graph/mod.rs:13-50, `Options` src/types.rs:52-117,
+`part_graph_kway` src/lib.rs:48-56, `PartitionResult` src/types.rs:125-130,
+`MetisError` src/types.rs:146-161) over the C ABI in include/rmetis.h. All
+compute runs in librmetis_gpu.so on the GPU; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import F32P, F64P, I32P, I64P
+
+__all__ = [
+    "CType", "IpType", "RType", "ObjType", "Options", "Graph", "PartitionResult", "MetisError", "InputError",
+    "OutOfMemoryError", "InternalError", "part_graph_kway", "set_default_options", "METIS_OK",
+    "METIS_ERROR_INPUT", "METIS_ERROR_MEMORY", "METIS_ERROR", "METIS_NOPTIONS",
+]
+
+METIS_OK = 1
+METIS_ERROR_INPUT = -2
+METIS_ERROR_MEMORY = -3
+METIS_ERROR = -4
+METIS_NOPTIONS = 40
+
+(OPT_PTYPE, OPT_OBJTYPE, OPT_CTYPE, OPT_IPTYPE, OPT_RTYPE, OPT_DBGLVL, OPT_NITER, OPT_NCUTS, OPT_SEED,
+ OPT_NO2HOP, OPT_MINCONN, OPT_CONTIG) = range(12)
+OPT_UFACTOR = 16
+OPT_NUMBERING = 17
+
+
+class CType(enum.IntEnum):
+    Rm = 0
+    Shem = 1
+
+
+class IpType(enum.IntEnum):
+    Grow = 0
+    Random = 1
+    MetisRb = 4
+
+
+class RType(enum.IntEnum):
+    Fm = 0
+    Greedy = 1
+
+
+class ObjType(enum.IntEnum):
+    Cut = 0
+    Vol = 1
+
+
+class MetisError(Exception):
+    """Base error (src/types.rs:146-161)."""
+    code = METIS_ERROR
+
+
+class InputError(MetisError):
+    code = METIS_ERROR_INPUT
+
+
+class OutOfMemoryError(MetisError):
+    code = METIS_ERROR_MEMORY
+
+
+class InternalError(MetisError):
+    code = METIS_ERROR
+
+
+def _raise_for(rc: int, what: str):
+    if rc == METIS_OK:
+        return
+    if rc == METIS_ERROR_INPUT:
+        raise InputError(f"{what}: input error")
+    if rc == METIS_ERROR_MEMORY:
+        raise OutOfMemoryError(f"{what}: out of memory")
+    raise InternalError(f"{what}: error {rc}")
+
+
+@dataclass
+class Options:
+    """All tuning parameters (src/types.rs:52-95); defaults mirror
+    Options::default(), including rtype Fm."""
+    ctype: CType = CType.Shem
+    iptype: IpType = IpType.Grow
+    rtype: RType = RType.Fm
+    objtype: ObjType = ObjType.Cut
+    no2hop: bool = False
+    ncuts: int = 1
+    niter: int = 10
+    seed: int = 0
+    minconn: bool = False
+    contig: bool = False
+    ufactor: int = 30
+    numbering: int = 0
+    dbglvl: int = 0
+
+    @classmethod
+    def for_kway(cls) -> "Options":  # src/types.rs:109-116
+        return cls(iptype=IpType.Grow, rtype=RType.Fm, ufactor=30)
+
+    @classmethod
+    def for_recursive(cls) -> "Options":  # src/types.rs:99-106
+        return cls(iptype=IpType.MetisRb, rtype=RType.Fm, ufactor=1)
+
+    def to_raw(self) -> np.ndarray:  # src/types.rs:227-245
+        a = np.full(METIS_NOPTIONS, -1, dtype=np.int32)
+        a[OPT_CTYPE] = int(self.ctype)
+        a[OPT_IPTYPE] = int(self.iptype)
+        a[OPT_RTYPE] = int(self.rtype)
+        a[OPT_OBJTYPE] = int(self.objtype)
+        a[OPT_NO2HOP] = int(self.no2hop)
+        a[OPT_NCUTS] = self.ncuts
+        a[OPT_NITER] = self.niter
+        a[OPT_SEED] = np.int64(self.seed).astype(np.int32)
+        a[OPT_MINCONN] = int(self.minconn)
+        a[OPT_CONTIG] = int(self.contig)
+        a[OPT_UFACTOR] = self.ufactor
+        a[OPT_NUMBERING] = self.numbering
+        a[OPT_DBGLVL] = self.dbglvl
+        return a
+
+    @classmethod
+    def from_raw(cls, a) -> "Options":  # src/types.rs:190-224
+        a = np.asarray(a, dtype=np.int32)
+        o = cls()
+        if a[OPT_CTYPE] == 0:
+            o.ctype = CType.Rm
+        if a[OPT_IPTYPE] == 1:
+            o.iptype = IpType.Random
+        elif a[OPT_IPTYPE] == 4:
+            o.iptype = IpType.MetisRb
+        if a[OPT_RTYPE] == 1:
+            o.rtype = RType.Greedy
+        if a[OPT_OBJTYPE] == 1:
+            o.objtype = ObjType.Vol
+        if a[OPT_NO2HOP] != 0:
+            o.no2hop = True
+        if a[OPT_NCUTS] > 0:
+            o.ncuts = int(a[OPT_NCUTS])
+        if a[OPT_NITER] > 0:
+            o.niter = int(a[OPT_NITER])
+        o.seed = max(int(a[OPT_SEED]), 0)
+        o.minconn = bool(a[OPT_MINCONN] != 0)
+        o.contig = bool(a[OPT_CONTIG] != 0)
+        if a[OPT_UFACTOR] > 0:
+            o.ufactor = int(a[OPT_UFACTOR])
+        o.numbering = int(a[OPT_NUMBERING]) & 0xFF
+        o.dbglvl = int(a[OPT_DBGLVL])
+        return o
+
+    def c_array(self) -> np.ndarray:
+        """The option array the C ABI reads: to_raw() with PTYPE set so that the
+        partitioner does not fall back to all defaults (src/ffi/c_api.rs:217)."""
+        a = self.to_raw()
+        a[OPT_PTYPE] = 0
+        return a
+
+
+@dataclass
+class PartitionResult:
+    part: np.ndarray
+    objval: int
+
+
+def _i32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _p(a, t=I32P):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def _validate(nvtxs, ncon, xadj, adjncy, vwgt, adjwgt):
+    """validate_csr (src/graph/validate.rs:16-142) on host arrays."""
+    if nvtxs <= 0:
+        raise InputError("nvtxs must be > 0")
+    if ncon <= 0:
+        raise InputError("ncon must be > 0")
+    if len(xadj) != nvtxs + 1:
+        raise InputError(f"xadj.len()={len(xadj)} but expected nvtxs+1={nvtxs + 1}")
+    if xadj[0] != 0:
+        raise InputError(f"xadj[0]={xadj[0]} but must be 0")
+    if np.any(np.diff(xadj.astype(np.int64)) < 0):
+        raise InputError("xadj is not monotone")
+    ne = int(xadj[nvtxs])
+    if len(adjncy) != ne:
+        raise InputError(f"adjncy.len()={len(adjncy)} but xadj[nvtxs]={ne}")
+    if ne:
+        if adjncy.min() < 0 or adjncy.max() >= nvtxs:
+            raise InputError("adjncy out of range")
+        src = np.repeat(np.arange(nvtxs, dtype=np.int64), np.diff(xadj.astype(np.int64)))
+        if np.any(src == adjncy):
+            raise InputError("self-loop detected")
+    deg_check = np.bincount(adjncy, minlength=nvtxs) if ne else np.zeros(nvtxs, np.int64)
+    if np.any(deg_check != np.diff(xadj.astype(np.int64))):
+        raise InputError("graph is not symmetric")
+    if adjwgt is not None and len(adjwgt) != ne:
+        raise InputError("adjwgt length mismatch")
+    if vwgt is not None:
+        if len(vwgt) != nvtxs * ncon:
+            raise InputError("vwgt length mismatch")
+        if np.any(vwgt <= 0):
+            raise InputError("vwgt must be > 0")
+
+
+class Graph:
+    """CSR graph (src/graph/mod.rs:13-50). Edge-level queries run on the GPU."""
+
+    def __init__(self, nvtxs, ncon, xadj, adjncy, vwgt=None, adjwgt=None, vsize=None, validate=True):
+        self.nvtxs = int(nvtxs)
+        self.ncon = int(ncon)
+        self.xadj = _i32(xadj)
+        self.adjncy = _i32(adjncy)
+        self.vwgt = _i32(vwgt)
+        self.adjwgt = _i32(adjwgt)
+        self.vsize = _i32(vsize)
+        if validate:
+            _validate(self.nvtxs, self.ncon, self.xadj, self.adjncy, self.vwgt, self.adjwgt)
+        self.nedges = len(self.adjncy) // 2
+
+    @classmethod
+    def new(cls, nvtxs, ncon, xadj, adjncy, vwgt=None, adjwgt=None, vsize=None) -> "Graph":
+        return cls(nvtxs, ncon, xadj, adjncy, vwgt, adjwgt, vsize)
+
+    @classmethod
+    def new_unweighted(cls, nvtxs, xadj, adjncy) -> "Graph":
+        return cls(nvtxs, 1, xadj, adjncy)
+
+    def neighbors(self, v):
+        return self.adjncy[self.xadj[v]:self.xadj[v + 1]]
+
+    def degree(self, v):
+        return int(self.xadj[v + 1] - self.xadj[v])
+
+    def edge_cut(self, part) -> int:
+        part = _i32(part)
+        cut = ctypes.c_int32(0)
+        rc = _lib.load().RMETIS_GPU_EdgeCut(self.nvtxs, _p(self.xadj), _p(self.adjncy), _p(self.adjwgt), _p(part),
+                                            ctypes.byref(cut))
+        _raise_for(rc, "edge_cut")
+        return int(cut.value)
+
+    def partition_weights(self, part, nparts) -> np.ndarray:
+        part = _i32(part)
+        out = np.zeros(nparts * self.ncon, dtype=np.int32)
+        rc = _lib.load().RMETIS_GPU_PartitionWeights(self.nvtxs, self.ncon, _p(self.vwgt), _p(part), nparts,
+                                                     _p(out))
+        _raise_for(rc, "partition_weights")
+        return out.reshape(nparts, self.ncon)
+
+    def total_weight(self) -> np.ndarray:
+        if self.vwgt is None:
+            return np.full(self.ncon, self.nvtxs, dtype=np.int32)
+        return self.vwgt.reshape(self.nvtxs, self.ncon).astype(np.int64).sum(axis=0).astype(np.int32)
+
+    def gain_table(self, part, nparts):
+        """Boundary flags, w_from and sorted explicit candidates (see
+        RMETIS_GPU_GainTable)."""
+        part = _i32(part)
+        n = self.nvtxs
+        m = len(self.adjncy)
+        b = np.zeros(n, np.int32); nc = np.zeros(n, np.int32); wf = np.zeros(n, np.int32)
+        cp = np.zeros(max(m, 1), np.int32); cg = np.zeros(max(m, 1), np.int32)
+        rc = _lib.load().RMETIS_GPU_GainTable(n, _p(self.xadj), _p(self.adjncy), _p(self.adjwgt), _p(part), nparts,
+                                              _p(b), _p(nc), _p(wf), _p(cp), _p(cg))
+        _raise_for(rc, "gain_table")
+        return b, nc, wf, cp, cg
+
+    def boundary_vertices(self, part) -> np.ndarray:
+        part = _i32(part)
+        b, *_ = self.gain_table(part, int(part.max()) + 1 if len(part) else 1)
+        return np.nonzero(b)[0].astype(np.int64)
+
+    def build_coarse_graph(self, matching):
+        """Returns (coarse Graph, cmap) (src/graph/mod.rs:284-384)."""
+        matching = _i32(matching)
+        n = self.nvtxs
+        m = len(self.adjncy)
+        cn = ctypes.c_int32(0)
+        cmap = np.zeros(n, np.int32); cx = np.zeros(n + 1, np.int32)
+        ca = np.zeros(max(m, 1), np.int32); cw = np.zeros(max(m, 1), np.int32)
+        cv = np.zeros(max(n * self.ncon, 1), np.int32)
+        rc = _lib.load().RMETIS_GPU_BuildCoarseGraph(n, self.ncon, _p(self.xadj), _p(self.adjncy), _p(self.vwgt),
+                                                     _p(self.adjwgt), _p(matching), ctypes.byref(cn), _p(cmap),
+                                                     _p(cx), _p(ca), _p(cw), _p(cv))
+        _raise_for(rc, "build_coarse_graph")
+        c = cn.value
+        cx = cx[:c + 1]
+        ce = int(cx[c])
+        cw = cw[:ce]
+        keep = self.adjwgt is not None or bool(np.any(cw != 1))
+        g = Graph(c, self.ncon, cx, ca[:ce], vwgt=None if self.vwgt is None else cv[:c * self.ncon],
+                  adjwgt=cw if keep else None, validate=False)
+        return g, cmap
+
+    def __repr__(self):
+        return f"Graph(nvtxs={self.nvtxs}, nedges={self.nedges}, ncon={self.ncon})"
+
+
+def set_default_options() -> np.ndarray:
+    a = np.zeros(METIS_NOPTIONS, dtype=np.int32)
+    _raise_for(_lib.load().RMETIS_SetDefaultOptions(_p(a)), "set_default_options")
+    return a
+
+
+def part_graph_kway(graph: Graph, nparts: int, tpwgts=None, ubvec=None, options: Options | None = None
+                    ) -> PartitionResult:
+    """Multilevel k-way partition (src/lib.rs:48-56) on the GPU.
+
+    Only RType::Greedy is on the GPU path; an Options with rtype Fm raises
+    InputError rather than running another algorithm."""
+    options = options or Options()
+    if nparts < 2:
+        raise InputError(f"nparts must be >= 2, got {nparts}")
+    if nparts > graph.nvtxs:
+        raise InputError(f"nparts={nparts} > nvtxs={graph.nvtxs}")
+    opts = options.c_array()
+    part = np.zeros(graph.nvtxs, dtype=np.int32)
+    obj = ctypes.c_int32(0)
+    nv = ctypes.c_int32(graph.nvtxs); nc = ctypes.c_int32(graph.ncon); npr = ctypes.c_int32(nparts)
+    tp = None if tpwgts is None else np.ascontiguousarray(tpwgts, dtype=np.float32)
+    ub = None if ubvec is None else np.ascontiguousarray(ubvec, dtype=np.float32)
+    rc = _lib.load().RMETIS_PartGraphKway(ctypes.byref(nv), ctypes.byref(nc), _p(graph.xadj), _p(graph.adjncy),
+                                          _p(graph.vwgt), _p(graph.vsize), _p(graph.adjwgt), ctypes.byref(npr),
+                                          _p(tp, F32P), _p(ub, F32P), _p(opts), ctypes.byref(obj), _p(part))
+    _raise_for(rc, "part_graph_kway")
+    return PartitionResult(part=part, objval=int(obj.value))
+
+
+def part_graph_kway_trace(graph: Graph, nparts: int, tpwgts=None, ubvec=None, options: Options | None = None):
+    """part_graph_kway plus the random choices of the kept attempt:
+    returns (PartitionResult, matchings per level, grow seeds, stats)."""
+    options = options or Options()
+    opts = options.c_array()
+    n = graph.nvtxs
+    part = np.zeros(n, dtype=np.int32)
+    obj = ctypes.c_int32(0)
+    nv = ctypes.c_int32(n); nc = ctypes.c_int32(graph.ncon); npr = ctypes.c_int32(nparts)
+    tp = None if tpwgts is None else np.ascontiguousarray(tpwgts, dtype=np.float32)
+    ub = None if ubvec is None else np.ascontiguousarray(ubvec, dtype=np.float32)
+    cap = 24 * n + 64
+    mats = np.zeros(cap, np.int32)
+    off = np.zeros(130, np.int64)
+    nl = ctypes.c_int64(0)
+    seeds = np.zeros(nparts, np.int32)
+    stats = np.zeros(4, np.int64)
+    rc = _lib.load().RMETIS_GPU_PartGraphKwayTrace(
+        ctypes.byref(nv), ctypes.byref(nc), _p(graph.xadj), _p(graph.adjncy), _p(graph.vwgt), _p(graph.adjwgt),
+        ctypes.byref(npr), _p(tp, F32P), _p(ub, F32P), _p(opts), ctypes.byref(obj), _p(part), _p(mats), cap,
+        _p(off, I64P), len(off), ctypes.byref(nl), _p(seeds), _p(stats, I64P))
+    _raise_for(rc, "part_graph_kway_trace")
+    L = nl.value
+    matchings = [mats[off[i]:off[i + 1]].copy() for i in range(L)]
+    return PartitionResult(part=part, objval=int(obj.value)), matchings, seeds, stats
+
+
+def set_tuning(grow_trials: int = -1, match_rounds: int = -1, summed_unit_weights: int = -1):
+    _raise_for(_lib.load().RMETIS_GPU_SetTuning(grow_trials, match_rounds, summed_unit_weights), "set_tuning")

@@ -1,0 +1,518 @@
+// extern "C" boundary: the reference's C ABI (src/ffi/c_api.rs) plus the GPU
+// extensions declared in include/rmetis.h.
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/rmetis.h"
+#include "engine.h"
+#include "prof.h"
+
+using namespace rmb;
+
+namespace {
+
+// Options::from_raw (src/types.rs:190-224) as read by parse_options
+// (src/ffi/c_api.rs:211-222): NULL or options[0] == -1 means all defaults.
+KwayOptions parse_options(const idx_t* a) {
+  KwayOptions o;
+  if (!a || a[METIS_OPTION_PTYPE] == -1) return o;
+  if (a[METIS_OPTION_CTYPE] == 0) o.ctype = 0;
+  if (a[METIS_OPTION_IPTYPE] == 1) o.iptype = 1;
+  else if (a[METIS_OPTION_IPTYPE] == 4) o.iptype = 4;
+  if (a[METIS_OPTION_RTYPE] == 1) o.rtype = 1;
+  if (a[METIS_OPTION_NCUTS] > 0) o.ncuts = a[METIS_OPTION_NCUTS];
+  if (a[METIS_OPTION_NITER] > 0) o.niter = a[METIS_OPTION_NITER];
+  o.seed = (uint64_t)(a[METIS_OPTION_SEED] > 0 ? a[METIS_OPTION_SEED] : 0);
+  if (a[METIS_OPTION_UFACTOR] > 0) o.ufactor = (uint32_t)a[METIS_OPTION_UFACTOR];
+  // objtype, no2hop, minconn, contig, numbering and dbglvl are decoded by the
+  // reference but never read on its k-way path; they have no effect here either.
+  return o;
+}
+
+struct Tuning {
+  int grow_trials = 8;
+  int match_rounds = 16;
+  int summed_unit_weights = 0;
+};
+Tuning& tuning() {
+  static Tuning t;
+  return t;
+}
+
+void apply_tuning(KwayOptions& o) {
+  o.grow_trials = tuning().grow_trials;
+  o.match_rounds = tuning().match_rounds;
+  o.summed_unit_weights = tuning().summed_unit_weights;
+}
+
+template <typename F>
+int guarded(F f) {
+  try {
+    return f();
+  } catch (const rmb::Error& e) {
+    if (std::getenv("RMETIS_B200_VERBOSE")) std::fprintf(stderr, "rmetis_b200: %s\n", e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    return METIS_ERROR_MEMORY;
+  } catch (...) {
+    return METIS_ERROR;
+  }
+}
+
+// Upload a host array into arena memory (nullptr stays nullptr).
+template <typename T>
+T* upload(Engine& E, const T* h, size_t count) {
+  if (!h) return nullptr;
+  T* d = E.arena().alloc<T>(count ? count : 1);
+  if (count) RMB_CUDA(cudaMemcpyAsync(d, h, sizeof(T) * count, cudaMemcpyHostToDevice, E.stream()));
+  return d;
+}
+
+template <typename T>
+void download(Engine& E, T* h, const T* d, size_t count) {
+  if (count) RMB_CUDA(cudaMemcpyAsync(h, d, sizeof(T) * count, cudaMemcpyDeviceToHost, E.stream()));
+}
+
+// The shared body of the host- and device-pointer entry points.
+int kway_common(Engine& E, int32_t n, int32_t nc, int32_t np, const idx_t* d_xadj, const idx_t* d_adj, int64_t ne,
+                const idx_t* d_vwgt, const idx_t* d_adjwgt, const real_t* tpwgts, const real_t* ubvec,
+                const idx_t* options, idx_t* objval, idx_t* d_part, KwayTrace* trace) {
+  KwayOptions o = parse_options(options);
+  if (o.rtype != 1) throw Error(METIS_ERROR_INPUT, "RType Fm is not on the GPU path; select Greedy");
+  apply_tuning(o);
+  DGraph g;
+  g.n = n;
+  g.m = ne;
+  g.ncon = nc;
+  g.xadj = d_xadj;
+  g.adjncy = d_adj;
+  g.adjwgt = d_adjwgt;
+  g.vwgt = d_vwgt;
+  // validate_csr (src/graph/validate.rs:16-142) on the device.
+  if (validate_device(g, E.arena(), E.stream(), E.host_scratch()) != 0)
+    throw Error(METIS_ERROR_INPUT, "graph failed validation");
+  if (np > n) throw Error(METIS_ERROR_INPUT, "nparts > nvtxs");  // kway.rs:34-37
+  int32_t obj = 0;
+  E.partition_kway(g, np, tpwgts, ubvec, o, d_part, &obj, trace);
+  if (objval) *objval = obj;
+  return METIS_OK;
+}
+
+int kway_host(const idx_t* nvtxs, const idx_t* ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
+              const idx_t* adjwgt, const idx_t* nparts, const real_t* tpwgts, const real_t* ubvec,
+              const idx_t* options, idx_t* objval, idx_t* part, KwayTrace* trace) {
+  // Mandatory pointers and scalar checks (src/ffi/c_api.rs:157-167).
+  if (!nvtxs || !ncon || !xadj || !adjncy || !nparts || !part) return METIS_ERROR_INPUT;
+  const int32_t n = *nvtxs, nc = *ncon, np = *nparts;
+  if (n <= 0 || nc <= 0 || np < 2) return METIS_ERROR_INPUT;
+  if (xadj[0] != 0 || xadj[n] < 0) return METIS_ERROR_INPUT;
+  const int64_t ne = xadj[n];
+  Engine& E = engine_for_current_device();
+  std::lock_guard<std::mutex> lk(E.mu);
+  Arena::Mark mk = E.arena().mark();
+  struct Rewind {
+    Engine& E;
+    Arena::Mark m;
+    ~Rewind() { E.arena().reset_to(m); }
+  } rw{E, mk};
+  idx_t* d_xadj = upload(E, xadj, (size_t)n + 1);
+  idx_t* d_adj = upload(E, adjncy, (size_t)ne);
+  idx_t* d_vwgt = upload(E, vwgt, (size_t)n * nc);
+  idx_t* d_adjwgt = upload(E, adjwgt, (size_t)ne);
+  idx_t* d_part = E.arena().alloc<idx_t>((size_t)n);
+  int rc = kway_common(E, n, nc, np, d_xadj, d_adj, ne, d_vwgt, d_adjwgt, tpwgts, ubvec, options, objval, d_part,
+                       trace);
+  download(E, part, d_part, (size_t)n);
+  RMB_CUDA(cudaStreamSynchronize(E.stream()));
+  return rc;
+}
+
+// Host arrays for the single-function entry points.
+struct HostCall {
+  Engine& E;
+  std::lock_guard<std::mutex> lk;
+  Arena::Mark mk;
+  HostCall() : E(engine_for_current_device()), lk(E.mu), mk(E.arena().mark()) {}
+  ~HostCall() { E.arena().reset_to(mk); }
+  cudaStream_t st() { return E.stream(); }
+  void sync() { RMB_CUDA(cudaStreamSynchronize(E.stream())); }
+};
+
+// Host-side structural checks for the single-function entry points: every
+// index a kernel will follow must be in range before anything is uploaded.
+void check_csr(idx_t n, const idx_t* xadj, const idx_t* adjncy) {
+  if (xadj[0] != 0) throw Error(METIS_ERROR_INPUT, "xadj[0] != 0");
+  for (idx_t i = 0; i < n; ++i)
+    if (xadj[i] > xadj[i + 1]) throw Error(METIS_ERROR_INPUT, "xadj not monotone");
+  for (int64_t j = 0; j < xadj[n]; ++j)
+    if (adjncy[j] < 0 || adjncy[j] >= n) throw Error(METIS_ERROR_INPUT, "adjncy out of range");
+}
+
+void check_range(const idx_t* a, int64_t len, idx_t hi, const char* what) {
+  for (int64_t i = 0; i < len; ++i)
+    if (a[i] < 0 || a[i] >= hi) throw Error(METIS_ERROR_INPUT, what);
+}
+
+DGraph dgraph(HostCall& h, idx_t n, idx_t ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
+              const idx_t* adjwgt) {
+  check_csr(n, xadj, adjncy);
+  DGraph g;
+  g.n = n;
+  g.ncon = ncon;
+  g.m = xadj ? xadj[n] : 0;
+  g.xadj = upload(h.E, xadj, (size_t)n + 1);
+  g.adjncy = upload(h.E, adjncy, (size_t)g.m);
+  g.adjwgt = upload(h.E, adjwgt, (size_t)g.m);
+  g.vwgt = upload(h.E, vwgt, (size_t)n * ncon);
+  return g;
+}
+
+}  // namespace
+
+extern "C" {
+
+int RMETIS_SetDefaultOptions(idx_t* options) {
+  if (!options) return METIS_ERROR_INPUT;
+  // Options::default().to_raw() (src/types.rs:77-95, :227-245)
+  for (int i = 0; i < METIS_NOPTIONS; ++i) options[i] = -1;
+  options[METIS_OPTION_CTYPE] = 1;      // Shem
+  options[METIS_OPTION_IPTYPE] = 0;     // Grow
+  options[METIS_OPTION_RTYPE] = 0;      // Fm
+  options[METIS_OPTION_OBJTYPE] = 0;    // Cut
+  options[METIS_OPTION_NO2HOP] = 0;
+  options[METIS_OPTION_NCUTS] = 1;
+  options[METIS_OPTION_NITER] = 10;
+  options[METIS_OPTION_SEED] = 0;
+  options[METIS_OPTION_MINCONN] = 0;
+  options[METIS_OPTION_CONTIG] = 0;
+  options[METIS_OPTION_UFACTOR] = 30;
+  options[METIS_OPTION_NUMBERING] = 0;
+  options[METIS_OPTION_DBGLVL] = 0;
+  return METIS_OK;
+}
+
+int RMETIS_PartGraphKway(const idx_t* nvtxs, const idx_t* ncon, const idx_t* xadj, const idx_t* adjncy,
+                         const idx_t* vwgt, const idx_t* vsize, const idx_t* adjwgt, const idx_t* nparts,
+                         const real_t* tpwgts, const real_t* ubvec, const idx_t* options, idx_t* objval,
+                         idx_t* part) {
+  (void)vsize;  // aggregated by the reference's contraction but never read on the k-way path
+  return guarded([&] {
+    return kway_host(nvtxs, ncon, xadj, adjncy, vwgt, adjwgt, nparts, tpwgts, ubvec, options, objval, part,
+                     nullptr);
+  });
+}
+
+int RMETIS_GPU_PartGraphKwayDevice(const idx_t* nvtxs, const idx_t* ncon, const idx_t* d_xadj,
+                                   const idx_t* d_adjncy, const idx_t* d_vwgt, const idx_t* d_adjwgt,
+                                   const idx_t* nparts, const real_t* tpwgts, const real_t* ubvec,
+                                   const idx_t* options, idx_t* objval, idx_t* d_part) {
+  return guarded([&] {
+    if (!nvtxs || !ncon || !d_xadj || !d_adjncy || !nparts || !d_part) return METIS_ERROR_INPUT;
+    const int32_t n = *nvtxs, nc = *ncon, np = *nparts;
+    if (n <= 0 || nc <= 0 || np < 2) return METIS_ERROR_INPUT;
+    Engine& E = engine_for_current_device();
+    std::lock_guard<std::mutex> lk(E.mu);
+    int32_t* hs = E.host_scratch();
+    RMB_CUDA(cudaMemcpyAsync(hs, d_xadj, sizeof(idx_t), cudaMemcpyDeviceToHost, E.stream()));
+    RMB_CUDA(cudaMemcpyAsync(hs + 1, d_xadj + n, sizeof(idx_t), cudaMemcpyDeviceToHost, E.stream()));
+    RMB_CUDA(cudaStreamSynchronize(E.stream()));
+    if (hs[0] != 0 || hs[1] < 0) return METIS_ERROR_INPUT;
+    const int64_t ne = hs[1];
+    Arena::Mark mk = E.arena().mark();
+    int rc;
+    try {
+      rc = kway_common(E, n, nc, np, d_xadj, d_adjncy, ne, d_vwgt, d_adjwgt, tpwgts, ubvec, options, objval, d_part,
+                       nullptr);
+      RMB_CUDA(cudaStreamSynchronize(E.stream()));
+    } catch (...) {
+      E.arena().reset_to(mk);
+      throw;
+    }
+    E.arena().reset_to(mk);
+    return rc;
+  });
+}
+
+int RMETIS_GPU_SetStream(void* stream) {
+  return guarded([&] {
+    Engine& E = engine_for_current_device();
+    std::lock_guard<std::mutex> lk(E.mu);
+    E.set_stream(reinterpret_cast<cudaStream_t>(stream));
+    return METIS_OK;
+  });
+}
+
+int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weights) {
+  if (grow_trials >= 0) tuning().grow_trials = grow_trials > 0 ? grow_trials : 1;
+  if (match_rounds >= 0) tuning().match_rounds = match_rounds > 0 ? match_rounds : 1;
+  if (summed_unit_weights >= 0) tuning().summed_unit_weights = summed_unit_weights ? 1 : 0;
+  return METIS_OK;
+}
+
+int RMETIS_GPU_SetProfiling(int on) {
+  return guarded([&] {
+    profiler().on = on != 0;
+    profiler().reset();
+    return METIS_OK;
+  });
+}
+
+int RMETIS_GPU_GetProfile(int64_t* launches, double* ms, double* bytes, int max_ids) {
+  return guarded([&] {
+    profiler().collect();
+    const int n = max_ids < (int)kProfCount ? max_ids : (int)kProfCount;
+    for (int i = 0; i < n; ++i) {
+      if (launches) launches[i] = profiler().totals.launches[i];
+      if (ms) ms[i] = profiler().totals.ms[i];
+      if (bytes) bytes[i] = profiler().totals.bytes[i];
+    }
+    // One slot past the kernel ids: all kernel launches of this library so far.
+    if (max_ids > (int)kProfCount && launches) launches[kProfCount] = launch_counter();
+    return (int)kProfCount;
+  });
+}
+
+int RMETIS_GPU_PartGraphKwayTrace(const idx_t* nvtxs, const idx_t* ncon, const idx_t* xadj, const idx_t* adjncy,
+                                  const idx_t* vwgt, const idx_t* adjwgt, const idx_t* nparts,
+                                  const real_t* tpwgts, const real_t* ubvec, const idx_t* options, idx_t* objval,
+                                  idx_t* part, idx_t* matchings, int64_t matchings_cap, int64_t* level_off,
+                                  int64_t level_off_cap, int64_t* nlevels, idx_t* grow_seeds, int64_t* stats) {
+  return guarded([&] {
+    KwayTrace tr;
+    int rc = kway_host(nvtxs, ncon, xadj, adjncy, vwgt, adjwgt, nparts, tpwgts, ubvec, options, objval, part, &tr);
+    if (rc != METIS_OK) return rc;
+    const int64_t L = (int64_t)tr.matchings.size();
+    if (level_off_cap < L + 1) return METIS_ERROR_MEMORY;
+    int64_t off = 0;
+    for (int64_t i = 0; i < L; ++i) {
+      level_off[i] = off;
+      const int64_t len = (int64_t)tr.matchings[i].size();
+      if (off + len > matchings_cap) return METIS_ERROR_MEMORY;
+      std::memcpy(matchings + off, tr.matchings[i].data(), sizeof(idx_t) * len);
+      off += len;
+    }
+    level_off[L] = off;
+    if (nlevels) *nlevels = L;
+    if (grow_seeds && !tr.grow_seeds.empty())
+      std::memcpy(grow_seeds, tr.grow_seeds.data(), sizeof(idx_t) * tr.grow_seeds.size());
+    if (stats) {
+      stats[0] = tr.refine_passes;
+      stats[1] = tr.refine_moves;
+      stats[2] = tr.decide_rounds;
+    }
+    return METIS_OK;
+  });
+}
+
+int RMETIS_GPU_EdgeCut(idx_t n, const idx_t* xadj, const idx_t* adjncy, const idx_t* adjwgt, const idx_t* part,
+                       idx_t* cut) {
+  return guarded([&] {
+    if (n <= 0 || !xadj || !adjncy || !part || !cut) return METIS_ERROR_INPUT;
+    HostCall h;
+    DGraph g = dgraph(h, n, 1, xadj, adjncy, nullptr, adjwgt);
+    idx_t* d_part = upload(h.E, part, (size_t)n);
+    unsigned long long* acc = h.E.arena().alloc<unsigned long long>(1);
+    cut_and_weights(g, d_part, 1, acc, nullptr, h.st());
+    unsigned long long v = 0;
+    RMB_CUDA(cudaMemcpyAsync(h.E.host_scratch(), acc, sizeof(v), cudaMemcpyDeviceToHost, h.st()));
+    h.sync();
+    std::memcpy(&v, h.E.host_scratch(), sizeof(v));
+    *cut = (idx_t)(uint32_t)v / 2;
+    return METIS_OK;
+  });
+}
+
+int RMETIS_GPU_PartitionWeights(idx_t n, idx_t ncon, const idx_t* vwgt, const idx_t* part, idx_t nparts,
+                                idx_t* pw) {
+  return guarded([&] {
+    if (n <= 0 || ncon <= 0 || nparts <= 0 || !part || !pw) return METIS_ERROR_INPUT;
+    HostCall h;
+    DGraph g;
+    g.n = n;
+    g.ncon = ncon;
+    g.vwgt = upload(h.E, vwgt, (size_t)n * ncon);
+    idx_t* d_part = upload(h.E, part, (size_t)n);
+    const size_t K = (size_t)nparts * ncon;
+    long long* d_pw = h.E.arena().alloc<long long>(K);
+    partition_weights_only(g, d_part, nparts, d_pw, h.st());
+    std::vector<long long> tmp(K);
+    download(h.E, tmp.data(), d_pw, K);
+    h.sync();
+    for (size_t i = 0; i < K; ++i) pw[i] = (idx_t)(uint32_t)(unsigned long long)tmp[i];
+    return METIS_OK;
+  });
+}
+
+int RMETIS_GPU_BuildCoarseGraph(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
+                                const idx_t* adjwgt, const idx_t* match, idx_t* cn, idx_t* cmap, idx_t* cxadj,
+                                idx_t* cadjncy, idx_t* cadjwgt, idx_t* cvwgt) {
+  return guarded([&] {
+    if (n <= 0 || ncon <= 0 || !xadj || !adjncy || !match || !cn || !cmap || !cxadj || !cadjncy || !cadjwgt)
+      return METIS_ERROR_INPUT;
+    check_range(match, n, n, "match out of range");
+    for (idx_t v = 0; v < n; ++v)
+      if (match[match[v]] != v) return METIS_ERROR_INPUT;  // must be an involution
+    HostCall h;
+    DGraph g = dgraph(h, n, ncon, xadj, adjncy, vwgt, adjwgt);
+    idx_t* d_match = upload(h.E, match, (size_t)n);
+    CoarseResult r = contract(g, d_match, vwgt ? 1 : 0, h.E.arena(), h.st(), h.E.host_scratch());
+    *cn = r.g.n;
+    download(h.E, cmap, r.cmap, (size_t)n);
+    download(h.E, cxadj, r.xadj, (size_t)r.g.n + 1);
+    download(h.E, cadjncy, r.adjncy, (size_t)r.g.m);
+    download(h.E, cadjwgt, r.adjwgt, (size_t)r.g.m);
+    if (vwgt && cvwgt) download(h.E, cvwgt, r.vwgt, (size_t)r.g.n * ncon);
+    h.sync();
+    return METIS_OK;
+  });
+}
+
+int RMETIS_GPU_Project(idx_t n_fine, const idx_t* cmap, idx_t n_coarse, const idx_t* coarse_part,
+                       idx_t* fine_part) {
+  return guarded([&] {
+    if (n_fine <= 0 || n_coarse <= 0 || !cmap || !coarse_part || !fine_part) return METIS_ERROR_INPUT;
+    check_range(cmap, n_fine, n_coarse, "cmap out of range");
+    HostCall h;
+    idx_t* d_cmap = upload(h.E, cmap, (size_t)n_fine);
+    idx_t* d_cp = upload(h.E, coarse_part, (size_t)n_coarse);
+    idx_t* d_fp = h.E.arena().alloc<idx_t>((size_t)n_fine);
+    project(n_fine, d_cmap, d_cp, d_fp, h.st());
+    download(h.E, fine_part, d_fp, (size_t)n_fine);
+    h.sync();
+    return METIS_OK;
+  });
+}
+
+int RMETIS_GPU_GainTable(idx_t n, const idx_t* xadj, const idx_t* adjncy, const idx_t* adjwgt, const idx_t* part,
+                         idx_t nparts, idx_t* boundary, idx_t* ncand, idx_t* wfrom, idx_t* cand_part,
+                         idx_t* cand_gain) {
+  return guarded([&] {
+    if (n <= 0 || nparts <= 0 || !xadj || !adjncy || !part || !boundary || !ncand || !wfrom || !cand_part ||
+        !cand_gain)
+      return METIS_ERROR_INPUT;
+    check_range(part, n, nparts, "part out of range");
+    HostCall h;
+    DGraph g = dgraph(h, n, 1, xadj, adjncy, nullptr, adjwgt);
+    idx_t* d_part = upload(h.E, part, (size_t)n);
+    idx_t* d_b = h.E.arena().alloc<idx_t>((size_t)n);
+    idx_t* d_nc = h.E.arena().alloc<idx_t>((size_t)n);
+    idx_t* d_wf = h.E.arena().alloc<idx_t>((size_t)n);
+    idx_t* d_cp = h.E.arena().alloc<idx_t>((size_t)g.m + 1);
+    idx_t* d_cg = h.E.arena().alloc<idx_t>((size_t)g.m + 1);
+    idx_t* d_heavy = h.E.arena().alloc<idx_t>((size_t)n);
+    const int32_t nh = heavy_list(g, d_heavy, h.E.arena(), h.st(), h.E.host_scratch());
+    RMB_CUDA(cudaMemsetAsync(d_nc, 0, sizeof(idx_t) * n, h.st()));
+    RMB_CUDA(cudaMemsetAsync(d_wf, 0, sizeof(idx_t) * n, h.st()));
+    gain_table(g, d_part, nparts, d_b, d_nc, d_wf, d_cp, d_cg, d_heavy, nh, h.st());
+    download(h.E, boundary, d_b, (size_t)n);
+    download(h.E, ncand, d_nc, (size_t)n);
+    download(h.E, wfrom, d_wf, (size_t)n);
+    download(h.E, cand_part, d_cp, (size_t)g.m);
+    download(h.E, cand_gain, d_cg, (size_t)g.m);
+    h.sync();
+    return METIS_OK;
+  });
+}
+
+int RMETIS_GPU_Match(idx_t n, const idx_t* xadj, const idx_t* adjncy, const idx_t* adjwgt, int mode, uint64_t seed,
+                     int rounds, idx_t* match) {
+  return guarded([&] {
+    if (n <= 0 || !xadj || !adjncy || !match || rounds <= 0) return METIS_ERROR_INPUT;
+    HostCall h;
+    DGraph g = dgraph(h, n, 1, xadj, adjncy, nullptr, adjwgt);
+    idx_t* d_heavy = h.E.arena().alloc<idx_t>((size_t)n);
+    const int32_t nh = heavy_list(g, d_heavy, h.E.arena(), h.st(), h.E.host_scratch());
+    idx_t* d_match = h.E.arena().alloc<idx_t>((size_t)n);
+    match_parallel(g, mode ? 1 : 0, seed, rounds, d_match, d_heavy, nh, h.E.arena(), h.st(), h.E.host_scratch());
+    download(h.E, match, d_match, (size_t)n);
+    h.sync();
+    return METIS_OK;
+  });
+}
+
+int RMETIS_GPU_GrowPartition(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
+                             const idx_t* adjwgt, idx_t nparts, const double* targets, idx_t ntrials,
+                             const idx_t* seeds, idx_t* parts, int64_t* cuts) {
+  return guarded([&] {
+    if (n <= 0 || ncon <= 0 || nparts <= 0 || ntrials <= 0 || !xadj || !adjncy || !targets || !seeds || !parts)
+      return METIS_ERROR_INPUT;
+    check_range(seeds, (int64_t)ntrials * nparts, n, "seed out of range");
+    for (idx_t t = 0; t < ntrials; ++t) {  // seeds of one trial are distinct (grow.rs:26-32)
+      std::vector<char> used(n, 0);
+      for (idx_t p = 0; p < nparts; ++p) {
+        const idx_t sv = seeds[(int64_t)t * nparts + p];
+        if (used[sv]) return METIS_ERROR_INPUT;
+        used[sv] = 1;
+      }
+    }
+    HostCall h;
+    DGraph g = dgraph(h, n, ncon, xadj, adjncy, vwgt, adjwgt);
+    const size_t K = (size_t)nparts * ncon;
+    std::vector<long long> grow(K);
+    for (size_t i = 0; i < K; ++i) {
+      long long f, o;
+      threshold_values(targets[i], 1.0, &f, &o, &grow[i]);
+    }
+    long long* d_grow = upload(h.E, grow.data(), K);
+    idx_t* d_seeds = upload(h.E, seeds, (size_t)ntrials * nparts);
+    idx_t* d_parts = h.E.arena().alloc<idx_t>((size_t)ntrials * n);
+    long long* d_cuts = h.E.arena().alloc<long long>((size_t)ntrials);
+    grow_trials(g, nparts, ntrials, d_seeds, d_grow, d_parts, d_cuts, h.E.arena(), h.st());
+    download(h.E, parts, d_parts, (size_t)ntrials * n);
+    std::vector<long long> c(ntrials);
+    download(h.E, c.data(), d_cuts, (size_t)ntrials);
+    h.sync();
+    if (cuts)
+      for (int i = 0; i < ntrials; ++i) cuts[i] = c[i];
+    return METIS_OK;
+  });
+}
+
+int RMETIS_GPU_GreedyRefine(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
+                            const idx_t* adjwgt, idx_t* part, idx_t nparts, const double* targets,
+                            const double* ubvec, idx_t niter, idx_t* cut, int64_t* stats) {
+  return guarded([&] {
+    if (n <= 0 || ncon <= 0 || nparts <= 0 || niter < 0 || !xadj || !adjncy || !part || !targets || !ubvec)
+      return METIS_ERROR_INPUT;
+    check_range(part, n, nparts, "part out of range");
+    HostCall h;
+    DGraph g = dgraph(h, n, ncon, xadj, adjncy, vwgt, adjwgt);
+    const size_t K = (size_t)nparts * ncon;
+    std::vector<long long> feas(K), over(K), grow(K);
+    for (int p = 0; p < nparts; ++p)
+      for (int c = 0; c < ncon; ++c) {
+        const size_t i = (size_t)p * ncon + c;
+        threshold_values(targets[i], ubvec[c], &feas[i], &over[i], &grow[i]);
+      }
+    long long* d_feas = upload(h.E, feas.data(), K);
+    long long* d_over = upload(h.E, over.data(), K);
+    idx_t* d_part = upload(h.E, part, (size_t)n);
+    idx_t* d_heavy = h.E.arena().alloc<idx_t>((size_t)n);
+    const int32_t nh = heavy_list(g, d_heavy, h.E.arena(), h.st(), h.E.host_scratch());
+    RefineParams rp;
+    rp.k = nparts;
+    rp.niter = niter;
+    rp.feas_max = d_feas;
+    rp.over_thr = d_over;
+    RefineStats rs = greedy_refine(g, d_part, rp, d_heavy, nh, h.E.arena(), h.st(), h.E.host_scratch());
+    unsigned long long* acc = h.E.arena().alloc<unsigned long long>(1);
+    cut_and_weights(g, d_part, nparts, acc, nullptr, h.st());
+    download(h.E, part, d_part, (size_t)n);
+    unsigned long long v = 0;
+    RMB_CUDA(cudaMemcpyAsync(h.E.host_scratch(), acc, sizeof(v), cudaMemcpyDeviceToHost, h.st()));
+    h.sync();
+    std::memcpy(&v, h.E.host_scratch(), sizeof(v));
+    if (cut) *cut = (idx_t)(uint32_t)v / 2;
+    if (stats) {
+      stats[0] = rs.passes;
+      stats[1] = rs.moves;
+      stats[2] = rs.decide_iters;
+      stats[3] = rs.movers;
+    }
+    return METIS_OK;
+  });
+}
+
+}  // extern "C"

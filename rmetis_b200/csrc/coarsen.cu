@@ -1,0 +1,482 @@
+// Coarsening: parallel matching (locally dominant edges) and contraction.
+#include "kernels.h"
+#include "prof.h"
+#include "scan.cuh"
+
+namespace rmb {
+
+// ---------------------------------------------------------------------------
+// Matching
+//
+// The reference visits vertices one at a time (shem.rs:13-56, rm.rs:13-43).
+// Here every unmatched vertex points at its best unmatched neighbour under a
+// global strict order on edges; mutual pointers match. The order is
+// (edge weight, seeded hash of the edge, endpoint ids) for SHEM and (hash,
+// ids) for RM. An edge that is the best for both endpoints always exists, so
+// every round matches at least one pair; this is the conflict-free form of
+// the reference's distributed proposal exchange (coarsen/mod.rs:75-143).
+// ---------------------------------------------------------------------------
+__device__ inline uint32_t edge_hash(uint64_t seed, int32_t a, int32_t b) {
+  int32_t lo = a < b ? a : b, hi = a < b ? b : a;
+  return (uint32_t)(mix64(seed ^ (((uint64_t)(uint32_t)lo << 32) | (uint32_t)hi)) >> 32);
+}
+
+struct EdgeKey {
+  int32_t w;
+  uint32_t h;
+  int32_t u;
+  __device__ bool better(const EdgeKey& o) const {
+    if (w != o.w) return w > o.w;
+    if (h != o.h) return h > o.h;
+    return u > o.u;
+  }
+};
+
+template <bool HAS_W, int MODE>
+__global__ void k_match_propose(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                                const idx_t* __restrict__ adjwgt, int32_t n, const idx_t* __restrict__ match,
+                                idx_t* __restrict__ prop, uint64_t seed) {
+  RMB_GRID_STRIDE(v, n) {
+    if (match[v] >= 0) continue;
+    const int32_t s = xadj[v], e = xadj[v + 1];
+    if (e - s > kHeavyDegree) continue;
+    EdgeKey best{INT32_MIN, 0u, -1};
+    bool have = false;
+    for (int32_t j = s; j < e; ++j) {
+      const int32_t u = adj[j];
+      if (match[u] >= 0) continue;
+      EdgeKey k{MODE == 1 ? (HAS_W ? adjwgt[j] : 1) : 0, edge_hash(seed, (int32_t)v, u), u};
+      if (!have || k.better(best)) { best = k; have = true; }
+    }
+    prop[v] = have ? best.u : -1;
+  }
+}
+
+template <bool HAS_W, int MODE>
+__global__ void k_match_propose_heavy(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                                      const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ heavy,
+                                      int32_t nheavy, const idx_t* __restrict__ match, idx_t* __restrict__ prop,
+                                      uint64_t seed) {
+  const int lane = threadIdx.x & 31;
+  const int32_t nw = gridDim.x * (blockDim.x >> 5);
+  for (int32_t i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < nheavy; i += nw) {
+    const int32_t v = heavy[i];
+    if (match[v] >= 0) continue;  // warp-uniform
+    EdgeKey best{INT32_MIN, 0u, -1};
+    bool have = false;
+    for (int32_t j = xadj[v] + lane; j < xadj[v + 1]; j += 32) {
+      const int32_t u = adj[j];
+      if (match[u] >= 0) continue;
+      EdgeKey k{MODE == 1 ? (HAS_W ? adjwgt[j] : 1) : 0, edge_hash(seed, v, u), u};
+      if (!have || k.better(best)) { best = k; have = true; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      EdgeKey other;
+      other.w = __shfl_xor_sync(0xffffffffu, best.w, o);
+      other.h = __shfl_xor_sync(0xffffffffu, best.h, o);
+      other.u = __shfl_xor_sync(0xffffffffu, best.u, o);
+      int oh = __shfl_xor_sync(0xffffffffu, (int)have, o);
+      if (oh && (!have || other.better(best))) { best = other; have = true; }
+    }
+    if (lane == 0) prop[v] = have ? best.u : -1;
+  }
+}
+
+__global__ void k_match_init(int32_t n, idx_t* match) {
+  RMB_GRID_STRIDE(v, n) { match[v] = -1; }
+}
+
+__global__ void k_match_accept(int32_t n, const idx_t* __restrict__ prop, idx_t* __restrict__ match,
+                               int32_t* __restrict__ newly) {
+  int32_t cnt = 0;
+  RMB_GRID_STRIDE(v, n) {
+    if (match[v] < 0) {
+      const int32_t u = prop[v];
+      if (u >= 0 && prop[u] == (int32_t)v) {
+        match[v] = u;
+        ++cnt;
+      }
+    }
+  }
+  cnt = warp_sum(cnt);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(newly, cnt);
+}
+
+__global__ void k_match_finalize(int32_t n, idx_t* match) {
+  RMB_GRID_STRIDE(v, n) {
+    if (match[v] < 0) match[v] = (idx_t)v;
+  }
+}
+
+void match_parallel(const DGraph& g, int mode, uint64_t seed, int rounds, idx_t* match, const idx_t* heavy,
+                    int32_t nheavy, Arena& arena, cudaStream_t st, int32_t* h_scratch) {
+  Arena::Mark mk = arena.mark();
+  idx_t* prop = arena.alloc<idx_t>((size_t)g.n);
+  int32_t* newly = arena.alloc<int32_t>((size_t)rounds + 1);
+  RMB_CUDA(cudaMemsetAsync(newly, 0, sizeof(int32_t) * ((size_t)rounds + 1), st));
+  const int blocks = grid_for(g.n, 256);
+  k_match_init<<<blocks, 256, 0, st>>>(g.n, match);
+  RMB_LAUNCH_CHECK();
+  const bool w = g.adjwgt != nullptr;
+  for (int r = 0; r < rounds; ++r) {
+    // Round 0 reads every row: xadj, match (own + gathers), adjncy, adjwgt, prop.
+    const int ph = r == 0 ? profiler().begin(kProfPropose, st) : -1;
+#define RMB_PROP(HW, MD)                                                                                  \
+  k_match_propose<HW, MD><<<blocks, 256, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, g.n, match, prop, seed);   \
+  if (nheavy > 0)                                                                                         \
+    k_match_propose_heavy<HW, MD><<<grid_for(nheavy, 8, 148 * 8), 256, 0, st>>>(                         \
+        g.xadj, g.adjncy, g.adjwgt, heavy, nheavy, match, prop, seed);
+    if (mode == 1) {
+      if (w) { RMB_PROP(true, 1) } else { RMB_PROP(false, 1) }
+    } else {
+      RMB_PROP(false, 0)
+    }
+#undef RMB_PROP
+    RMB_LAUNCH_CHECK();
+    profiler().end(ph, st, 12.0 * g.n + (w && mode == 1 ? 12.0 : 8.0) * (double)g.m);
+    k_match_accept<<<blocks, 256, 0, st>>>(g.n, prop, match, newly + r);
+    RMB_LAUNCH_CHECK();
+    // On large levels stop once a round matches almost nothing new.
+    if (g.n > 200000 && r >= 3 && (r & 1) == 1) {
+      RMB_CUDA(cudaMemcpyAsync(h_scratch, newly + r, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+      RMB_CUDA(cudaStreamSynchronize(st));
+      if ((int64_t)h_scratch[0] * 2 * 200 < (int64_t)g.n) break;
+    }
+  }
+  k_match_finalize<<<blocks, 256, 0, st>>>(g.n, match);
+  RMB_LAUNCH_CHECK();
+  arena.reset_to(mk);
+}
+
+// ---------------------------------------------------------------------------
+// Contraction (src/graph/mod.rs:284-384)
+// ---------------------------------------------------------------------------
+struct LoadLeader {
+  const idx_t* match;
+  __device__ idx_t operator()(int64_t v) const { return match[v] >= (idx_t)v ? 1 : 0; }
+};
+
+// cmap numbering identical to the reference's ascending scan (mod.rs:286-297):
+// the coarse id of a pair is the number of leaders (min endpoint) before it.
+__global__ void k_build_cmap(const idx_t* __restrict__ xadj, int32_t n, const idx_t* __restrict__ match,
+                             const idx_t* __restrict__ cidx, idx_t* __restrict__ cmap, idx_t* __restrict__ mem0,
+                             idx_t* __restrict__ mem1, idx_t* __restrict__ ub) {
+  RMB_GRID_STRIDE(v, n) {
+    const int32_t m = match[v];
+    if (m >= (int32_t)v) {
+      const int32_t c = cidx[v];
+      cmap[v] = c;
+      mem0[c] = (idx_t)v;
+      const bool pair = m != (int32_t)v;
+      mem1[c] = pair ? m : -1;
+      ub[c] = (xadj[v + 1] - xadj[v]) + (pair ? (xadj[m + 1] - xadj[m]) : 0);
+    } else {
+      cmap[v] = cidx[m];
+    }
+  }
+}
+
+__global__ void k_coarse_vwgt(int32_t cn, int32_t ncon, const idx_t* __restrict__ mem0,
+                              const idx_t* __restrict__ mem1, const idx_t* __restrict__ vwgt,
+                              idx_t* __restrict__ cvwgt) {
+  RMB_GRID_STRIDE(i, (int64_t)cn * ncon) {
+    const int64_t c = i / ncon;
+    const int cc = (int)(i - c * ncon);
+    const int32_t a = mem0[c], b = mem1[c];
+    idx_t w = vwgt ? vwgt[(int64_t)a * ncon + cc] : 1;
+    if (b >= 0) w += vwgt ? vwgt[(int64_t)b * ncon + cc] : 1;
+    cvwgt[i] = w;
+  }
+}
+
+// Merge of one coarse row in registers (bound <= kContractThreadMax). The
+// row of the first member is scanned before the second, each in CSR order,
+// and a neighbour is appended at its first appearance (mod.rs:323-341).
+template <bool HAS_W>
+__global__ void k_contract_thread(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                                  const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ cmap, int32_t cn,
+                                  const idx_t* __restrict__ mem0, const idx_t* __restrict__ mem1,
+                                  const idx_t* __restrict__ ub, const idx_t* __restrict__ ub_off,
+                                  idx_t* __restrict__ tmp_adj, idx_t* __restrict__ tmp_w, idx_t* __restrict__ cdeg,
+                                  idx_t* __restrict__ hlist, int32_t* __restrict__ hcount) {
+  constexpr int T = kContractThreadMax;
+  RMB_GRID_STRIDE(c, cn) {
+    if (ub[c] > T) {
+      hlist[atomicAdd(hcount, 1)] = (idx_t)c;
+      continue;
+    }
+    int32_t keys[T];
+    int32_t wts[T];
+#pragma unroll
+    for (int i = 0; i < T; ++i) { keys[i] = -1; wts[i] = 0; }
+    int cnt = 0;
+#pragma unroll
+    for (int mbr = 0; mbr < 2; ++mbr) {
+      const int32_t src = mbr == 0 ? mem0[c] : mem1[c];
+      if (src < 0) continue;
+      const int32_t s = xadj[src], e = xadj[src + 1];
+      for (int32_t j = s; j < e; ++j) {
+        const int32_t cu = cmap[adj[j]];
+        if (cu == (int32_t)c) continue;
+        const int32_t w = HAS_W ? adjwgt[j] : 1;
+        bool found = false;
+#pragma unroll
+        for (int i = 0; i < T; ++i) {
+          if (i < cnt && keys[i] == cu) { wts[i] += w; found = true; }
+        }
+        if (!found) {
+#pragma unroll
+          for (int i = 0; i < T; ++i) {
+            if (i == cnt) { keys[i] = cu; wts[i] = w; }
+          }
+          ++cnt;
+        }
+      }
+    }
+    const int32_t off = ub_off[c];
+#pragma unroll
+    for (int i = 0; i < T; ++i) {
+      if (i < cnt) { tmp_adj[off + i] = keys[i]; tmp_w[off + i] = wts[i]; }
+    }
+    cdeg[c] = cnt;
+  }
+}
+
+constexpr int kWarpTable = 1024;  // shared hash slots per warp
+
+// Merge of a long coarse row by one warp, 32 entries at a time, with an
+// open-addressing table (shared memory, or global scratch for long rows).
+// New keys of a chunk get slots in lane order, which keeps first-appearance
+// order; each key's weights are summed by the lowest lane holding it.
+template <bool HAS_W>
+__global__ void k_contract_warp(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                                const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ cmap,
+                                const idx_t* __restrict__ mem0, const idx_t* __restrict__ mem1,
+                                const idx_t* __restrict__ ub, const idx_t* __restrict__ ub_off,
+                                const idx_t* __restrict__ hlist, const int32_t* __restrict__ hcount,
+                                idx_t* __restrict__ tmp_adj, idx_t* __restrict__ tmp_w, idx_t* __restrict__ cdeg,
+                                int32_t* __restrict__ gkey, int32_t* __restrict__ gslot) {
+  __shared__ int32_t skey_all[4][kWarpTable];
+  __shared__ int32_t sslot_all[4][kWarpTable];
+  __shared__ int32_t lanew_all[4][32];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int32_t* lanew = lanew_all[wib];
+  const int32_t nh = *hcount;
+  const int32_t nw = gridDim.x * (blockDim.x >> 5);
+  for (int32_t hi = blockIdx.x * (blockDim.x >> 5) + wib; hi < nh; hi += nw) {
+    const int32_t c = hlist[hi];
+    const int32_t ubc = ub[c];
+    const int32_t off = ub_off[c];
+    int32_t tsize;
+    int32_t *tkey, *tslot;
+    if (2 * ubc <= kWarpTable) {
+      tsize = 2 * ubc;
+      tkey = skey_all[wib];
+      tslot = sslot_all[wib];
+    } else {
+      tsize = 2 * ubc;
+      tkey = gkey + 2 * (int64_t)off;
+      tslot = gslot + 2 * (int64_t)off;
+    }
+    for (int32_t i = lane; i < tsize; i += 32) tkey[i] = -1;
+    __syncwarp();
+    int32_t U = 0;
+    for (int mbr = 0; mbr < 2; ++mbr) {
+      const int32_t src = mbr == 0 ? mem0[c] : mem1[c];
+      if (src < 0) break;
+      const int32_t e = xadj[src + 1];
+      for (int32_t base = xadj[src]; base < e; base += 32) {
+        const int32_t j = base + lane;
+        int32_t cu = -1, w = 0;
+        bool valid = j < e;
+        if (valid) {
+          cu = cmap[adj[j]];
+          valid = cu != c;
+          w = HAS_W ? adjwgt[j] : 1;
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, valid ? cu : -(lane + 2));
+        const bool leader = valid && (__ffs(peers) - 1) == lane;
+        lanew[lane] = valid ? w : 0;
+        __syncwarp();
+        int32_t gsum = 0;
+        if (leader) {
+          unsigned m = peers;
+          while (m) {
+            const int b = __ffs(m) - 1;
+            gsum += lanew[b];
+            m &= m - 1;
+          }
+        }
+        int32_t slot = -1, hpos = -1;
+        bool isnew = false;
+        if (leader) {
+          int32_t h = (int32_t)(((uint32_t)cu * 0x9E3779B1u) % (uint32_t)tsize);
+          for (int32_t probe = 0; probe < tsize; ++probe) {
+            const int32_t k0 = atomicCAS(&tkey[h], -1, cu);
+            if (k0 == -1) { isnew = true; hpos = h; break; }
+            if (k0 == cu) { slot = tslot[h]; break; }
+            h = (h + 1 == tsize) ? 0 : h + 1;
+          }
+        }
+        const unsigned newmask = __ballot_sync(0xffffffffu, isnew);
+        if (isnew) {
+          slot = U + __popc(newmask & lanemask_lt());
+          tslot[hpos] = slot;
+          tmp_adj[off + slot] = cu;
+          tmp_w[off + slot] = gsum;
+        } else if (leader && slot >= 0) {
+          tmp_w[off + slot] += gsum;
+        }
+        U += __popc(newmask);
+        __syncwarp();
+      }
+    }
+    if (lane == 0) cdeg[c] = U;
+    __syncwarp();
+  }
+}
+
+// Gather the merged rows into the final coarse CSR (one warp per 32 coarse
+// vertices, striding over their contiguous scratch range).
+__global__ void k_contract_compact(int32_t cn, const idx_t* __restrict__ ub_off, const idx_t* __restrict__ cdeg,
+                                   const idx_t* __restrict__ cxadj, const idx_t* __restrict__ tmp_adj,
+                                   const idx_t* __restrict__ tmp_w, idx_t* __restrict__ cadj,
+                                   idx_t* __restrict__ cw) {
+  __shared__ int32_t xs_all[8][33];
+  int32_t* xs = xs_all[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int32_t nw = gridDim.x * (blockDim.x >> 5);
+  for (int32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); (int64_t)w * 32 < cn; w += nw) {
+    const int32_t v0 = w * 32;
+    const int32_t vend = min(v0 + 32, cn);
+    const int cnt = vend - v0;
+    if (lane < cnt) xs[lane] = ub_off[v0 + lane];
+    if (lane == 0) xs[cnt] = ub_off[vend];
+    __syncwarp();
+    const int32_t e0 = xs[0], e1 = xs[cnt];
+    for (int32_t p = e0 + lane; p < e1; p += 32) {
+      int lo = 0, hi = cnt;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (xs[mid] <= p) lo = mid; else hi = mid;
+      }
+      const int32_t c = v0 + lo;
+      const int32_t i = p - xs[lo];
+      if (i < cdeg[c]) {
+        const int32_t dst = cxadj[c] + i;
+        cadj[dst] = tmp_adj[p];
+        cw[dst] = tmp_w[p];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+struct LoadHeavy {
+  const idx_t* xadj;
+  __device__ idx_t operator()(int64_t v) const { return (xadj[v + 1] - xadj[v]) > kHeavyDegree ? 1 : 0; }
+};
+struct StoreHeavy {
+  const idx_t* xadj;
+  idx_t* out;
+  __device__ void operator()(int64_t v, idx_t pos) const {
+    if ((xadj[v + 1] - xadj[v]) > kHeavyDegree) out[pos] = (idx_t)v;
+  }
+};
+
+int32_t heavy_list(const DGraph& g, idx_t* out, Arena& arena, cudaStream_t st, int32_t* h_scratch) {
+  Arena::Mark mk = arena.mark();
+  idx_t* cnt = arena.alloc<idx_t>(1);
+  exclusive_scan<idx_t>(LoadHeavy{g.xadj}, StoreHeavy{g.xadj, out}, g.n, cnt, arena, st);
+  RMB_CUDA(cudaMemcpyAsync(h_scratch, cnt, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  RMB_CUDA(cudaStreamSynchronize(st));
+  arena.reset_to(mk);
+  return h_scratch[0];
+}
+
+CoarseResult contract(const DGraph& g, const idx_t* match, int coarse_vwgt, Arena& arena, cudaStream_t st,
+                      int32_t* h_scratch) {
+  CoarseResult r;
+  const int32_t n = g.n;
+  // The coarse level is allocated first at upper-bound sizes (cn <= n,
+  // cm <= m) so that all scratch below the mark is released on return.
+  idx_t* cmap = arena.alloc<idx_t>((size_t)n);
+  idx_t* counts = arena.alloc<idx_t>(4);  // [0] = cn, [1] = heavy rows
+  idx_t* cxadj = arena.alloc<idx_t>((size_t)n + 1);
+  idx_t* cadj = arena.alloc<idx_t>((size_t)g.m + 1);
+  idx_t* cw = arena.alloc<idx_t>((size_t)g.m + 1);
+  idx_t* cvwgt = coarse_vwgt ? arena.alloc<idx_t>((size_t)n * g.ncon) : nullptr;
+  Arena::Mark mk = arena.mark();
+  idx_t* cidx = arena.alloc<idx_t>((size_t)n);
+  exclusive_scan<idx_t>(LoadLeader{match}, StoreArr<idx_t>{cidx}, n, counts, arena, st);
+  // cn sizes the coarse level; one readback per level.
+  RMB_CUDA(cudaMemcpyAsync(h_scratch, counts, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  RMB_CUDA(cudaStreamSynchronize(st));
+  const int32_t cn = h_scratch[0];
+  idx_t* mem0 = arena.alloc<idx_t>((size_t)cn);
+  idx_t* mem1 = arena.alloc<idx_t>((size_t)cn);
+  idx_t* ub = arena.alloc<idx_t>((size_t)cn);
+  idx_t* ub_off = arena.alloc<idx_t>((size_t)cn + 1);
+  idx_t* cdeg = arena.alloc<idx_t>((size_t)cn);
+  idx_t* hlist = arena.alloc<idx_t>((size_t)cn);
+  idx_t* tmp_adj = arena.alloc<idx_t>((size_t)g.m + 1);
+  idx_t* tmp_w = arena.alloc<idx_t>((size_t)g.m + 1);
+  k_build_cmap<<<grid_for(n, 256), 256, 0, st>>>(g.xadj, n, match, cidx, cmap, mem0, mem1, ub);
+  RMB_LAUNCH_CHECK();
+  exclusive_scan_arr<idx_t>(ub, ub_off, cn, ub_off + cn, arena, st);
+  RMB_CUDA(cudaMemsetAsync(counts + 1, 0, sizeof(idx_t), st));
+  // members, bounds, offsets (20 B per coarse vertex), member row offsets,
+  // adjncy + cmap gathers (+ adjwgt), merged rows written (8 B per entry).
+  const int ph = profiler().begin(kProfContract, st);
+  if (g.adjwgt)
+    k_contract_thread<true><<<grid_for(cn, 128), 128, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, cmap, cn, mem0, mem1,
+                                                                ub, ub_off, tmp_adj, tmp_w, cdeg, hlist, counts + 1);
+  else
+    k_contract_thread<false><<<grid_for(cn, 128), 128, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, cmap, cn, mem0, mem1,
+                                                                 ub, ub_off, tmp_adj, tmp_w, cdeg, hlist, counts + 1);
+  RMB_LAUNCH_CHECK();
+  profiler().end(ph, st, 20.0 * cn + 8.0 * n + (g.adjwgt ? 12.0 : 8.0) * (double)g.m + 8.0 * (double)g.m);
+  RMB_CUDA(cudaMemcpyAsync(h_scratch + 1, counts + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  RMB_CUDA(cudaStreamSynchronize(st));
+  const int32_t nheavy = h_scratch[1];
+  if (nheavy > 0) {
+    int32_t* gkey = arena.alloc<int32_t>(2 * (size_t)g.m + 2);
+    int32_t* gslot = arena.alloc<int32_t>(2 * (size_t)g.m + 2);
+    const int blocks = grid_for(nheavy, 4, 148 * 8);
+    if (g.adjwgt)
+      k_contract_warp<true><<<blocks, 128, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, cmap, mem0, mem1, ub, ub_off, hlist,
+                                                     counts + 1, tmp_adj, tmp_w, cdeg, gkey, gslot);
+    else
+      k_contract_warp<false><<<blocks, 128, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, cmap, mem0, mem1, ub, ub_off, hlist,
+                                                      counts + 1, tmp_adj, tmp_w, cdeg, gkey, gslot);
+    RMB_LAUNCH_CHECK();
+  }
+  exclusive_scan_arr<idx_t>(cdeg, cxadj, cn, cxadj + cn, arena, st);
+  k_contract_compact<<<grid_for(ceil_div(cn, 32), 8, 148 * 8), 256, 0, st>>>(cn, ub_off, cdeg, cxadj, tmp_adj,
+                                                                            tmp_w, cadj, cw);
+  RMB_LAUNCH_CHECK();
+  if (coarse_vwgt) {
+    k_coarse_vwgt<<<grid_for((int64_t)cn * g.ncon, 256), 256, 0, st>>>(cn, g.ncon, mem0, mem1, g.vwgt, cvwgt);
+    RMB_LAUNCH_CHECK();
+  }
+  RMB_CUDA(cudaMemcpyAsync(h_scratch + 2, cxadj + cn, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  RMB_CUDA(cudaStreamSynchronize(st));
+  const int32_t cm = h_scratch[2];
+  arena.reset_to(mk);
+  r.cmap = cmap;
+  r.xadj = cxadj;
+  r.adjncy = cadj;
+  r.adjwgt = cw;
+  r.vwgt = cvwgt;
+  r.g.n = cn;
+  r.g.m = cm;
+  r.g.ncon = g.ncon;
+  r.g.xadj = cxadj;
+  r.g.adjncy = cadj;
+  r.g.adjwgt = cw;
+  r.g.vwgt = cvwgt;
+  return r;
+}
+
+}  // namespace rmb

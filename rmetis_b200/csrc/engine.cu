@@ -1,0 +1,344 @@
+// Host orchestration of the multilevel k-way pipeline
+// (src/partition/kway.rs:20-162 and src/coarsen/mod.rs:36-71).
+#include <cmath>
+#include <cstring>
+#include <random>
+
+#include "engine.h"
+#include "hostrng.h"
+#include "prof.h"
+
+namespace rmb {
+
+// ---------------------------------------------------------------------------
+// Profiler
+// ---------------------------------------------------------------------------
+Profiler& profiler() {
+  static Profiler p;
+  return p;
+}
+
+long long& launch_counter() {
+  static long long c = 0;
+  return c;
+}
+
+cudaEvent_t Profiler::get() {
+  if (!pool_.empty()) {
+    cudaEvent_t e = pool_.back();
+    pool_.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  RMB_CUDA(cudaEventCreate(&e));
+  return e;
+}
+
+int Profiler::begin(int id, cudaStream_t st) {
+  if (!on) return -1;
+  Rec r{id, get(), get(), 0.0};
+  RMB_CUDA(cudaEventRecord(r.a, st));
+  recs_.push_back(r);
+  return (int)recs_.size() - 1;
+}
+
+void Profiler::end(int h, cudaStream_t st, double bytes) {
+  if (h < 0) return;
+  recs_[h].bytes = bytes;
+  RMB_CUDA(cudaEventRecord(recs_[h].b, st));
+}
+
+void Profiler::collect() {
+  for (auto& r : recs_) {
+    RMB_CUDA(cudaEventSynchronize(r.b));
+    float ms = 0.f;
+    RMB_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+    totals.launches[r.id] += 1;
+    totals.ms[r.id] += ms;
+    totals.bytes[r.id] += r.bytes;
+    pool_.push_back(r.a);
+    pool_.push_back(r.b);
+  }
+  recs_.clear();
+}
+
+void Profiler::reset() {
+  collect();
+  totals = ProfTotals{};
+}
+
+// ---------------------------------------------------------------------------
+// Thresholds
+// ---------------------------------------------------------------------------
+void threshold_values(double t, double ub, long long* feas, long long* over, long long* grow) {
+  const double lim = 9.0e18;
+  const double x = t * ub;
+  if (std::isnan(x)) {
+    *feas = LLONG_MIN;
+    *over = LLONG_MAX;
+  } else if (x >= lim) {
+    *feas = LLONG_MAX;
+    *over = LLONG_MAX;
+  } else if (x <= -lim) {
+    *feas = LLONG_MIN;
+    *over = LLONG_MIN;
+  } else {
+    const long long f = (long long)std::floor(x);
+    *feas = f;
+    *over = f;
+  }
+  if (std::isnan(t) || t >= lim) *grow = LLONG_MAX;
+  else if (t <= -lim) *grow = LLONG_MIN;
+  else *grow = (long long)std::ceil(t);
+}
+
+// ---------------------------------------------------------------------------
+// Engine
+// ---------------------------------------------------------------------------
+Engine::Engine() {
+  RMB_CUDA(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
+  stream_ = own_stream_;
+  RMB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_scratch_), 4096));
+}
+
+Engine::~Engine() {
+  // Process teardown may already have unloaded the driver; ignore errors.
+  arena_.release();
+  if (h_thr_) cudaFreeHost(h_thr_);
+  if (h_scratch_) cudaFreeHost(h_scratch_);
+  if (own_stream_) cudaStreamDestroy(own_stream_);
+}
+
+void Engine::reset_stats() { profiler().reset(); }
+
+void Engine::thresholds(const std::vector<int32_t>& total, int k, int ncon, const float* tpwgts,
+                        const std::vector<double>& ub, long long* d_feas, long long* d_over, long long* d_grow) {
+  const size_t K = (size_t)k * ncon;
+  if (h_thr_cap_ < 3 * K) {
+    if (h_thr_) {
+      RMB_CUDA(cudaStreamSynchronize(stream_));
+      cudaFreeHost(h_thr_);
+    }
+    RMB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_thr_), sizeof(long long) * 3 * K));
+    h_thr_cap_ = 3 * K;
+  }
+  // The staging buffer may still feed an earlier copy.
+  RMB_CUDA(cudaStreamSynchronize(stream_));
+  for (int p = 0; p < k; ++p)
+    for (int c = 0; c < ncon; ++c) {
+      // compute_target_weights (src/graph/mod.rs:392-410), f64
+      const double f = tpwgts ? (double)tpwgts[(size_t)p * ncon + c] : 1.0 / (double)k;
+      const double t = f * (double)total[c];
+      const size_t i = (size_t)p * ncon + c;
+      threshold_values(t, ub[c], &h_thr_[i], &h_thr_[K + i], &h_thr_[2 * K + i]);
+    }
+  RMB_CUDA(cudaMemcpyAsync(d_feas, h_thr_, sizeof(long long) * K, cudaMemcpyHostToDevice, stream_));
+  RMB_CUDA(cudaMemcpyAsync(d_over, h_thr_ + K, sizeof(long long) * K, cudaMemcpyHostToDevice, stream_));
+  RMB_CUDA(cudaMemcpyAsync(d_grow, h_thr_ + 2 * K, sizeof(long long) * K, cudaMemcpyHostToDevice, stream_));
+}
+
+__global__ void k_random_part(int32_t n, int32_t k, uint64_t seed, idx_t* part) {
+  RMB_GRID_STRIDE(v, n) { part[v] = (idx_t)(mix64(seed ^ (uint64_t)v * 0x9e3779b97f4a7c15ULL) % (uint64_t)k); }
+}
+
+int Engine::partition_kway(const DGraph& g0, int nparts, const float* tpwgts, const float* ubvec,
+                           const KwayOptions& o, idx_t* part_out, int32_t* objval, KwayTrace* trace) {
+  cudaStream_t st = stream_;
+  const int k = nparts;
+  const int ncon = g0.ncon;
+  if (k < 2 || k > g0.n) throw Error(-2, "nparts out of range");   // kway.rs:31-38
+  if (ncon > 8) throw Error(-2, "ncon above the supported maximum of 8");
+  std::vector<double> ub(ncon);                                     // kway.rs:44-49
+  for (int c = 0; c < ncon; ++c) ub[c] = ubvec ? (double)ubvec[c] : 1.0 + (double)o.ufactor / 1000.0;
+
+  Arena::Mark call_mark = arena_.mark();
+  const size_t K = (size_t)k * ncon;
+  long long* d_feas = arena_.alloc<long long>(K);
+  long long* d_over = arena_.alloc<long long>(K);
+  long long* d_grow = arena_.alloc<long long>(K);
+  long long* d_tot = arena_.alloc<long long>((size_t)ncon);
+  unsigned long long* d_cut = arena_.alloc<unsigned long long>(1);
+
+  // Total weight of the input (i32 with wrap-around, like the reference).
+  std::vector<int32_t> total0(ncon, g0.n);
+  if (g0.vwgt) {
+    total_weight(g0, d_tot, st);
+    RMB_CUDA(cudaMemcpyAsync(h_scratch_ + 16, d_tot, sizeof(long long) * ncon, cudaMemcpyDeviceToHost, st));
+    RMB_CUDA(cudaStreamSynchronize(st));
+    for (int c = 0; c < ncon; ++c) {
+      long long t;
+      std::memcpy(&t, reinterpret_cast<char*>(h_scratch_ + 16) + sizeof(long long) * c, sizeof(long long));
+      total0[c] = (int32_t)(uint32_t)(unsigned long long)t;
+    }
+  }
+
+  const size_t limit = std::max<size_t>((size_t)20 * k, 20);         // coarsen/mod.rs:43
+  bool have_best = false;
+  int32_t best_obj = 0;
+  std::random_device rd;
+
+  for (int attempt = 0; attempt < o.ncuts; ++attempt) {              // kway.rs:54
+    Arena::Mark att_mark = arena_.mark();
+    uint64_t seed64;
+    if (o.seed == 0) seed64 = ((uint64_t)rd() << 32) ^ (uint64_t)rd();
+    else seed64 = o.seed + (uint64_t)attempt;
+    KwayTrace local;
+
+    // ---- coarsening (coarsen/mod.rs:36-71) ----
+    std::vector<DGraph> levels{g0};
+    std::vector<idx_t*> cmaps;
+    std::vector<idx_t*> heavy_lists;
+    std::vector<int32_t> heavy_counts;
+    std::vector<bool> has_vw{g0.vwgt != nullptr};
+    for (int lvl = 0;; ++lvl) {
+      const DGraph& cur = levels.back();
+      idx_t* hl = arena_.alloc<idx_t>((size_t)cur.n);
+      const int32_t nh = heavy_list(cur, hl, arena_, st, h_scratch_);
+      heavy_lists.push_back(hl);
+      heavy_counts.push_back(nh);
+      Arena::Mark mm = arena_.mark();
+      idx_t* match = arena_.alloc<idx_t>((size_t)cur.n);
+      const uint64_t lseed = mix64(seed64 * 0x100000001b3ULL + (uint64_t)lvl + 1);
+      match_parallel(cur, o.ctype == 0 ? 0 : 1, lseed, o.match_rounds, match, hl, nh, arena_, st, h_scratch_);
+      if (trace) {
+        std::vector<int32_t> hm(cur.n);
+        RMB_CUDA(cudaMemcpyAsync(hm.data(), match, sizeof(int32_t) * cur.n, cudaMemcpyDeviceToHost, st));
+        RMB_CUDA(cudaStreamSynchronize(st));
+        local.matchings.push_back(std::move(hm));
+      }
+      // Coarse vertex weights: the reference gives a coarse graph vwgt only
+      // when the fine graph has it (graph/mod.rs:300).
+      const bool coarse_vw = has_vw.back() || o.summed_unit_weights;
+      CoarseResult cr = contract(cur, match, coarse_vw ? 1 : 0, arena_, st, h_scratch_);
+      // The matching is scratch once contracted; keep the coarse level.
+      (void)mm;
+      const float ratio = (float)cr.g.n / (float)cur.n;
+      if ((size_t)cr.g.n < (size_t)k) {
+        // A coarsest graph with fewer vertices than parts cannot seed k parts
+        // (the reference's seed draw would never end); keep the finer level.
+        break;
+      }
+      levels.push_back(cr.g);
+      cmaps.push_back(cr.cmap);
+      has_vw.push_back(coarse_vw);
+      if ((size_t)cr.g.n <= limit || ratio > 0.95f) break;
+    }
+    const int L = (int)levels.size() - 1;  // number of coarse levels
+    // heavy list of the coarsest level (the loop computed lists for 0..L-1)
+    if ((int)heavy_lists.size() < (int)levels.size()) {
+      idx_t* hl = arena_.alloc<idx_t>((size_t)levels.back().n);
+      heavy_counts.push_back(heavy_list(levels.back(), hl, arena_, st, h_scratch_));
+      heavy_lists.push_back(hl);
+    }
+    if (trace) {
+      for (auto& lv : levels) {
+        local.level_n.push_back(lv.n);
+        local.level_m.push_back(lv.m);
+      }
+    }
+
+    auto level_total = [&](int l) {
+      if (has_vw[l]) return total0;
+      if (!g0.vwgt && o.summed_unit_weights) return std::vector<int32_t>(ncon, g0.n);
+      return std::vector<int32_t>(ncon, levels[l].n);
+    };
+
+    // ---- initial partition of the coarsest graph (initial/mod.rs:11-22) ----
+    const DGraph& cg = levels.back();
+    idx_t* part = arena_.alloc<idx_t>((size_t)cg.n);
+    thresholds(level_total(L), k, ncon, tpwgts, ub, d_feas, d_over, d_grow);
+    if (o.iptype == 1) {
+      k_random_part<<<grid_for(cg.n, 256), 256, 0, st>>>(cg.n, k, mix64(seed64 ^ 0x52414e44ULL), part);
+      RMB_LAUNCH_CHECK();
+    } else {
+      const int T = std::max(1, o.grow_trials);
+      std::vector<int32_t> seeds((size_t)T * k);
+      std::vector<char> used(cg.n);
+      for (int t = 0; t < T; ++t) {
+        HostRng rng(mix64(seed64 ^ (0x9E3779B97F4A7C15ULL * (uint64_t)(t + 1))));
+        std::fill(used.begin(), used.end(), 0);
+        for (int p = 0; p < k;) {                                     // grow.rs:26-32
+          const int32_t v = (int32_t)rng.below((uint64_t)cg.n);
+          if (!used[v]) {
+            used[v] = 1;
+            seeds[(size_t)t * k + p] = v;
+            ++p;
+          }
+        }
+      }
+      Arena::Mark gm = arena_.mark();
+      idx_t* d_seeds = arena_.alloc<idx_t>(seeds.size());
+      idx_t* d_parts = arena_.alloc<idx_t>((size_t)T * cg.n);
+      long long* d_cuts = arena_.alloc<long long>((size_t)T);
+      RMB_CUDA(cudaMemcpyAsync(d_seeds, seeds.data(), sizeof(int32_t) * seeds.size(), cudaMemcpyHostToDevice, st));
+      grow_trials(cg, k, T, d_seeds, d_grow, d_parts, d_cuts, arena_, st);
+      std::vector<long long> cuts(T);
+      RMB_CUDA(cudaMemcpyAsync(cuts.data(), d_cuts, sizeof(long long) * T, cudaMemcpyDeviceToHost, st));
+      RMB_CUDA(cudaStreamSynchronize(st));
+      int bt = 0;
+      for (int t = 1; t < T; ++t)
+        if (cuts[t] < cuts[bt]) bt = t;
+      RMB_CUDA(cudaMemcpyAsync(part, d_parts + (size_t)bt * cg.n, sizeof(idx_t) * cg.n, cudaMemcpyDeviceToDevice,
+                               st));
+      if (trace) local.grow_seeds.assign(seeds.begin() + (size_t)bt * k, seeds.begin() + (size_t)(bt + 1) * k);
+      (void)gm;
+    }
+
+    // ---- refinement at the coarsest level and on the way up (kway.rs:72-92) ----
+    RefineParams rp;
+    rp.k = k;
+    rp.niter = o.niter;
+    rp.feas_max = d_feas;
+    rp.over_thr = d_over;
+    {
+      RefineStats rs = greedy_refine(cg, part, rp, heavy_lists[L], heavy_counts[L], arena_, st, h_scratch_);
+      local.refine_passes += rs.passes;
+      local.refine_moves += rs.moves;
+      local.decide_rounds += rs.decide_iters;
+    }
+    for (int i = L - 1; i >= 0; --i) {
+      const DGraph& fg = levels[i];
+      idx_t* fpart = arena_.alloc<idx_t>((size_t)fg.n);
+      project(fg.n, cmaps[i], part, fpart, st);
+      part = fpart;
+      thresholds(level_total(i), k, ncon, tpwgts, ub, d_feas, d_over, d_grow);
+      RefineStats rs = greedy_refine(fg, part, rp, heavy_lists[i], heavy_counts[i], arena_, st, h_scratch_);
+      local.refine_passes += rs.passes;
+      local.refine_moves += rs.moves;
+      local.decide_rounds += rs.decide_iters;
+    }
+
+    // ---- objective (kway.rs:94-98) ----
+    cut_and_weights(g0, part, k, d_cut, nullptr, st);
+    unsigned long long cut_raw = 0;
+    RMB_CUDA(cudaMemcpyAsync(h_scratch_ + 32, d_cut, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    RMB_CUDA(cudaStreamSynchronize(st));
+    std::memcpy(&cut_raw, h_scratch_ + 32, sizeof(cut_raw));
+    const int32_t obj = (int32_t)(uint32_t)cut_raw / 2;
+    if (!have_best || obj < best_obj) {
+      best_obj = obj;
+      have_best = true;
+      RMB_CUDA(cudaMemcpyAsync(part_out, part, sizeof(idx_t) * g0.n, cudaMemcpyDeviceToDevice, st));
+      if (trace) *trace = std::move(local);
+    }
+    RMB_CUDA(cudaStreamSynchronize(st));
+    arena_.reset_to(att_mark);
+  }
+  arena_.reset_to(call_mark);
+  if (objval) *objval = best_obj;
+  if (profiler().on) profiler().collect();
+  return 1;
+}
+
+Engine& engine_for_current_device() {
+  static std::mutex m;
+  static std::vector<Engine*> engines;
+  int dev = 0;
+  RMB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(m);
+  if ((int)engines.size() <= dev) engines.resize(dev + 1, nullptr);
+  if (!engines[dev]) engines[dev] = new Engine();  // lives until process exit
+  return *engines[dev];
+}
+
+}  // namespace rmb

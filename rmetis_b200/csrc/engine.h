@@ -1,0 +1,94 @@
+// Host orchestration of the multilevel k-way pipeline on one GPU.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <vector>
+
+#include "arena.h"
+#include "kernels.h"
+
+namespace rmb {
+
+// Decoded options of the reference (src/types.rs:52-95, from_raw :190-224)
+// plus engine knobs that have no slot in the METIS option array.
+struct KwayOptions {
+  int ctype = 1;    // 0 = Rm, 1 = Shem
+  int iptype = 0;   // 0 = Grow, 1 = Random, 4 = MetisRb (grown like Grow)
+  int rtype = 0;    // 0 = Fm, 1 = Greedy
+  int niter = 10;
+  int ncuts = 1;
+  uint64_t seed = 0;
+  uint32_t ufactor = 30;
+  // engine knobs
+  int grow_trials = 8;       // grown partitions per attempt; the lowest cut is kept
+  int match_rounds = 16;     // proposal rounds per coarsening level (upper bound)
+  int summed_unit_weights = 0;  // 1: a graph without vwgt gets summed coarse weights
+};
+
+// Per-kernel-family device time, measured with CUDA events on the engine's
+// stream when profiling is on.
+struct KernelStat {
+  int64_t launches = 0;
+  double ms = 0.0;
+  double bytes = 0.0;  // algorithmic bytes (counted per launch from sizes)
+};
+enum StatId { kStatMatch = 0, kStatContract, kStatGrow, kStatRefine, kStatProject, kStatCut, kStatCount };
+
+// Optional record of the random choices of the kept attempt, so that a
+// checker can replay them.
+struct KwayTrace {
+  std::vector<std::vector<int32_t>> matchings;
+  std::vector<int32_t> grow_seeds;
+  std::vector<int64_t> level_n, level_m;
+  int64_t refine_passes = 0, refine_moves = 0, decide_rounds = 0;
+};
+
+class Engine {
+ public:
+  Engine();
+  ~Engine();
+
+  // The whole k-way partition of a device-resident graph. part_out is a
+  // device array of g.n entries. tpwgts/ubvec are host arrays (or null).
+  // Returns 1 (METIS_OK) or throws rmb::Error.
+  int partition_kway(const DGraph& g, int nparts, const float* tpwgts, const float* ubvec, const KwayOptions& o,
+                     idx_t* part_out, int32_t* objval, KwayTrace* trace);
+
+  void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
+  cudaStream_t stream() const { return stream_; }
+  Arena& arena() { return arena_; }
+  int32_t* host_scratch() { return h_scratch_; }
+
+  void set_profiling(bool on) { profiling_ = on; }
+  void reset_stats();
+  const KernelStat* stats() const { return stats_; }
+
+  std::mutex mu;
+
+ private:
+  void thresholds(const std::vector<int32_t>& total, int k, int ncon, const float* tpwgts,
+                  const std::vector<double>& ub, long long* d_feas, long long* d_over, long long* d_grow);
+
+  struct Timer;
+  Arena arena_;
+  cudaStream_t own_stream_ = nullptr;
+  cudaStream_t stream_ = nullptr;
+  int32_t* h_scratch_ = nullptr;   // pinned
+  long long* h_thr_ = nullptr;     // pinned staging for thresholds
+  size_t h_thr_cap_ = 0;
+  bool profiling_ = false;
+  KernelStat stats_[kStatCount];
+};
+
+// One engine per device, created on first use.
+Engine& engine_for_current_device();
+
+// Host-side threshold form of the reference's f64 tests:
+//   feasible   (pw + vw) as f64 <= t * ub   <=>  pw + vw <= feas
+//   overweight  pw as f64 > t * ub          <=>  pw > over
+//   at target   pw as f64 >= t              <=>  pw >= grow
+void threshold_values(double t, double ub, long long* feas, long long* over, long long* grow);
+
+}  // namespace rmb

@@ -1,0 +1,126 @@
+// Launchers for the sm_100a kernels of the k-way hot path. Each launcher
+// names the reference function it replaces.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "arena.h"
+#include "common.cuh"
+
+namespace rmb {
+
+// Device view of one CSR level. adjwgt == nullptr means unit edge weights,
+// vwgt == nullptr means unit vertex weights (the reference's `None`).
+struct DGraph {
+  int32_t n = 0;
+  int64_t m = 0;
+  int32_t ncon = 1;
+  const idx_t* xadj = nullptr;
+  const idx_t* adjncy = nullptr;
+  const idx_t* adjwgt = nullptr;
+  const idx_t* vwgt = nullptr;
+};
+
+// Vertices whose degree exceeds this go to the warp-per-vertex paths.
+constexpr int kHeavyDegree = 64;
+// Coarse vertices whose merged row bound exceeds this use the warp merge.
+constexpr int kContractThreadMax = 16;
+// Movers per block in the refinement decision kernel.
+constexpr int kDecideBlock = 256;
+
+// ---- graph_kernels.cu ----------------------------------------------------
+// Validation of a device CSR (src/graph/validate.rs:16-142). Returns a bit
+// mask of failed checks (0 = valid). Requires xadj[0]==0 and xadj[n]==m,
+// checked by the caller on the host.
+int validate_device(const DGraph& g, Arena& arena, cudaStream_t st, int32_t* h_scratch);
+
+// edge_cut (src/graph/mod.rs:123-137) and partition_weights (:140-149) in one
+// pass. Results stay on the device: cut_acc (u64, sum of cross weights taken
+// mod 2^32 later), pw (i64 [k][ncon]). Both are zeroed here.
+void cut_and_weights(const DGraph& g, const idx_t* part, int k, unsigned long long* cut_acc,
+                     long long* pw, cudaStream_t st);
+void partition_weights_only(const DGraph& g, const idx_t* part, int k, long long* pw, cudaStream_t st);
+
+// total_weight (src/graph/mod.rs:152-160): i64 sums per constraint (zeroed here).
+void total_weight(const DGraph& g, long long* tot, cudaStream_t st);
+
+// Projection fine[v] = coarse[cmap[v]] (src/partition/kway.rs:81-84).
+void project(int32_t n_fine, const idx_t* cmap, const idx_t* coarse_part, idx_t* fine_part,
+             cudaStream_t st);
+
+// boundary flags (src/graph/mod.rs:164-171): flag[v] = 1 if v has a
+// neighbour in another part.
+void boundary_flags(const DGraph& g, const idx_t* part, idx_t* flag, cudaStream_t st);
+
+// Compact the ids v with flag[v] != 0 into out (ascending). count_dev gets
+// the number written.
+void compact_flags(const idx_t* flag, int32_t n, idx_t* out, idx_t* count_dev, Arena& arena,
+                   cudaStream_t st);
+
+// ---- coarsen.cu ----------------------------------------------------------
+// Parallel matching (replaces shem_matching src/coarsen/shem.rs:13-56 and
+// random_matching src/coarsen/rm.rs:13-43). mode 1 = heavy edge first
+// (SHEM), 0 = random (RM). match[v] is an involution, self = unmatched.
+// heavy/nheavy: precomputed list of vertices with degree > kHeavyDegree.
+void match_parallel(const DGraph& g, int mode, uint64_t seed, int rounds, idx_t* match,
+                    const idx_t* heavy, int32_t nheavy, Arena& arena, cudaStream_t st,
+                    int32_t* h_scratch);
+
+struct CoarseResult {
+  DGraph g;
+  idx_t* cmap = nullptr;
+  idx_t* xadj = nullptr;
+  idx_t* adjncy = nullptr;
+  idx_t* adjwgt = nullptr;
+  idx_t* vwgt = nullptr;
+};
+
+// build_coarse_graph (src/graph/mod.rs:284-384): cmap numbering by ascending
+// leader, merged rows in first-appearance order with summed weights.
+// coarse_vwgt: 0 = coarse graph has no vwgt (reference rule when the fine
+// graph has none), 1 = sum (materialising 1 for a unit fine graph).
+CoarseResult contract(const DGraph& g, const idx_t* match, int coarse_vwgt, Arena& arena,
+                      cudaStream_t st, int32_t* h_scratch);
+
+// Degree > kHeavyDegree vertex list of a level (ascending ids).
+int32_t heavy_list(const DGraph& g, idx_t* out, Arena& arena, cudaStream_t st, int32_t* h_scratch);
+
+// ---- initial.cu ----------------------------------------------------------
+// grow_partition (src/initial/grow.rs:12-103), exact given the seed vertices:
+// one warp per trial. seeds: [ntrials][k]; grow_tgt: [k][ncon] integer form of
+// the `pw as f64 >= t` test (pw >= grow_tgt). parts: [ntrials][n]. cuts:
+// [ntrials] edge cut of each grown partition.
+void grow_trials(const DGraph& g, int k, int ntrials, const idx_t* seeds, const long long* grow_tgt,
+                 idx_t* parts, long long* cuts, Arena& arena, cudaStream_t st);
+
+// ---- refine.cu -----------------------------------------------------------
+struct RefineParams {
+  int k = 2;
+  int niter = 10;
+  const long long* feas_max = nullptr;  // [k][ncon]: feasible iff pw + vw <= feas_max
+  const long long* over_thr = nullptr;  // [k][ncon]: overweight iff pw > over_thr
+};
+
+struct RefineStats {
+  int passes = 0;
+  int64_t moves = 0;
+  int decide_iters = 0;
+  int64_t movers = 0;
+};
+
+// greedy_refine_with_comm with one rank (src/refine/greedy.rs:36-193):
+// balance-repair pass, then up to niter positive-gain passes, every pass
+// bit-identical to the sequential reference pass. part is updated in place.
+RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, const idx_t* heavy,
+                          int32_t nheavy, Arena& arena, cudaStream_t st, int32_t* h_scratch);
+
+// Gain table of one pass (boundary_vertices + compute_move_gain,
+// src/graph/mod.rs:164-171, src/refine/greedy.rs:197-218): per vertex the
+// boundary flag, w_from and the explicit candidate list sorted by
+// (gain desc, part asc), stored at cand[xadj[v] ..].
+void gain_table(const DGraph& g, const idx_t* part, int k, idx_t* boundary, idx_t* ncand,
+                idx_t* wfrom, idx_t* cand_p, idx_t* cand_g, const idx_t* heavy, int32_t nheavy,
+                cudaStream_t st);
+
+}  // namespace rmb

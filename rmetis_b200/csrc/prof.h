@@ -1,0 +1,51 @@
+// Per-launch device timing with CUDA events (off unless enabled). Used by the
+// benchmark to measure the dominant kernel's average launch duration on the
+// stream it runs on.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+namespace rmb {
+
+enum ProfId {
+  kProfGain = 0,      // k_gain: gain table of one refinement pass
+  kProfDecide,        // k_decide / k_decide_seq
+  kProfPropose,       // k_match_propose
+  kProfContract,      // k_contract_thread
+  kProfCut,           // k_cut
+  kProfGrow,          // k_grow
+  kProfCount
+};
+
+struct ProfTotals {
+  long long launches[kProfCount];
+  double ms[kProfCount];
+  double bytes[kProfCount];
+};
+
+class Profiler {
+ public:
+  bool on = false;
+  int begin(int id, cudaStream_t st);
+  void end(int handle, cudaStream_t st, double bytes);
+  // Synchronises on the recorded events and adds them to the totals.
+  void collect();
+  void reset();
+  ProfTotals totals{};
+
+ private:
+  struct Rec {
+    int id;
+    cudaEvent_t a, b;
+    double bytes;
+  };
+  std::vector<Rec> recs_;
+  std::vector<cudaEvent_t> pool_;
+  cudaEvent_t get();
+};
+
+Profiler& profiler();
+
+}  // namespace rmb

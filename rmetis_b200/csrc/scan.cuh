@@ -1,0 +1,162 @@
+// Device-wide exclusive prefix sums (reduce-then-scan, three launches, no
+// inter-block waiting). Used for cmap numbering, coarse CSR offsets and mover
+// compaction.
+#pragma once
+
+#include "arena.h"
+#include "common.cuh"
+
+namespace rmb {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+template <typename T>
+__device__ inline T block_exclusive_scan(T v, T* smem_warp, T* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  T x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) smem_warp[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    T w = lane < nw ? smem_warp[lane] : T(0);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      T y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < nw) smem_warp[lane] = w;  // inclusive per warp
+  }
+  __syncthreads();
+  T warp_prefix = wid > 0 ? smem_warp[wid - 1] : T(0);
+  if (total) *total = smem_warp[(blockDim.x >> 5) - 1];
+  T r = warp_prefix + x - v;
+  __syncthreads();
+  return r;
+}
+
+// Phase 1: sum of each tile.
+template <typename T, typename Load>
+__global__ void k_tile_reduce(Load load, int64_t n, T* tile_sums) {
+  __shared__ T sw[32];
+  int64_t base = (int64_t)blockIdx.x * kScanTile;
+  T s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    int64_t j = base + (int64_t)i * kScanThreads + threadIdx.x;
+    if (j < n) s += load(j);
+  }
+  T tot;
+  block_exclusive_scan<T>(s, sw, &tot);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+// Phase 2: exclusive scan of tile sums in one block; writes the grand total.
+template <typename T>
+__global__ void k_scan_tile_sums(T* tile_sums, int64_t ntiles, T* total_out) {
+  __shared__ T sw[32];
+  T carry = 0;
+  for (int64_t base = 0; base < ntiles; base += (int64_t)blockDim.x * kScanItems) {
+    T vals[kScanItems];
+    T s = 0;
+    int64_t my = base + (int64_t)threadIdx.x * kScanItems;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+      vals[i] = (my + i < ntiles) ? tile_sums[my + i] : T(0);
+      s += vals[i];
+    }
+    T tot;
+    T ex = block_exclusive_scan<T>(s, sw, &tot);
+    T run = carry + ex;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+      if (my + i < ntiles) tile_sums[my + i] = run;
+      run += vals[i];
+    }
+    carry += tot;
+  }
+  if (threadIdx.x == 0 && total_out) *total_out = carry;
+}
+
+// Phase 3: per-tile exclusive scan plus the tile offset; out[n] gets the total
+// when `write_end` (so out can serve as a CSR offset array of length n+1).
+template <typename T, typename Load, typename Store>
+__global__ void k_tile_scan(Load load, Store store, int64_t n, const T* tile_offsets) {
+  __shared__ T sw[32];
+  __shared__ T tile[kScanTile];
+  int64_t base = (int64_t)blockIdx.x * kScanTile;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    int64_t j = base + (int64_t)i * kScanThreads + threadIdx.x;
+    tile[i * kScanThreads + threadIdx.x] = (j < n) ? load(j) : T(0);
+  }
+  __syncthreads();
+  T vals[kScanItems];
+  T s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    vals[i] = tile[threadIdx.x * kScanItems + i];
+    s += vals[i];
+  }
+  T ex = block_exclusive_scan<T>(s, sw, nullptr);
+  T run = ex + tile_offsets[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    tile[threadIdx.x * kScanItems + i] = run;
+    run += vals[i];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    int64_t j = base + (int64_t)i * kScanThreads + threadIdx.x;
+    if (j < n) store(j, tile[i * kScanThreads + threadIdx.x]);
+  }
+}
+
+template <typename T>
+struct LoadArr {
+  const T* p;
+  __device__ T operator()(int64_t i) const { return p[i]; }
+};
+template <typename T>
+struct StoreArr {
+  T* p;
+  __device__ void operator()(int64_t i, T v) const { p[i] = v; }
+};
+
+// Exclusive scan of `load(0..n-1)` into `store`; the total is written to
+// device memory at `total_dev` (may be null). Scratch comes from the arena and
+// is released on return.
+template <typename T, typename Load, typename Store>
+void exclusive_scan(Load load, Store store, int64_t n, T* total_dev, Arena& arena, cudaStream_t st) {
+  Arena::Mark mk = arena.mark();
+  int64_t ntiles = ceil_div(n, kScanTile);
+  if (ntiles < 1) ntiles = 1;
+  T* sums = arena.alloc<T>((size_t)ntiles);
+  if (n > 0) {
+    k_tile_reduce<T, Load><<<(unsigned)ntiles, kScanThreads, 0, st>>>(load, n, sums);
+    RMB_LAUNCH_CHECK();
+  } else {
+    RMB_CUDA(cudaMemsetAsync(sums, 0, sizeof(T), st));
+  }
+  k_scan_tile_sums<T><<<1, 1024, 0, st>>>(sums, ntiles, total_dev);
+  RMB_LAUNCH_CHECK();
+  if (n > 0) {
+    k_tile_scan<T, Load, Store><<<(unsigned)ntiles, kScanThreads, 0, st>>>(load, store, n, sums);
+    RMB_LAUNCH_CHECK();
+  }
+  arena.reset_to(mk);
+}
+
+template <typename T>
+void exclusive_scan_arr(const T* in, T* out, int64_t n, T* total_dev, Arena& arena, cudaStream_t st) {
+  exclusive_scan<T>(LoadArr<T>{in}, StoreArr<T>{out}, n, total_dev, arena, st);
+}
+
+}  // namespace rmb
