@@ -32,8 +32,8 @@ KwayOptions parse_options(const idx_t* a) {
 }
 
 struct Tuning {
-  int grow_trials = 8;
-  int match_rounds = 16;
+  int grow_trials = 32;
+  int match_rounds = 24;
   int summed_unit_weights = 0;
 };
 Tuning& tuning() {

@@ -8,13 +8,21 @@ namespace rmb {
 // ---------------------------------------------------------------------------
 // Matching
 //
-// The reference visits vertices one at a time (shem.rs:13-56, rm.rs:13-43).
-// Here every unmatched vertex points at its best unmatched neighbour under a
-// global strict order on edges; mutual pointers match. The order is
-// (edge weight, seeded hash of the edge, endpoint ids) for SHEM and (hash,
-// ids) for RM. An edge that is the best for both endpoints always exists, so
-// every round matches at least one pair; this is the conflict-free form of
-// the reference's distributed proposal exchange (coarsen/mod.rs:75-143).
+// The reference visits vertices one at a time, light (low degree) first, and
+// each takes its heaviest still-free neighbour (shem.rs:13-56; rm.rs:13-43
+// takes the first free neighbour in random order). The parallel form keeps
+// both ingredients:
+//   handshake rounds: every free vertex proposes to its best free neighbour
+//     (heaviest edge, ties by a seeded edge hash; RM: the hash alone); a pair
+//     that proposed to each other matches; otherwise a vertex that received
+//     no proposal ("pure" proposer) competes for its target, and the target
+//     takes the competitor that comes first in the reference's visit order
+//     (lowest degree, then a seeded vertex hash);
+//   finishing rounds: mutual proposals under the edge hash alone, a strict
+//     total order, so each round matches at least one pair.
+// Choosing partners by heaviest edge alone (locally dominant edges) lets
+// large coarse vertices absorb each other level after level, which leaves
+// star-like graphs that stop coarsening; the visit-order competition avoids it.
 // ---------------------------------------------------------------------------
 __device__ inline uint32_t edge_hash(uint64_t seed, int32_t a, int32_t b) {
   int32_t lo = a < b ? a : b, hi = a < b ? b : a;
@@ -87,6 +95,58 @@ __global__ void k_match_init(int32_t n, idx_t* match) {
   RMB_GRID_STRIDE(v, n) { match[v] = -1; }
 }
 
+// Marks every vertex that received a proposal this round (stamp = round + 1).
+__global__ void k_match_stamp(int32_t n, const idx_t* __restrict__ match, const idx_t* __restrict__ prop,
+                              int32_t* __restrict__ stamp, int32_t round) {
+  RMB_GRID_STRIDE(v, n) {
+    if (match[v] < 0) {
+      const int32_t t = prop[v];
+      if (t >= 0) stamp[t] = round + 1;
+    }
+  }
+}
+
+// Pure proposers compete for their target with their visit-order key.
+__global__ void k_match_compete(const idx_t* __restrict__ xadj, int32_t n, const idx_t* __restrict__ match,
+                                const idx_t* __restrict__ prop, const int32_t* __restrict__ stamp, int32_t round,
+                                unsigned long long* __restrict__ best, uint64_t vseed, int use_degree) {
+  RMB_GRID_STRIDE(v, n) {
+    if (match[v] >= 0) continue;
+    const int32_t t = prop[v];
+    if (t < 0 || stamp[v] == round + 1 || prop[t] == (int32_t)v) continue;
+    const uint32_t deg = (uint32_t)min(xadj[v + 1] - xadj[v], 0x7FFF);
+    const uint32_t h = (uint32_t)(mix64(vseed ^ (uint64_t)v) >> 48);
+    const uint32_t pri = use_degree ? (((0x7FFFu - deg) << 16) | h) : h;
+    const unsigned long long key = (1ULL << 63) | ((unsigned long long)pri << 32) | (uint32_t)v;
+    atomicMax(&best[t], key);
+  }
+}
+
+// Mutual pairs match; a target that is not in a mutual pair takes its winning
+// competitor. Only the target writes the pair, the winner (a pure proposer)
+// writes nothing this round.
+__global__ void k_match_resolve(int32_t n, const idx_t* __restrict__ prop, idx_t* __restrict__ match,
+                                unsigned long long* __restrict__ best, int32_t* __restrict__ newly) {
+  int32_t cnt = 0;
+  RMB_GRID_STRIDE(u, n) {
+    if (match[u] >= 0) continue;
+    const int32_t t = prop[u];
+    const unsigned long long b = best[u];
+    if (b) best[u] = 0;
+    if (t >= 0 && prop[t] == (int32_t)u) {
+      match[u] = t;
+      ++cnt;
+    } else if (b) {
+      const int32_t v = (int32_t)(uint32_t)(b & 0xffffffffULL);
+      match[u] = v;
+      match[v] = (idx_t)u;
+      cnt += 2;
+    }
+  }
+  cnt = warp_sum(cnt);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(newly, cnt);
+}
+
 __global__ void k_match_accept(int32_t n, const idx_t* __restrict__ prop, idx_t* __restrict__ match,
                                int32_t* __restrict__ newly) {
   int32_t cnt = 0;
@@ -113,13 +173,21 @@ void match_parallel(const DGraph& g, int mode, uint64_t seed, int rounds, idx_t*
                     int32_t nheavy, Arena& arena, cudaStream_t st, int32_t* h_scratch) {
   Arena::Mark mk = arena.mark();
   idx_t* prop = arena.alloc<idx_t>((size_t)g.n);
+  int32_t* stamp = arena.alloc<int32_t>((size_t)g.n);
+  unsigned long long* best = arena.alloc<unsigned long long>((size_t)g.n);
   int32_t* newly = arena.alloc<int32_t>((size_t)rounds + 1);
   RMB_CUDA(cudaMemsetAsync(newly, 0, sizeof(int32_t) * ((size_t)rounds + 1), st));
+  RMB_CUDA(cudaMemsetAsync(stamp, 0, sizeof(int32_t) * (size_t)g.n, st));
+  RMB_CUDA(cudaMemsetAsync(best, 0, sizeof(unsigned long long) * (size_t)g.n, st));
   const int blocks = grid_for(g.n, 256);
   k_match_init<<<blocks, 256, 0, st>>>(g.n, match);
   RMB_LAUNCH_CHECK();
   const bool w = g.adjwgt != nullptr;
+  const uint64_t vseed = mix64(seed ^ 0x7669736974ULL);
+  bool handshake = true;  // first phase; the finishing phase follows when it stalls
+  int phase_start = 0;
   for (int r = 0; r < rounds; ++r) {
+    const bool by_weight = handshake && mode == 1;
     // Round 0 reads every row: xadj, match (own + gathers), adjncy, adjwgt, prop.
     const int ph = r == 0 ? profiler().begin(kProfPropose, st) : -1;
 #define RMB_PROP(HW, MD)                                                                                  \
@@ -127,21 +195,34 @@ void match_parallel(const DGraph& g, int mode, uint64_t seed, int rounds, idx_t*
   if (nheavy > 0)                                                                                         \
     k_match_propose_heavy<HW, MD><<<grid_for(nheavy, 8, 148 * 8), 256, 0, st>>>(                         \
         g.xadj, g.adjncy, g.adjwgt, heavy, nheavy, match, prop, seed);
-    if (mode == 1) {
+    if (by_weight) {
       if (w) { RMB_PROP(true, 1) } else { RMB_PROP(false, 1) }
     } else {
       RMB_PROP(false, 0)
     }
 #undef RMB_PROP
     RMB_LAUNCH_CHECK();
-    profiler().end(ph, st, 12.0 * g.n + (w && mode == 1 ? 12.0 : 8.0) * (double)g.m);
-    k_match_accept<<<blocks, 256, 0, st>>>(g.n, prop, match, newly + r);
+    profiler().end(ph, st, 12.0 * g.n + (w && by_weight ? 12.0 : 8.0) * (double)g.m);
+    if (handshake) {
+      k_match_stamp<<<blocks, 256, 0, st>>>(g.n, match, prop, stamp, r);
+      RMB_LAUNCH_CHECK();
+      k_match_compete<<<blocks, 256, 0, st>>>(g.xadj, g.n, match, prop, stamp, r, best, vseed, mode == 1 ? 1 : 0);
+      RMB_LAUNCH_CHECK();
+      k_match_resolve<<<blocks, 256, 0, st>>>(g.n, prop, match, best, newly + r);
+    } else {
+      k_match_accept<<<blocks, 256, 0, st>>>(g.n, prop, match, newly + r);
+    }
     RMB_LAUNCH_CHECK();
-    // On large levels stop once a round matches almost nothing new.
-    if (g.n > 200000 && r >= 3 && (r & 1) == 1) {
-      RMB_CUDA(cudaMemcpyAsync(h_scratch, newly + r, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    // Every other round, look at the progress of the last two rounds.
+    if (r - phase_start >= 1 && ((r - phase_start) & 1) == 1) {
+      RMB_CUDA(cudaMemcpyAsync(h_scratch, newly + r - 1, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
       RMB_CUDA(cudaStreamSynchronize(st));
-      if ((int64_t)h_scratch[0] * 2 * 200 < (int64_t)g.n) break;
+      const int64_t last2 = (int64_t)h_scratch[0] + h_scratch[1];
+      if (last2 * 1000 < (int64_t)g.n) {
+        if (!handshake) break;
+        handshake = false;
+        phase_start = r + 1;
+      }
     }
   }
   k_match_finalize<<<blocks, 256, 0, st>>>(g.n, match);

@@ -22,8 +22,8 @@ struct KwayOptions {
   uint64_t seed = 0;
   uint32_t ufactor = 30;
   // engine knobs
-  int grow_trials = 8;       // grown partitions per attempt; the lowest cut is kept
-  int match_rounds = 16;     // proposal rounds per coarsening level (upper bound)
+  int grow_trials = 32;       // grown partitions per attempt; the lowest cut is kept
+  int match_rounds = 24;     // proposal rounds per coarsening level (upper bound)
   int summed_unit_weights = 0;  // 1: a graph without vwgt gets summed coarse weights
 };
 

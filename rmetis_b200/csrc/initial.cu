@@ -17,25 +17,33 @@ namespace rmb {
 // in ascending order, to the part with the smallest weight on constraint 0
 // (first minimum).
 //
-// Per-trial state lives in global scratch: part[n], queue links next[n],
-// part weights pw[k][ncon] (i64), queue head/tail[k].
+// One warp (one block) per trial. Its mutable state (part[n], queue links
+// next[n], part weights pw[k][ncon] as i64, queue head/tail[k], and a bitmap
+// of the parts below target in the current round) lives in shared memory when
+// it fits, else in the trial's global scratch. A part's weight only changes
+// during its own turn, so the parts that may grow in a round are known at the
+// round's start.
 template <bool HAS_VW>
-__global__ void k_grow(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
-                       const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ vwgt, int32_t n, int32_t ncon,
-                       int32_t k, int32_t ntrials, const idx_t* __restrict__ seeds,
-                       const long long* __restrict__ grow_tgt, idx_t* __restrict__ parts, idx_t* __restrict__ nexts,
-                       long long* __restrict__ pws, idx_t* __restrict__ heads, idx_t* __restrict__ tails,
-                       long long* __restrict__ cuts) {
+__global__ void __launch_bounds__(32) k_grow(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                                             const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ vwgt,
+                                             int32_t n, int32_t ncon, int32_t k, const idx_t* __restrict__ seeds,
+                                             const long long* __restrict__ grow_tgt, idx_t* __restrict__ parts,
+                                             unsigned char* __restrict__ gscratch, size_t scratch_bytes,
+                                             int use_smem, long long* __restrict__ cuts) {
+  extern __shared__ __align__(16) unsigned char smem[];
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  const int trial = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (trial >= ntrials) return;  // whole warp
-  idx_t* part = parts + (int64_t)trial * n;
-  idx_t* next = nexts + (int64_t)trial * n;
-  long long* pw = pws + (int64_t)trial * k * ncon;
-  idx_t* head = heads + (int64_t)trial * k;
-  idx_t* tail = tails + (int64_t)trial * k;
+  const int trial = blockIdx.x;
+  unsigned char* base = use_smem ? smem : gscratch + (size_t)trial * scratch_bytes;
+  long long* pw = reinterpret_cast<long long*>(base);
+  idx_t* part = reinterpret_cast<idx_t*>(pw + (size_t)k * ncon);
+  idx_t* next = part + n;
+  idx_t* head = next + n;
+  idx_t* tail = head + k;
+  unsigned* needy = reinterpret_cast<unsigned*>(tail + k);
+  const int32_t nwords = (k + 31) >> 5;
   const idx_t* sd = seeds + (int64_t)trial * k;
+  idx_t* out = parts + (int64_t)trial * n;
 
   for (int32_t v = lane; v < n; v += 32) part[v] = -1;
   __syncwarp();
@@ -49,64 +57,78 @@ __global__ void k_grow(const idx_t* __restrict__ xadj, const idx_t* __restrict__
   }
   __syncwarp();
 
-  int32_t active = k;
-  while (active > 0) {
-    active = 0;
-    for (int32_t p = 0; p < k; ++p) {
-      bool at_target = true;
-      for (int c = 0; c < ncon; ++c)
-        if (!(pw[(int64_t)p * ncon + c] >= grow_tgt[(int64_t)p * ncon + c])) { at_target = false; break; }
-      if (at_target) continue;
-      bool grew = false;
-      int32_t qh = head[p], qt = tail[p];
-      while (qh != -1) {
-        const int32_t v = qh;
-        qh = next[v];
-        const int32_t e = xadj[v + 1];
-        for (int32_t b = xadj[v]; b < e; b += 32) {
-          const int32_t j = b + lane;
-          int32_t u = -1;
-          bool cand = false;
-          if (j < e) {
-            u = adj[j];
-            cand = part[u] == -1;
-          }
-          const unsigned peers = __match_any_sync(FULL, cand ? u : -(lane + 2));
-          const bool first = cand && (__ffs(peers) - 1) == lane;
-          const unsigned fm = __ballot_sync(FULL, first);
-          if (fm) {
-            grew = true;
-            if (first) part[u] = p;
-            for (int c = 0; c < ncon; ++c) {
-              long long w = first ? (long long)(HAS_VW ? vwgt[(int64_t)u * ncon + c] : 1) : 0;
-              w = warp_sum(w);
-              if (lane == 0) pw[(int64_t)p * ncon + c] += w;
-            }
-            // Link the claimed vertices in lane order and append them.
-            const unsigned above = fm & ~((2u << lane) - 1u);
-            const int nl = above ? (__ffs(above) - 1) : lane;
-            const int32_t unext = __shfl_sync(FULL, u, nl);
-            if (first) next[u] = above ? unext : -1;
-            const int32_t ufirst = __shfl_sync(FULL, u, __ffs(fm) - 1);
-            const int32_t ulast = __shfl_sync(FULL, u, 31 - __clz(fm));
-            if (qh == -1) {
-              qh = ufirst;
-            } else if (lane == 0) {
-              next[qt] = ufirst;
-            }
-            qt = ulast;
-          }
-          __syncwarp();
-        }
-        if (grew) break;
+  bool any_active = true;
+  while (any_active) {
+    // Parts below target on some constraint (grow.rs:54-58), as a bitmap.
+    for (int32_t w0 = 0; w0 < nwords; ++w0) {
+      const int32_t p = w0 * 32 + lane;
+      bool needs = false;
+      if (p < k) {
+        for (int c = 0; c < ncon; ++c)
+          if (!(pw[(int64_t)p * ncon + c] >= grow_tgt[(int64_t)p * ncon + c])) { needs = true; break; }
       }
-      if (lane == 0) {
-        head[p] = qh;
-        tail[p] = qt;
-      }
-      __syncwarp();
-      if (grew) ++active;
+      const unsigned m = __ballot_sync(FULL, needs);
+      if (lane == 0) needy[w0] = m;
     }
+    __syncwarp();
+    int32_t active = 0;
+    for (int32_t w0 = 0; w0 < nwords; ++w0) {
+      unsigned bits = needy[w0];
+      while (bits) {
+        const int32_t p = w0 * 32 + __ffs(bits) - 1;
+        bits &= bits - 1;
+        bool grew = false;
+        int32_t qh = head[p], qt = tail[p];
+        while (qh != -1) {
+          const int32_t v = qh;
+          qh = next[v];
+          const int32_t e = __ldg(&xadj[v + 1]);
+          for (int32_t b = __ldg(&xadj[v]); b < e; b += 32) {
+            const int32_t j = b + lane;
+            int32_t u = -1;
+            bool cand = false;
+            if (j < e) {
+              u = __ldg(&adj[j]);
+              cand = part[u] == -1;
+            }
+            const unsigned peers = __match_any_sync(FULL, cand ? u : -(lane + 2));
+            const bool first = cand && (__ffs(peers) - 1) == lane;
+            const unsigned fm = __ballot_sync(FULL, first);
+            if (fm) {
+              grew = true;
+              if (first) part[u] = p;
+              for (int c = 0; c < ncon; ++c) {
+                long long w = first ? (long long)(HAS_VW ? __ldg(&vwgt[(int64_t)u * ncon + c]) : 1) : 0;
+                w = warp_sum(w);
+                if (lane == 0) pw[(int64_t)p * ncon + c] += w;
+              }
+              // Link the claimed vertices in lane order and append them.
+              const unsigned above = fm & ~((2u << lane) - 1u);
+              const int nl = above ? (__ffs(above) - 1) : lane;
+              const int32_t unext = __shfl_sync(FULL, u, nl);
+              if (first) next[u] = above ? unext : -1;
+              const int32_t ufirst = __shfl_sync(FULL, u, __ffs(fm) - 1);
+              const int32_t ulast = __shfl_sync(FULL, u, 31 - __clz(fm));
+              if (qh == -1) {
+                qh = ufirst;
+              } else if (lane == 0) {
+                next[qt] = ufirst;
+              }
+              qt = ulast;
+            }
+            __syncwarp();
+          }
+          if (grew) break;
+        }
+        if (lane == 0) {
+          head[p] = qh;
+          tail[p] = qt;
+        }
+        __syncwarp();
+        if (grew) ++active;
+      }
+    }
+    any_active = active > 0;
   }
 
   // Leftovers (disconnected or unreachable): lightest part on constraint 0.
@@ -138,12 +160,13 @@ __global__ void k_grow(const idx_t* __restrict__ xadj, const idx_t* __restrict__
   }
   __syncwarp();
 
-  // Edge cut of this trial (sum over both directions).
+  // Write the partition out and compute its edge cut (both directions).
   long long acc = 0;
   for (int32_t v = lane; v < n; v += 32) {
     const int32_t pv = part[v];
-    for (int32_t j = xadj[v]; j < xadj[v + 1]; ++j)
-      if (part[adj[j]] != pv) acc += adjwgt ? adjwgt[j] : 1;
+    out[v] = pv;
+    for (int32_t j = __ldg(&xadj[v]); j < __ldg(&xadj[v + 1]); ++j)
+      if (part[__ldg(&adj[j])] != pv) acc += adjwgt ? __ldg(&adjwgt[j]) : 1;
   }
   acc = warp_sum(acc);
   if (lane == 0) cuts[trial] = acc;
@@ -152,19 +175,18 @@ __global__ void k_grow(const idx_t* __restrict__ xadj, const idx_t* __restrict__
 void grow_trials(const DGraph& g, int k, int ntrials, const idx_t* seeds, const long long* grow_tgt, idx_t* parts,
                  long long* cuts, Arena& arena, cudaStream_t st) {
   Arena::Mark mk = arena.mark();
-  idx_t* nexts = arena.alloc<idx_t>((size_t)ntrials * g.n);
-  long long* pws = arena.alloc<long long>((size_t)ntrials * k * g.ncon);
-  idx_t* heads = arena.alloc<idx_t>((size_t)ntrials * k);
-  idx_t* tails = arena.alloc<idx_t>((size_t)ntrials * k);
-  const int wpb = 4;
-  const int blocks = (int)ceil_div(ntrials, wpb);
+  const size_t bytes = sizeof(long long) * (size_t)k * g.ncon + sizeof(idx_t) * (2 * (size_t)g.n + 2 * (size_t)k) +
+                       sizeof(unsigned) * (((size_t)k + 31) / 32) + 16;
+  const size_t bytes_al = (bytes + 255) & ~(size_t)255;
+  const size_t kSmemLimit = 200 * 1024;
+  const int use_smem = bytes_al <= kSmemLimit ? 1 : 0;
+  unsigned char* scratch = use_smem ? nullptr : arena.alloc<unsigned char>(bytes_al * (size_t)ntrials);
+  const size_t dyn = use_smem ? bytes_al : 0;
+  auto kern = g.vwgt ? k_grow<true> : k_grow<false>;
+  RMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimit));
   const int ph = profiler().begin(kProfGrow, st);
-  if (g.vwgt)
-    k_grow<true><<<blocks, 32 * wpb, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, g.vwgt, g.n, g.ncon, k, ntrials, seeds,
-                                              grow_tgt, parts, nexts, pws, heads, tails, cuts);
-  else
-    k_grow<false><<<blocks, 32 * wpb, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, g.vwgt, g.n, g.ncon, k, ntrials, seeds,
-                                               grow_tgt, parts, nexts, pws, heads, tails, cuts);
+  kern<<<ntrials, 32, dyn, st>>>(g.xadj, g.adjncy, g.adjwgt, g.vwgt, g.n, g.ncon, k, seeds, grow_tgt, parts, scratch,
+                                 bytes_al, use_smem, cuts);
   RMB_LAUNCH_CHECK();
   profiler().end(ph, st, (double)ntrials * (16.0 * g.n + 8.0 * (double)g.m));
   arena.reset_to(mk);

@@ -8,17 +8,19 @@
 //
 // Gains and candidate orders depend only on the start-of-pass part vector, so
 // they are computed for all vertices at once (k_gain). The only sequential
-// dependency is `pw`. Movers (vertices that may move) are split into blocks of
-// kDecideBlock in ascending id. Given the exact part weights at the start of a
-// block, a block finds its exact decisions by iterating "decide every mover
-// against the weights implied by the decisions of the movers before it" to a
-// fixed point (mover t is final after t iterations). Blocks run in parallel
-// against the prefix implied by the previous round's decisions of the blocks
-// before them (a per-block delta table and its column scan), and rounds
-// repeat until no decision changes, at which point every block saw the exact
-// prefix. Block b is exact after b+1 rounds at the latest, so the loop always
-// ends, and the result equals the sequential pass.
+// dependency is `pw`: near the balance limit a move into a part is feasible
+// only because earlier moves left it, which chains decisions together. The
+// decisions are therefore made in mover order by a walker (k_walk: one
+// block, part weights in shared memory, mover records streamed through
+// shared memory while the walking warp works). Before the walk, a parallel
+// pass resolves every mover whose decision cannot depend on the order: a
+// candidate part that stays feasible even if every potential move into it
+// happens first, or that stays infeasible even if every potential move out
+// of it happens first (k_walk_classify). The walker only evaluates the rest.
+#include <chrono>
 #include <climits>
+#include <cstdio>
+#include <cstdlib>
 
 #include "kernels.h"
 #include "prof.h"
@@ -193,225 +195,298 @@ __global__ void k_gain_heavy(const idx_t* __restrict__ xadj, const idx_t* __rest
   }
 }
 
+
 // ---------------------------------------------------------------------------
-// Decision kernel. One block = kDecideBlock consecutive movers.
+// Mover records and the walk
 // ---------------------------------------------------------------------------
-struct DecideArgs {
-  int32_t nm;
-  const idx_t* movers;
-  const idx_t* part;
-  const idx_t* vwgt;
-  int32_t ncon;
-  int32_t k;
-  const idx_t* xadj;
-  const idx_t* ncand;
-  const idx_t* wfrom;
-  const idx_t* cand_p;
-  const idx_t* cand_g;
-  const long long* pw0;
-  const long long* feas_max;
-  const long long* over_thr;
+constexpr int kInline = 4;          // candidates kept inline in a mover record
+constexpr int kWalkChunk = 256;     // mover records per shared-memory chunk
+constexpr int kWalkThreads = 256;   // warp 0 walks, the other warps stream records
+constexpr int32_t kContended = -2;  // decision not known before the walk
+constexpr int kWalkSmemParts = 4096;  // [k][ncon] entries kept in shared memory
+
+struct MoverRecs {  // structure of arrays, nm entries each
+  int32_t* pv;
+  int32_t* ne;
+  int32_t* wf;
+  int32_t* coff;   // xadj[v]: start of the vertex's candidate slots
+  int32_t* known;  // decision fixed before the walk, or kContended
+  int32_t* cp;     // [nm][kInline] candidate parts
+  int32_t* cg;     // [nm][kInline] candidate gains
+  int32_t* vw;     // [nm][ncon]
 };
 
-struct BlockShared {
-  int32_t d[kDecideBlock];
-  int32_t pv[kDecideBlock];
-  int32_t vw[kDecideBlock * kMaxCon];
-};
-
-// Part weights seen by mover t of the block: base (exact weights at the start
-// of the block) plus the moves of movers 0..t-1 of the block.
-__device__ inline void pw_at(const DecideArgs& a, const BlockShared& sh, const long long* base, int t, int32_t p,
-                             long long* out) {
-  const int ncon = a.ncon;
-  for (int c = 0; c < ncon; ++c) out[c] = base[(int64_t)p * ncon + c];
-  for (int t2 = 0; t2 < t; ++t2) {
-    const int32_t d2 = sh.d[t2];
-    if (d2 < 0) continue;
-    if (d2 == p)
-      for (int c = 0; c < ncon; ++c) out[c] += sh.vw[t2 * kMaxCon + c];
-    if (sh.pv[t2] == p)
-      for (int c = 0; c < ncon; ++c) out[c] -= sh.vw[t2 * kMaxCon + c];
-  }
-}
-
-__device__ inline bool feasible(const DecideArgs& a, const BlockShared& sh, const long long* base, int t,
-                                int32_t p) {
-  long long w[kMaxCon];
-  pw_at(a, sh, base, t, p, w);
-  for (int c = 0; c < a.ncon; ++c)
-    if (w[c] + sh.vw[t * kMaxCon + c] > a.feas_max[(int64_t)p * a.ncon + c]) return false;
-  return true;
-}
-
-// The reference's choice for mover t (greedy.rs:64-107 repair, :131-164 cut):
-// candidates in (gain desc, part asc) order = explicit ones with gain above
-// the non-adjacent gain, then non-adjacent parts by id, then the explicit ones
-// below; the first feasible candidate with gain above the pass threshold.
+// One thread per mover: copy its data into a record and add its weight to
+// the bounds: in_max[p] over every part it may move to, out_max[pv].
 template <int MODE>
-__device__ int32_t decide_one(const DecideArgs& a, const BlockShared& sh, const long long* base, int t, int32_t v) {
-  const int32_t pv = sh.pv[t];
-  if (MODE == kRepair) {
-    long long w[kMaxCon];
-    pw_at(a, sh, base, t, pv, w);
-    bool over = false;
-    for (int c = 0; c < a.ncon; ++c)
-      if (w[c] > a.over_thr[(int64_t)pv * a.ncon + c]) over = true;
-    if (!over) return -1;
-  }
-  const int32_t thr = (MODE == kRepair) ? INT_MIN : 0;
-  const int32_t s = a.xadj[v];
-  const int32_t ne = a.ncand[v];
-  const int32_t ig = (int32_t)(0u - (uint32_t)a.wfrom[v]);
-  int32_t i = 0;
-  for (; i < ne; ++i) {
-    const int32_t g = a.cand_g[s + i];
-    if (g <= ig) break;
-    if (g <= thr) return -1;
-    const int32_t p = a.cand_p[s + i];
-    if (feasible(a, sh, base, t, p)) return p;
-  }
-  if (ig > thr) {
-    for (int32_t p = 0; p < a.k; ++p) {
-      if (p == pv) continue;
-      bool in_e = false;
-      for (int32_t q = 0; q < ne; ++q)
-        if (a.cand_p[s + q] == p) { in_e = true; break; }
-      if (in_e) continue;
-      if (feasible(a, sh, base, t, p)) return p;
+__global__ void k_walk_prep(const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
+                            const idx_t* __restrict__ part, const idx_t* __restrict__ vwgt, int32_t ncon,
+                            const idx_t* __restrict__ xadj, const idx_t* __restrict__ ncand,
+                            const idx_t* __restrict__ wfrom, const idx_t* __restrict__ cand_p,
+                            const idx_t* __restrict__ cand_g, MoverRecs r, long long* __restrict__ in_max,
+                            long long* __restrict__ out_max) {
+  const int32_t nm = *nm_dev;
+  RMB_GRID_STRIDE(j, nm) {
+    const int32_t v = movers[j];
+    const int32_t pv = part[v];
+    const int32_t s = xadj[v];
+    const int32_t ne = ncand[v];
+    r.pv[j] = pv;
+    if (MODE != kCut) r.known[j] = kContended;
+    r.ne[j] = ne;
+    r.wf[j] = wfrom[v];
+    r.coff[j] = s;
+    for (int i = 0; i < kInline; ++i) {
+      r.cp[j * kInline + i] = i < ne ? cand_p[s + i] : -1;
+      r.cg[j * kInline + i] = i < ne ? cand_g[s + i] : 0;
+    }
+    for (int c = 0; c < ncon; ++c) {
+      const int32_t w = vwgt ? vwgt[(int64_t)v * ncon + c] : 1;
+      r.vw[(int64_t)j * ncon + c] = w;
+      if (MODE == kCut) {
+        atomic_add_i64(&out_max[(int64_t)pv * ncon + c], w);
+        for (int i = 0; i < ne; ++i) {
+          if (cand_g[s + i] <= 0) break;  // sorted: the rest never qualify
+          atomic_add_i64(&in_max[(int64_t)cand_p[s + i] * ncon + c], w);
+        }
+      }
     }
   }
-  for (; i < ne; ++i) {
-    const int32_t g = a.cand_g[s + i];
+}
+
+// Cut passes: fix the decision of every mover whose walk through its
+// candidates meets only parts that are infeasible whatever happens before it,
+// and then a part that is feasible whatever happens before it (or runs out).
+__global__ void k_walk_classify(const int32_t* __restrict__ nm_dev, int32_t ncon, const idx_t* __restrict__ cand_p,
+                                const idx_t* __restrict__ cand_g, MoverRecs r, const long long* __restrict__ pw0,
+                                const long long* __restrict__ feas, const long long* __restrict__ in_max,
+                                const long long* __restrict__ out_max) {
+  const int32_t nm = *nm_dev;
+  RMB_GRID_STRIDE(j, nm) {
+    const int32_t ne = r.ne[j];
+    const int32_t ig = (int32_t)(0u - (uint32_t)r.wf[j]);
+    int32_t known = -1;
+    if (ig > 0) {
+      known = kContended;  // non-adjacent parts have positive gain (negative weights)
+    } else {
+      const int32_t s = r.coff[j];
+      for (int32_t i = 0; i < ne; ++i) {
+        const int32_t g = i < kInline ? r.cg[j * kInline + i] : cand_g[s + i];
+        if (g <= 0) break;
+        const int32_t p = i < kInline ? r.cp[j * kInline + i] : cand_p[s + i];
+        bool always = true, never = false;
+        for (int c = 0; c < ncon; ++c) {
+          const int64_t x = (int64_t)p * ncon + c;
+          if (pw0[x] + in_max[x] > feas[x]) always = false;
+          if (pw0[x] - out_max[x] + r.vw[(int64_t)j * ncon + c] > feas[x]) never = true;
+        }
+        if (always) { known = p; break; }
+        if (never) continue;
+        known = kContended;
+        break;
+      }
+    }
+    r.known[j] = known;
+  }
+}
+
+struct WalkBuf {
+  int32_t pv[kWalkChunk];
+  int32_t ne[kWalkChunk];
+  int32_t wf[kWalkChunk];
+  int32_t coff[kWalkChunk];
+  int32_t known[kWalkChunk];
+  int32_t cp[kWalkChunk * kInline];
+  int32_t cg[kWalkChunk * kInline];
+  int32_t vw[kWalkChunk * kMaxCon];
+};
+
+__device__ inline void walk_load(WalkBuf& b, const MoverRecs& r, int32_t j0, int32_t nm, int32_t ncon, int tid,
+                                 int nthreads) {
+  for (int i = tid; i < kWalkChunk; i += nthreads) {
+    const int32_t j = j0 + i;
+    if (j < nm) {
+      b.pv[i] = r.pv[j];
+      b.ne[i] = r.ne[j];
+      b.wf[i] = r.wf[j];
+      b.coff[i] = r.coff[j];
+      b.known[i] = r.known[j];
+    }
+  }
+  for (int i = tid; i < kWalkChunk * kInline; i += nthreads) {
+    const int64_t j = (int64_t)j0 * kInline + i;
+    if (j < (int64_t)nm * kInline) {
+      b.cp[i] = r.cp[j];
+      b.cg[i] = r.cg[j];
+    }
+  }
+  for (int i = tid; i < kWalkChunk * ncon; i += nthreads) {
+    const int64_t j = (int64_t)j0 * ncon + i;
+    if (j < (int64_t)nm * ncon) b.vw[(i / ncon) * kMaxCon + (i % ncon)] = r.vw[j];
+  }
+}
+
+// The decision of one mover (greedy.rs:64-107 repair, :131-164 cut) against
+// the part weights given by `pwf(p, c)`: candidates in (gain desc, part asc)
+// order = explicit ones with gain above the non-adjacent gain -w_from, then
+// the non-adjacent parts by id, then the explicit ones below it; the first
+// feasible candidate with gain above the pass threshold, or -1.
+template <int MODE, typename PW>
+__device__ inline int32_t walk_decide(const WalkBuf& b, int i, int32_t ncon, int32_t k,
+                                      const idx_t* __restrict__ cand_p, const idx_t* __restrict__ cand_g,
+                                      const long long* feas, const long long* over, PW pwf) {
+  const int32_t pv = b.pv[i];
+  const int32_t* vw = &b.vw[i * kMaxCon];
+  if (MODE == kRepair) {
+    bool is_over = false;
+    for (int c = 0; c < ncon; ++c)
+      if (pwf(pv, c) > over[(int64_t)pv * ncon + c]) is_over = true;
+    if (!is_over) return -1;
+  }
+  const int32_t thr = (MODE == kRepair) ? INT_MIN : 0;
+  const int32_t ne = b.ne[i];
+  const int32_t s = b.coff[i];
+  const int32_t ig = (int32_t)(0u - (uint32_t)b.wf[i]);
+  auto cpart = [&](int32_t q) { return q < kInline ? b.cp[i * kInline + q] : cand_p[s + q]; };
+  auto cgain = [&](int32_t q) { return q < kInline ? b.cg[i * kInline + q] : cand_g[s + q]; };
+  auto feasible = [&](int32_t p) {
+    for (int c = 0; c < ncon; ++c)
+      if (pwf(p, c) + vw[c] > feas[(int64_t)p * ncon + c]) return false;
+    return true;
+  };
+  int32_t q = 0;
+  for (; q < ne; ++q) {
+    const int32_t g = cgain(q);
+    if (g <= ig) break;
     if (g <= thr) return -1;
-    const int32_t p = a.cand_p[s + i];
-    if (feasible(a, sh, base, t, p)) return p;
+    const int32_t p = cpart(q);
+    if (feasible(p)) return p;
+  }
+  if (ig > thr) {
+    for (int32_t p = 0; p < k; ++p) {
+      if (p == pv) continue;
+      bool in_e = false;
+      for (int32_t e = 0; e < ne; ++e)
+        if (cpart(e) == p) { in_e = true; break; }
+      if (!in_e && feasible(p)) return p;
+    }
+  }
+  for (; q < ne; ++q) {
+    const int32_t g = cgain(q);
+    if (g <= thr) return -1;
+    const int32_t p = cpart(q);
+    if (feasible(p)) return p;
   }
   return -1;
 }
 
-// Exact decisions of one block given `base` (weights before its first mover).
+// The walk. Warp 0 takes the movers of a chunk in windows of 32 consecutive
+// movers, one per lane. Every lane decides against the weights at the window
+// start (d0), then again against those weights plus the moves d0 of the lanes
+// before it (d1). Up to the first lane whose d1 differs from d0, every d0 is
+// the sequential decision (by induction from lane 0, which sees exact
+// weights), and that lane's d1 is too; those lanes commit and the next window
+// starts after them. Warps 1.. stream the next chunk meanwhile. The part
+// weights pw, feas and over live in shared memory when [k][ncon] fits.
 template <int MODE>
-__device__ int32_t block_fixpoint(const DecideArgs& a, BlockShared& sh, const long long* base, int32_t j0,
-                                  int32_t d_init) {
-  const int t = threadIdx.x;
-  const int32_t j = j0 + t;
-  const bool valid = j < a.nm;
-  const int32_t v = valid ? a.movers[j] : -1;
-  if (valid) {
-    sh.pv[t] = a.part[v];
-    for (int c = 0; c < a.ncon; ++c) sh.vw[t * kMaxCon + c] = a.vwgt ? a.vwgt[(int64_t)v * a.ncon + c] : 1;
-  } else {
-    sh.pv[t] = -1;
-  }
-  int32_t d = valid ? d_init : -1;
-  for (int it = 0; it <= kDecideBlock; ++it) {
-    sh.d[t] = d;
-    __syncthreads();
-    const int32_t nd = valid ? decide_one<MODE>(a, sh, base, t, v) : -1;
-    const int changed = __syncthreads_or(nd != d);
-    d = nd;
-    if (!changed) break;
-  }
-  sh.d[t] = d;
-  __syncthreads();
-  return d;
-}
-
-// Parallel round: block b decides against pw0 + PD[b] (PD == nullptr: zero
-// prefix), writes its decisions, its delta row D[b] and counts a change
-// against d_prev.
-template <int MODE>
-__global__ void __launch_bounds__(kDecideBlock) k_decide(DecideArgs a, const long long* __restrict__ PD,
-                                                        const idx_t* __restrict__ d_prev, idx_t* __restrict__ d_out,
-                                                        int32_t* __restrict__ D, long long* __restrict__ base_scratch,
-                                                        int32_t* __restrict__ changed) {
-  __shared__ BlockShared sh;
-  const int32_t b = blockIdx.x;
-  const int32_t K = a.k * a.ncon;
-  long long* base = base_scratch + (int64_t)b * K;
-  for (int32_t x = threadIdx.x; x < K; x += blockDim.x) base[x] = a.pw0[x] + (PD ? PD[(int64_t)b * K + x] : 0);
-  __syncthreads();
-  const int32_t j0 = b * kDecideBlock;
-  const int32_t j = j0 + threadIdx.x;
-  const int32_t dinit = (d_prev && j < a.nm) ? d_prev[j] : -1;
-  const int32_t d = block_fixpoint<MODE>(a, sh, base, j0, dinit);
-  int ch = 0;
-  if (j < a.nm) {
-    d_out[j] = d;
-    ch = d_prev ? (d != d_prev[j]) : 1;
-  }
-  if (__syncthreads_or(ch) && threadIdx.x == 0) atomicAdd(changed, 1);
-  int32_t* row = D + (int64_t)b * K;
-  for (int32_t x = threadIdx.x; x < K; x += blockDim.x) row[x] = 0;
-  __syncthreads();
-  if (d >= 0) {
-    const int t = threadIdx.x;
-    for (int c = 0; c < a.ncon; ++c) {
-      atomicAdd(&row[d * a.ncon + c], sh.vw[t * kMaxCon + c]);
-      atomicAdd(&row[sh.pv[t] * a.ncon + c], -sh.vw[t * kMaxCon + c]);
+__global__ void __launch_bounds__(kWalkThreads) k_walk(const int32_t* __restrict__ nm_dev, MoverRecs r,
+                                                       int32_t ncon, int32_t k, const idx_t* __restrict__ cand_p,
+                                                       const idx_t* __restrict__ cand_g, long long* __restrict__ pw,
+                                                       const long long* __restrict__ feas_g,
+                                                       const long long* __restrict__ over_g,
+                                                       idx_t* __restrict__ d_out, int32_t* __restrict__ nmoves) {
+  extern __shared__ long long sparts[];
+  __shared__ WalkBuf buf[2];
+  __shared__ int32_t win_d[32], win_pv[32], win_vw[32 * kMaxCon];
+  const int32_t nm = *nm_dev;
+  const int32_t K = k * ncon;
+  const bool in_smem = K <= kWalkSmemParts;
+  long long* spw = in_smem ? sparts : pw;
+  const long long* sfeas = in_smem ? sparts + K : feas_g;
+  const long long* sover = in_smem ? sparts + 2 * K : over_g;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (in_smem) {
+    for (int32_t x = tid; x < K; x += blockDim.x) {
+      sparts[x] = pw[x];
+      sparts[K + x] = feas_g[x];
+      sparts[2 * K + x] = over_g[x];
     }
   }
-}
-
-// Sequential variant: one block walks all mover blocks in order, carrying
-// the exact running weights in `run` (K entries, initialised to pw0).
-template <int MODE>
-__global__ void __launch_bounds__(kDecideBlock) k_decide_seq(DecideArgs a, idx_t* __restrict__ d_out,
-                                                            long long* __restrict__ run) {
-  __shared__ BlockShared sh;
-  const int32_t K = a.k * a.ncon;
-  for (int32_t x = threadIdx.x; x < K; x += blockDim.x) run[x] = a.pw0[x];
+  if (nm > 0) walk_load(buf[0], r, 0, nm, ncon, tid, blockDim.x);
   __syncthreads();
-  for (int32_t j0 = 0; j0 < a.nm; j0 += kDecideBlock) {
-    const int32_t d = block_fixpoint<MODE>(a, sh, run, j0, -1);
-    const int32_t j = j0 + threadIdx.x;
-    if (j < a.nm) d_out[j] = d;
-    __syncthreads();  // every thread has finished reading `run`
-    if (d >= 0) {
-      const int t = threadIdx.x;
-      for (int c = 0; c < a.ncon; ++c) {
-        atomic_add_i64(&run[(int64_t)d * a.ncon + c], sh.vw[t * kMaxCon + c]);
-        atomic_add_i64(&run[(int64_t)sh.pv[t] * a.ncon + c], -(long long)sh.vw[t * kMaxCon + c]);
+  int32_t moves = 0;
+  const int32_t nchunks = (int32_t)ceil_div(nm, kWalkChunk);
+  for (int32_t ch = 0; ch < nchunks; ++ch) {
+    if (warp == 0) {
+      const WalkBuf& b = buf[ch & 1];
+      const int32_t j0 = ch * kWalkChunk;
+      const int32_t cnt = min(kWalkChunk, nm - j0);
+      auto pw_start = [&](int32_t p, int c) { return spw[(int64_t)p * ncon + c]; };
+      int32_t i0 = 0;
+      while (i0 < cnt) {
+        const int i = i0 + lane;
+        const bool valid = i < cnt;
+        int32_t d0 = -1, pv = -1;
+        if (valid) {
+          pv = b.pv[i];
+          d0 = b.known[i];
+          if (d0 == kContended) d0 = walk_decide<MODE>(b, i, ncon, k, cand_p, cand_g, sfeas, sover, pw_start);
+          for (int c = 0; c < ncon; ++c) win_vw[lane * kMaxCon + c] = b.vw[i * kMaxCon + c];
+        }
+        win_d[lane] = d0;
+        win_pv[lane] = pv;
+        __syncwarp();
+        int32_t d1 = d0;
+        if (valid && b.known[i] == kContended && lane > 0) {
+          auto pw_prefix = [&](int32_t p, int c) {
+            long long x = spw[(int64_t)p * ncon + c];
+            for (int l = 0; l < lane; ++l) {
+              const int32_t dl = win_d[l];
+              if (dl < 0) continue;
+              if (dl == p) x += win_vw[l * kMaxCon + c];
+              if (win_pv[l] == p) x -= win_vw[l * kMaxCon + c];
+            }
+            return x;
+          };
+          d1 = walk_decide<MODE>(b, i, ncon, k, cand_p, cand_g, sfeas, sover, pw_prefix);
+        }
+        const unsigned mism = __ballot_sync(0xffffffffu, valid && d1 != d0);
+        const int f = mism ? (__ffs(mism) - 1) : 32;
+        const bool commit = valid && lane <= f;
+        const int32_t d = (lane == f) ? d1 : d0;
+        if (commit) {
+          d_out[j0 + i] = d;
+          if (d >= 0) {
+            for (int c = 0; c < ncon; ++c) {
+              const long long w = win_vw[lane * kMaxCon + c];
+              atomicAdd(reinterpret_cast<unsigned long long*>(&spw[(int64_t)pv * ncon + c]),
+                        (unsigned long long)(-w));
+              atomicAdd(reinterpret_cast<unsigned long long*>(&spw[(int64_t)d * ncon + c]), (unsigned long long)w);
+            }
+          }
+        }
+        moves += __popc(__ballot_sync(0xffffffffu, commit && d >= 0));
+        __syncwarp();
+        i0 += (f < 32) ? f + 1 : 32;
       }
+    } else if (ch + 1 < nchunks) {
+      walk_load(buf[(ch + 1) & 1], r, (ch + 1) * kWalkChunk, nm, ncon, tid - 32, blockDim.x - 32);
     }
     __syncthreads();
   }
+  if (in_smem)
+    for (int32_t x = tid; x < K; x += blockDim.x) pw[x] = sparts[x];
+  if (tid == 0) *nmoves = moves;
 }
 
-// PD[b][x] = sum over b' < b of D[b'][x].
-__global__ void k_prefix_blocks(const int32_t* __restrict__ D, int32_t nb, int32_t K, long long* __restrict__ PD) {
-  RMB_GRID_STRIDE(x, K) {
-    long long run = 0;
-    for (int32_t b = 0; b < nb; ++b) {
-      PD[(int64_t)b * K + x] = run;
-      run += D[(int64_t)b * K + x];
-    }
-  }
-}
-
-// Apply the pass's moves together (greedy.rs:111-119, :168-181) and keep the
-// part weights current.
-__global__ void k_apply(int32_t nm, const idx_t* __restrict__ movers, const idx_t* __restrict__ d,
-                        idx_t* __restrict__ part, const idx_t* __restrict__ vwgt, int32_t ncon,
-                        long long* __restrict__ pw, int32_t* __restrict__ nmoves) {
-  int32_t cnt = 0;
+// Apply the pass's moves together (greedy.rs:111-119, :168-181).
+__global__ void k_apply(const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
+                        const idx_t* __restrict__ d, idx_t* __restrict__ part) {
+  const int32_t nm = *nm_dev;
   RMB_GRID_STRIDE(j, nm) {
     const int32_t dd = d[j];
-    if (dd >= 0) {
-      const int32_t v = movers[j];
-      const int32_t pv = part[v];
-      part[v] = dd;
-      for (int c = 0; c < ncon; ++c) {
-        const long long w = vwgt ? vwgt[(int64_t)v * ncon + c] : 1;
-        atomic_add_i64(&pw[(int64_t)dd * ncon + c], w);
-        atomic_add_i64(&pw[(int64_t)pv * ncon + c], -w);
-      }
-      ++cnt;
-    }
+    if (dd >= 0) part[movers[j]] = dd;
   }
-  cnt = warp_sum(cnt);
-  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(nmoves, cnt);
 }
 
 // ---------------------------------------------------------------------------
@@ -456,6 +531,35 @@ void gain_table(const DGraph& g, const idx_t* part, int k, idx_t* boundary, idx_
   if (ghist) RMB_CUDA(cudaFreeAsync(ghist, st));
 }
 
+template <int MODE>
+static void launch_walk(int32_t nmax, const int32_t* nm_dev, const idx_t* movers, const DGraph& g, const idx_t* part,
+                        int k, const idx_t* ncand, const idx_t* wfrom, const idx_t* cand_p, const idx_t* cand_g,
+                        const MoverRecs& r, long long* pw, const long long* feas, const long long* over,
+                        long long* in_max, long long* out_max, idx_t* d_out, int32_t* nmoves, cudaStream_t st) {
+  const int32_t K = k * g.ncon;
+  const int blocks = grid_for(nmax, 256);
+  if (MODE == kCut) {
+    RMB_CUDA(cudaMemsetAsync(in_max, 0, sizeof(long long) * (size_t)K, st));
+    RMB_CUDA(cudaMemsetAsync(out_max, 0, sizeof(long long) * (size_t)K, st));
+  }
+  k_walk_prep<MODE><<<blocks, 256, 0, st>>>(nm_dev, movers, part, g.vwgt, g.ncon, g.xadj, ncand, wfrom, cand_p,
+                                            cand_g, r, in_max, out_max);
+  RMB_LAUNCH_CHECK();
+  if (MODE == kCut) {
+    k_walk_classify<<<blocks, 256, 0, st>>>(nm_dev, g.ncon, cand_p, cand_g, r, pw, feas, in_max, out_max);
+    RMB_LAUNCH_CHECK();
+  }
+  const size_t smem = K <= kWalkSmemParts ? sizeof(long long) * 3 * (size_t)K : 0;
+  RMB_CUDA(cudaFuncSetAttribute(k_walk<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(long long) * 3 * kWalkSmemParts)));
+  const int ph = profiler().begin(kProfDecide, st);
+  k_walk<MODE><<<1, kWalkThreads, smem, st>>>(nm_dev, r, g.ncon, k, cand_p, cand_g, pw, feas, over, d_out, nmoves);
+  RMB_LAUNCH_CHECK();
+  profiler().end(ph, st, 0.0);
+  k_apply<<<blocks, 256, 0, st>>>(nm_dev, movers, d_out, const_cast<idx_t*>(part));
+  RMB_LAUNCH_CHECK();
+}
+
 RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, const idx_t* heavy, int32_t nheavy,
                           Arena& arena, cudaStream_t st, int32_t* h_scratch) {
   if (g.ncon > kMaxCon) throw Error(-2, "ncon above the supported maximum of 8");
@@ -464,103 +568,58 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
   const int32_t K = k * g.ncon;
   Arena::Mark mk = arena.mark();
   long long* pw = arena.alloc<long long>((size_t)K);
+  long long* in_max = arena.alloc<long long>((size_t)K);
+  long long* out_max = arena.alloc<long long>((size_t)K);
   idx_t* mover = arena.alloc<idx_t>((size_t)g.n);
   idx_t* ncand = arena.alloc<idx_t>((size_t)g.n);
   idx_t* wfrom = arena.alloc<idx_t>((size_t)g.n);
   idx_t* cand_p = arena.alloc<idx_t>((size_t)g.m + 1);
   idx_t* cand_g = arena.alloc<idx_t>((size_t)g.m + 1);
   idx_t* movers = arena.alloc<idx_t>((size_t)g.n);
-  idx_t* d_a = arena.alloc<idx_t>((size_t)g.n);
-  idx_t* d_b = arena.alloc<idx_t>((size_t)g.n);
-  int32_t* counters = arena.alloc<int32_t>(8);  // [0] nm, [1] changed, [2] moves
+  idx_t* dec = arena.alloc<idx_t>((size_t)g.n);
+  int32_t* counters = arena.alloc<int32_t>(8);  // [0] nm, [2] moves
+  MoverRecs r;
+  r.pv = arena.alloc<int32_t>((size_t)g.n);
+  r.ne = arena.alloc<int32_t>((size_t)g.n);
+  r.wf = arena.alloc<int32_t>((size_t)g.n);
+  r.coff = arena.alloc<int32_t>((size_t)g.n);
+  r.known = arena.alloc<int32_t>((size_t)g.n);
+  r.cp = arena.alloc<int32_t>((size_t)g.n * kInline);
+  r.cg = arena.alloc<int32_t>((size_t)g.n * kInline);
+  r.vw = arena.alloc<int32_t>((size_t)g.n * g.ncon);
   int32_t* ghist = (nheavy > 0 && k > kGainHist) ? arena.alloc<int32_t>((size_t)k * 256 * 4) : nullptr;
   partition_weights_only(g, part, k, pw, st);
 
-  DecideArgs a;
-  a.movers = movers;
-  a.part = part;
-  a.vwgt = g.vwgt;
-  a.ncon = g.ncon;
-  a.k = k;
-  a.xadj = g.xadj;
-  a.ncand = ncand;
-  a.wfrom = wfrom;
-  a.cand_p = cand_p;
-  a.cand_g = cand_g;
-  a.pw0 = pw;
-  a.feas_max = rp.feas_max;
-  a.over_thr = rp.over_thr;
-
+  static const bool trace = std::getenv("RMETIS_B200_TRACE") != nullptr;
   for (int pass = 0; pass <= rp.niter; ++pass) {
     const int mode = pass == 0 ? kRepair : kCut;
+    const auto t_pass0 = std::chrono::steady_clock::now();
     if (mode == kRepair)
       launch_gain<kRepair>(g, part, k, pw, rp.over_thr, mover, ncand, wfrom, cand_p, cand_g, heavy, nheavy, ghist, st);
     else
       launch_gain<kCut>(g, part, k, pw, rp.over_thr, mover, ncand, wfrom, cand_p, cand_g, heavy, nheavy, ghist, st);
     compact_flags(mover, g.n, movers, counters, arena, st);
-    RMB_CUDA(cudaMemcpyAsync(h_scratch, counters, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    if (mode == kRepair)
+      launch_walk<kRepair>(g.n, counters, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r, pw, rp.feas_max,
+                           rp.over_thr, in_max, out_max, dec, counters + 2, st);
+    else
+      launch_walk<kCut>(g.n, counters, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r, pw, rp.feas_max,
+                        rp.over_thr, in_max, out_max, dec, counters + 2, st);
+    RMB_CUDA(cudaMemcpyAsync(h_scratch, counters, 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     RMB_CUDA(cudaStreamSynchronize(st));
     const int32_t nm = h_scratch[0];
+    const int32_t nmoves = h_scratch[2];
     stats.passes += 1;
     stats.movers += nm;
-    if (nm == 0) {
-      if (mode == kCut) break;
-      continue;
+    stats.moves += nmoves;
+    stats.decide_iters += 1;
+    if (trace) {
+      const double ms =
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_pass0).count();
+      std::fprintf(stderr, "refine n=%d m=%lld k=%d pass=%d mode=%d movers=%d moves=%d ms=%.3f\n", g.n,
+                   (long long)g.m, k, pass, mode, nm, nmoves, ms);
     }
-    a.nm = nm;
-    const int32_t nb = (int32_t)ceil_div(nm, kDecideBlock);
-    idx_t* dfinal = nullptr;
-    Arena::Mark pm = arena.mark();
-    if (nb <= 4 || (int64_t)nb * K > ((int64_t)1 << 24)) {
-      long long* run = arena.alloc<long long>((size_t)K);
-      const int ph = profiler().begin(kProfDecide, st);
-      if (mode == kRepair) k_decide_seq<kRepair><<<1, kDecideBlock, 0, st>>>(a, d_a, run);
-      else k_decide_seq<kCut><<<1, kDecideBlock, 0, st>>>(a, d_a, run);
-      RMB_LAUNCH_CHECK();
-      profiler().end(ph, st, 0.0);
-      dfinal = d_a;
-      stats.decide_iters += 1;
-    } else {
-      int32_t* D = arena.alloc<int32_t>((size_t)nb * K);
-      long long* PD = arena.alloc<long long>((size_t)nb * K);
-      long long* base = arena.alloc<long long>((size_t)nb * K);
-      idx_t* prev = nullptr;
-      idx_t* cur = d_a;
-      const long long* pd_in = nullptr;
-      for (int round = 0; round <= nb; ++round) {
-        RMB_CUDA(cudaMemsetAsync(counters + 1, 0, sizeof(int32_t), st));
-        const int ph = profiler().begin(kProfDecide, st);
-        if (mode == kRepair)
-          k_decide<kRepair><<<nb, kDecideBlock, 0, st>>>(a, pd_in, prev, cur, D, base, counters + 1);
-        else
-          k_decide<kCut><<<nb, kDecideBlock, 0, st>>>(a, pd_in, prev, cur, D, base, counters + 1);
-        RMB_LAUNCH_CHECK();
-        profiler().end(ph, st, 0.0);
-        stats.decide_iters += 1;
-        k_prefix_blocks<<<grid_for(K, 128), 128, 0, st>>>(D, nb, K, PD);
-        RMB_LAUNCH_CHECK();
-        pd_in = PD;
-        if (round >= 1) {
-          RMB_CUDA(cudaMemcpyAsync(h_scratch + 1, counters + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-          RMB_CUDA(cudaStreamSynchronize(st));
-          if (h_scratch[1] == 0) {
-            dfinal = cur;
-            break;
-          }
-        }
-        prev = cur;
-        cur = (cur == d_a) ? d_b : d_a;
-      }
-      if (!dfinal) throw Error(-4, "refinement decisions did not settle");
-    }
-    RMB_CUDA(cudaMemsetAsync(counters + 2, 0, sizeof(int32_t), st));
-    k_apply<<<grid_for(nm, 256), 256, 0, st>>>(nm, movers, dfinal, part, g.vwgt, g.ncon, pw, counters + 2);
-    RMB_LAUNCH_CHECK();
-    RMB_CUDA(cudaMemcpyAsync(h_scratch + 2, counters + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    RMB_CUDA(cudaStreamSynchronize(st));
-    arena.reset_to(pm);
-    stats.moves += h_scratch[2];
-    if (mode == kCut && h_scratch[2] == 0) break;
+    if (mode == kCut && nmoves == 0) break;
   }
   arena.reset_to(mk);
   return stats;

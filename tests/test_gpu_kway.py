@@ -59,15 +59,16 @@ CASES = [
 def test_kway_valid_balanced_and_close_to_reference(rmb, oracle, name, make, k):
     x, a, v, w = make()
     n = len(x) - 1
+    seeds = range(1, 7)
     cuts = []
-    for seed in (1, 2, 3):
+    for seed in seeds:
         opts = greedy_options(seed=seed)
         rc, part, obj = call_c_abi(rmb, x, a, k, vwgt=v, adjwgt=w, options=opts)
         assert rc == 1
         check_partition(oracle, x, a, v, w, part, k, obj)
         cuts.append(obj)
     ref = []
-    for seed in (1, 2, 3):
+    for seed in seeds:
         rc, part, obj = oracle.part_graph_kway(x, a, k, vwgt=v, adjwgt=w, options=greedy_options(seed=seed))
         assert rc == 1
         ref.append(obj)
