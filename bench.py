@@ -202,6 +202,7 @@ def main():
     ap.add_argument("--workload", default="grid3d_128", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -300,18 +301,20 @@ def main():
             raise RuntimeError(f"RMETIS_PartGraphKway returned {rc}")
 
     e2e_steps = args.e2e_steps or max(3, args.steps // 2)
-    for _ in range(2):
-        step_host()
-    e2e_times = []
-    for _ in range(e2e_steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        step_host()
-        e2e_times.append(time.perf_counter() - t0)
-    e2e_local = float(np.mean(e2e_times))
-    assert int(obj.value) == cut_val and bool((hpart.numpy() == dpart.cpu().numpy()).all()), \
-        "host and device entry points disagree"
+    e2e_local = float("nan")
+    if not args.no_e2e:
+        for _ in range(2):
+            step_host()
+        e2e_times = []
+        for _ in range(e2e_steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            step_host()
+            e2e_times.append(time.perf_counter() - t0)
+        e2e_local = float(np.mean(e2e_times))
+        assert int(obj.value) == cut_val and bool((hpart.numpy() == dpart.cpu().numpy()).all()), \
+            "host and device entry points disagree"
 
     if world > 1:
         tt = torch.tensor([ms_local, e2e_local], dtype=torch.float64, device=dev)

@@ -496,6 +496,7 @@ int RMETIS_GPU_GreedyRefine(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t*
     rp.niter = niter;
     rp.feas_max = d_feas;
     rp.over_thr = d_over;
+    rp.collect_stats = stats != nullptr;
     RefineStats rs = greedy_refine(g, d_part, rp, d_heavy, nh, h.E.arena(), h.st(), h.E.host_scratch());
     unsigned long long* acc = h.E.arena().alloc<unsigned long long>(1);
     cut_and_weights(g, d_part, nparts, acc, nullptr, h.st());

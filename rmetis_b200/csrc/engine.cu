@@ -111,30 +111,29 @@ Engine::~Engine() {
 
 void Engine::reset_stats() { profiler().reset(); }
 
-void Engine::thresholds(const std::vector<int32_t>& total, int k, int ncon, const float* tpwgts,
-                        const std::vector<double>& ub, long long* d_feas, long long* d_over, long long* d_grow) {
+void Engine::thresholds(const std::vector<std::vector<int32_t>>& totals, int k, int ncon, const float* tpwgts,
+                        const std::vector<double>& ub, long long* d_thr) {
   const size_t K = (size_t)k * ncon;
-  if (h_thr_cap_ < 3 * K) {
-    if (h_thr_) {
-      RMB_CUDA(cudaStreamSynchronize(stream_));
-      cudaFreeHost(h_thr_);
-    }
-    RMB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_thr_), sizeof(long long) * 3 * K));
-    h_thr_cap_ = 3 * K;
-  }
+  const size_t need = 3 * K * totals.size();
   // The staging buffer may still feed an earlier copy.
   RMB_CUDA(cudaStreamSynchronize(stream_));
-  for (int p = 0; p < k; ++p)
-    for (int c = 0; c < ncon; ++c) {
-      // compute_target_weights (src/graph/mod.rs:392-410), f64
-      const double f = tpwgts ? (double)tpwgts[(size_t)p * ncon + c] : 1.0 / (double)k;
-      const double t = f * (double)total[c];
-      const size_t i = (size_t)p * ncon + c;
-      threshold_values(t, ub[c], &h_thr_[i], &h_thr_[K + i], &h_thr_[2 * K + i]);
-    }
-  RMB_CUDA(cudaMemcpyAsync(d_feas, h_thr_, sizeof(long long) * K, cudaMemcpyHostToDevice, stream_));
-  RMB_CUDA(cudaMemcpyAsync(d_over, h_thr_ + K, sizeof(long long) * K, cudaMemcpyHostToDevice, stream_));
-  RMB_CUDA(cudaMemcpyAsync(d_grow, h_thr_ + 2 * K, sizeof(long long) * K, cudaMemcpyHostToDevice, stream_));
+  if (h_thr_cap_ < need) {
+    if (h_thr_) cudaFreeHost(h_thr_);
+    RMB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_thr_), sizeof(long long) * need));
+    h_thr_cap_ = need;
+  }
+  for (size_t l = 0; l < totals.size(); ++l) {
+    long long* h = h_thr_ + 3 * K * l;
+    for (int p = 0; p < k; ++p)
+      for (int c = 0; c < ncon; ++c) {
+        // compute_target_weights (src/graph/mod.rs:392-410), f64
+        const double f = tpwgts ? (double)tpwgts[(size_t)p * ncon + c] : 1.0 / (double)k;
+        const double t = f * (double)totals[l][c];
+        const size_t i = (size_t)p * ncon + c;
+        threshold_values(t, ub[c], &h[i], &h[K + i], &h[2 * K + i]);
+      }
+  }
+  RMB_CUDA(cudaMemcpyAsync(d_thr, h_thr_, sizeof(long long) * need, cudaMemcpyHostToDevice, stream_));
 }
 
 __global__ void k_random_part(int32_t n, int32_t k, uint64_t seed, idx_t* part) {
@@ -153,9 +152,6 @@ int Engine::partition_kway(const DGraph& g0, int nparts, const float* tpwgts, co
 
   Arena::Mark call_mark = arena_.mark();
   const size_t K = (size_t)k * ncon;
-  long long* d_feas = arena_.alloc<long long>(K);
-  long long* d_over = arena_.alloc<long long>(K);
-  long long* d_grow = arena_.alloc<long long>(K);
   long long* d_tot = arena_.alloc<long long>((size_t)ncon);
   unsigned long long* d_cut = arena_.alloc<unsigned long long>(1);
 
@@ -243,10 +239,20 @@ int Engine::partition_kway(const DGraph& g0, int nparts, const float* tpwgts, co
       return std::vector<int32_t>(ncon, levels[l].n);
     };
 
+    // Thresholds of every level (one upload): [l][feas, over, grow][k][ncon].
+    long long* d_thr = arena_.alloc<long long>(3 * K * (size_t)(L + 1));
+    {
+      std::vector<std::vector<int32_t>> totals;
+      for (int l = 0; l <= L; ++l) totals.push_back(level_total(l));
+      thresholds(totals, k, ncon, tpwgts, ub, d_thr);
+    }
+    auto feas_of = [&](int l) { return d_thr + 3 * K * (size_t)l; };
+    auto over_of = [&](int l) { return d_thr + 3 * K * (size_t)l + K; };
+    long long* d_grow = d_thr + 3 * K * (size_t)L + 2 * K;
+
     // ---- initial partition of the coarsest graph (initial/mod.rs:11-22) ----
     const DGraph& cg = levels.back();
     idx_t* part = arena_.alloc<idx_t>((size_t)cg.n);
-    thresholds(level_total(L), k, ncon, tpwgts, ub, d_feas, d_over, d_grow);
     if (o.iptype == 1) {
       k_random_part<<<grid_for(cg.n, 256), 256, 0, st>>>(cg.n, k, mix64(seed64 ^ 0x52414e44ULL), part);
       RMB_LAUNCH_CHECK();
@@ -288,8 +294,9 @@ int Engine::partition_kway(const DGraph& g0, int nparts, const float* tpwgts, co
     RefineParams rp;
     rp.k = k;
     rp.niter = o.niter;
-    rp.feas_max = d_feas;
-    rp.over_thr = d_over;
+    rp.feas_max = feas_of(L);
+    rp.over_thr = over_of(L);
+    rp.collect_stats = trace != nullptr;
     {
       RefineStats rs = greedy_refine(cg, part, rp, heavy_lists[L], heavy_counts[L], arena_, st, h_scratch_);
       local.refine_passes += rs.passes;
@@ -301,7 +308,8 @@ int Engine::partition_kway(const DGraph& g0, int nparts, const float* tpwgts, co
       idx_t* fpart = arena_.alloc<idx_t>((size_t)fg.n);
       project(fg.n, cmaps[i], part, fpart, st);
       part = fpart;
-      thresholds(level_total(i), k, ncon, tpwgts, ub, d_feas, d_over, d_grow);
+      rp.feas_max = feas_of(i);
+      rp.over_thr = over_of(i);
       RefineStats rs = greedy_refine(fg, part, rp, heavy_lists[i], heavy_counts[i], arena_, st, h_scratch_);
       local.refine_passes += rs.passes;
       local.refine_moves += rs.moves;

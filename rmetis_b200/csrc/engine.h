@@ -68,8 +68,10 @@ class Engine {
   std::mutex mu;
 
  private:
-  void thresholds(const std::vector<int32_t>& total, int k, int ncon, const float* tpwgts,
-                  const std::vector<double>& ub, long long* d_feas, long long* d_over, long long* d_grow);
+  // Thresholds of every level at once: totals[l] per level, written to
+  // d_thr[l][3][k*ncon] (feas, over, grow) with a single upload.
+  void thresholds(const std::vector<std::vector<int32_t>>& totals, int k, int ncon, const float* tpwgts,
+                  const std::vector<double>& ub, long long* d_thr);
 
   struct Timer;
   Arena arena_;

@@ -100,6 +100,7 @@ struct RefineParams {
   int niter = 10;
   const long long* feas_max = nullptr;  // [k][ncon]: feasible iff pw + vw <= feas_max
   const long long* over_thr = nullptr;  // [k][ncon]: overweight iff pw > over_thr
+  bool collect_stats = false;           // read the per-pass counts back (one sync)
 };
 
 struct RefineStats {

@@ -202,7 +202,8 @@ __global__ void k_gain_heavy(const idx_t* __restrict__ xadj, const idx_t* __rest
 constexpr int kInline = 4;          // candidates kept inline in a mover record
 constexpr int kWalkChunk = 256;     // mover records per shared-memory chunk
 constexpr int kWalkThreads = 256;   // warp 0 walks, the other warps stream records
-constexpr int32_t kContended = -2;  // decision not known before the walk
+constexpr int32_t kContended = -2;  // decision not known before the walk (general path)
+constexpr int32_t kFast = -3;       // not known; at most two candidates, cut pass
 constexpr int kWalkSmemParts = 4096;  // [k][ncon] entries kept in shared memory
 
 struct MoverRecs {  // structure of arrays, nm entries each
@@ -285,6 +286,16 @@ __global__ void k_walk_classify(const int32_t* __restrict__ nm_dev, int32_t ncon
         known = kContended;
         break;
       }
+      if (known == kContended) {
+        // Fast path: every candidate with positive gain is among the first two
+        // inline slots (cut pass, no non-adjacent candidate since ig <= 0).
+        int32_t npos = 0;
+        for (int32_t i = 0; i < ne && i < 3; ++i) {
+          const int32_t g = i < kInline ? r.cg[j * kInline + i] : cand_g[s + i];
+          if (g > 0) ++npos;
+        }
+        if (npos <= 2) known = kFast;
+      }
     }
     r.known[j] = known;
   }
@@ -326,21 +337,21 @@ __device__ inline void walk_load(WalkBuf& b, const MoverRecs& r, int32_t j0, int
   }
 }
 
-// The decision of one mover (greedy.rs:64-107 repair, :131-164 cut) against
-// the part weights given by `pwf(p, c)`: candidates in (gain desc, part asc)
-// order = explicit ones with gain above the non-adjacent gain -w_from, then
-// the non-adjacent parts by id, then the explicit ones below it; the first
+// The decision of one mover (greedy.rs:64-107 repair, :131-164 cut) given
+// the part weights `pwf(p, c)`: candidates in (gain desc, part asc) order =
+// explicit ones with gain above the non-adjacent gain -w_from, then the
+// non-adjacent parts by id, then the explicit ones below it; the first
 // feasible candidate with gain above the pass threshold, or -1.
 template <int MODE, typename PW>
-__device__ inline int32_t walk_decide(const WalkBuf& b, int i, int32_t ncon, int32_t k,
-                                      const idx_t* __restrict__ cand_p, const idx_t* __restrict__ cand_g,
-                                      const long long* feas, const long long* over, PW pwf) {
+__device__ __forceinline__ int32_t walk_decide(const WalkBuf& b, int i, int32_t ncon, int32_t k,
+                                               const idx_t* __restrict__ cand_p, const idx_t* __restrict__ cand_g,
+                                               const long long* feas, const long long* over, PW pwf) {
   const int32_t pv = b.pv[i];
   const int32_t* vw = &b.vw[i * kMaxCon];
   if (MODE == kRepair) {
     bool is_over = false;
     for (int c = 0; c < ncon; ++c)
-      if (pwf(pv, c) > over[(int64_t)pv * ncon + c]) is_over = true;
+      if (pwf(pv, c) > over[pv * ncon + c]) is_over = true;
     if (!is_over) return -1;
   }
   const int32_t thr = (MODE == kRepair) ? INT_MIN : 0;
@@ -351,7 +362,7 @@ __device__ inline int32_t walk_decide(const WalkBuf& b, int i, int32_t ncon, int
   auto cgain = [&](int32_t q) { return q < kInline ? b.cg[i * kInline + q] : cand_g[s + q]; };
   auto feasible = [&](int32_t p) {
     for (int c = 0; c < ncon; ++c)
-      if (pwf(p, c) + vw[c] > feas[(int64_t)p * ncon + c]) return false;
+      if (pwf(p, c) + vw[c] > feas[p * ncon + c]) return false;
     return true;
   };
   int32_t q = 0;
@@ -380,15 +391,16 @@ __device__ inline int32_t walk_decide(const WalkBuf& b, int i, int32_t ncon, int
   return -1;
 }
 
-// The walk. Warp 0 takes the movers of a chunk in windows of 32 consecutive
-// movers, one per lane. Every lane decides against the weights at the window
-// start (d0), then again against those weights plus the moves d0 of the lanes
-// before it (d1). Up to the first lane whose d1 differs from d0, every d0 is
-// the sequential decision (by induction from lane 0, which sees exact
-// weights), and that lane's d1 is too; those lanes commit and the next window
-// starts after them. Warps 1.. stream the next chunk meanwhile. The part
-// weights pw, feas and over live in shared memory when [k][ncon] fits.
-template <int MODE>
+// The walk. Warp 0 takes the movers of a chunk in windows of 32, one per
+// lane, and iterates each window to its fixed point: every lane decides
+// against the weights at the window start plus the moves the lanes before it
+// made in the previous round. Lane t is final after t rounds (lane 0 sees the
+// exact weights from the start), so at most 32 rounds, and the fixed point is
+// the sequential result; independent decisions settle in the same round. The
+// window then applies its moves and the next one starts. Warps 1.. stream the
+// next chunk of mover records meanwhile. SMEM: [k][ncon] part weights and
+// thresholds fit in shared memory (else they stay in global memory).
+template <int MODE, bool SMEM>
 __global__ void __launch_bounds__(kWalkThreads) k_walk(const int32_t* __restrict__ nm_dev, MoverRecs r,
                                                        int32_t ncon, int32_t k, const idx_t* __restrict__ cand_p,
                                                        const idx_t* __restrict__ cand_g, long long* __restrict__ pw,
@@ -400,12 +412,11 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const int32_t* __restrict
   __shared__ int32_t win_d[32], win_pv[32], win_vw[32 * kMaxCon];
   const int32_t nm = *nm_dev;
   const int32_t K = k * ncon;
-  const bool in_smem = K <= kWalkSmemParts;
-  long long* spw = in_smem ? sparts : pw;
-  const long long* sfeas = in_smem ? sparts + K : feas_g;
-  const long long* sover = in_smem ? sparts + 2 * K : over_g;
+  long long* spw = SMEM ? sparts : pw;
+  const long long* sfeas = SMEM ? sparts + K : feas_g;
+  const long long* sover = SMEM ? sparts + 2 * K : over_g;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (in_smem) {
+  if (SMEM) {
     for (int32_t x = tid; x < K; x += blockDim.x) {
       sparts[x] = pw[x];
       sparts[K + x] = feas_g[x];
@@ -421,61 +432,221 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const int32_t* __restrict
       const WalkBuf& b = buf[ch & 1];
       const int32_t j0 = ch * kWalkChunk;
       const int32_t cnt = min(kWalkChunk, nm - j0);
-      auto pw_start = [&](int32_t p, int c) { return spw[(int64_t)p * ncon + c]; };
-      int32_t i0 = 0;
-      while (i0 < cnt) {
+      auto pw_start = [&](int32_t p, int c) { return spw[p * ncon + c]; };
+      for (int32_t i0 = 0; i0 < cnt; i0 += 32) {
         const int i = i0 + lane;
         const bool valid = i < cnt;
-        int32_t d0 = -1, pv = -1;
-        if (valid) {
-          pv = b.pv[i];
-          d0 = b.known[i];
-          if (d0 == kContended) d0 = walk_decide<MODE>(b, i, ncon, k, cand_p, cand_g, sfeas, sover, pw_start);
-          for (int c = 0; c < ncon; ++c) win_vw[lane * kMaxCon + c] = b.vw[i * kMaxCon + c];
-        }
-        win_d[lane] = d0;
+        const int32_t known = valid ? b.known[i] : -1;
+        const bool open = valid && (known == kContended || known == kFast);
+        const int32_t pv = valid ? b.pv[i] : -1;
+        for (int c = 0; c < ncon; ++c) win_vw[lane * kMaxCon + c] = valid ? b.vw[i * kMaxCon + c] : 0;
         win_pv[lane] = pv;
-        __syncwarp();
-        int32_t d1 = d0;
-        if (valid && b.known[i] == kContended && lane > 0) {
-          auto pw_prefix = [&](int32_t p, int c) {
-            long long x = spw[(int64_t)p * ncon + c];
-            for (int l = 0; l < lane; ++l) {
-              const int32_t dl = win_d[l];
-              if (dl < 0) continue;
-              if (dl == p) x += win_vw[l * kMaxCon + c];
-              if (win_pv[l] == p) x -= win_vw[l * kMaxCon + c];
-            }
-            return x;
-          };
-          d1 = walk_decide<MODE>(b, i, ncon, k, cand_p, cand_g, sfeas, sover, pw_prefix);
+        int32_t d = open ? walk_decide<MODE>(b, i, ncon, k, cand_p, cand_g, sfeas, sover, pw_start) : known;
+        for (int round = 0; round < 32; ++round) {
+          win_d[lane] = d;
+          __syncwarp();
+          int32_t nd = d;
+          if (open && lane > 0) {
+            auto pw_prefix = [&](int32_t p, int c) {
+              long long x = spw[p * ncon + c];
+              for (int l = 0; l < lane; ++l) {
+                const int32_t dl = win_d[l];
+                if (dl < 0) continue;
+                if (dl == p) x += win_vw[l * kMaxCon + c];
+                if (win_pv[l] == p) x -= win_vw[l * kMaxCon + c];
+              }
+              return x;
+            };
+            nd = walk_decide<MODE>(b, i, ncon, k, cand_p, cand_g, sfeas, sover, pw_prefix);
+          }
+          const bool changed = __any_sync(0xffffffffu, nd != d);
+          d = nd;
+          __syncwarp();
+          if (!changed) break;
         }
-        const unsigned mism = __ballot_sync(0xffffffffu, valid && d1 != d0);
-        const int f = mism ? (__ffs(mism) - 1) : 32;
-        const bool commit = valid && lane <= f;
-        const int32_t d = (lane == f) ? d1 : d0;
-        if (commit) {
+        if (valid) {
           d_out[j0 + i] = d;
           if (d >= 0) {
             for (int c = 0; c < ncon; ++c) {
               const long long w = win_vw[lane * kMaxCon + c];
-              atomicAdd(reinterpret_cast<unsigned long long*>(&spw[(int64_t)pv * ncon + c]),
-                        (unsigned long long)(-w));
-              atomicAdd(reinterpret_cast<unsigned long long*>(&spw[(int64_t)d * ncon + c]), (unsigned long long)w);
+              atomicAdd(reinterpret_cast<unsigned long long*>(&spw[pv * ncon + c]), (unsigned long long)(-w));
+              atomicAdd(reinterpret_cast<unsigned long long*>(&spw[d * ncon + c]), (unsigned long long)w);
             }
           }
         }
-        moves += __popc(__ballot_sync(0xffffffffu, commit && d >= 0));
+        moves += __popc(__ballot_sync(0xffffffffu, valid && d >= 0));
         __syncwarp();
-        i0 += (f < 32) ? f + 1 : 32;
       }
     } else if (ch + 1 < nchunks) {
       walk_load(buf[(ch + 1) & 1], r, (ch + 1) * kWalkChunk, nm, ncon, tid - 32, blockDim.x - 32);
     }
     __syncthreads();
   }
-  if (in_smem)
+  if (SMEM)
     for (int32_t x = tid; x < K; x += blockDim.x) pw[x] = sparts[x];
+  if (tid == 0) *nmoves = moves;
+}
+
+// Register-resident walk for k <= 32*R parts and NC <= 2 constraints. Only
+// warp 0 walks: lane l holds, for parts l, l+32, ..., l+32*(R-1), the slack
+// to the feasibility threshold (feas - pw) and to the overweight threshold
+// (over - pw) in registers. Every lane reads the same mover record, so control
+// flow stays uniform: a move into p is feasible iff w <= slack[p] in p's lane
+// (one compare and one vote), the source is overweight iff its over-slack is
+// negative. Cut-pass movers with at most two positive-gain candidates take a
+// branch-free path (both tests and votes at once, then a select). The other
+// warps stream mover records.
+template <int R, int NC>
+struct PartRegs {
+  long long sl[R][NC];  // feas - pw
+  long long ov[R][NC];  // over - pw
+};
+
+template <int R, int NC>
+__device__ __forceinline__ bool lane_fits(const PartRegs<R, NC>& s, int lane, int32_t p, const int32_t* w) {
+  bool ok = p >= 0 && (p & 31) == lane;
+  const int slot = p >> 5;
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int c = 0; c < NC; ++c) ok = ok && (r != slot || (long long)w[c] <= s.sl[r][c]);
+  return ok;
+}
+
+template <int MODE, int R, int NC>
+__device__ __forceinline__ int32_t reg_decide(const PartRegs<R, NC>& s, int lane, const WalkBuf& b, int i,
+                                              int32_t k, const idx_t* __restrict__ cand_p,
+                                              const idx_t* __restrict__ cand_g, const int32_t* w) {
+  const int32_t pv = b.pv[i];
+  if (MODE == kRepair) {
+    bool over = false;
+    if ((pv & 31) == lane) {
+      const int slot = pv >> 5;
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+          if (r == slot && s.ov[r][c] < 0) over = true;
+    }
+    if (!__any_sync(0xffffffffu, over)) return -1;
+  }
+  const int32_t thr = (MODE == kRepair) ? INT_MIN : 0;
+  const int32_t ne = b.ne[i];
+  const int32_t st = b.coff[i];
+  const int32_t ig = (int32_t)(0u - (uint32_t)b.wf[i]);
+  auto cpart = [&](int32_t q) { return q < kInline ? b.cp[i * kInline + q] : cand_p[st + q]; };
+  auto cgain = [&](int32_t q) { return q < kInline ? b.cg[i * kInline + q] : cand_g[st + q]; };
+  int32_t q = 0;
+  for (; q < ne; ++q) {
+    const int32_t g = cgain(q);
+    if (g <= ig) break;
+    if (g <= thr) return -1;
+    const int32_t p = cpart(q);
+    if (__any_sync(0xffffffffu, lane_fits(s, lane, p, w))) return p;
+  }
+  if (ig > thr) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int32_t p = r * 32 + lane;
+      bool ok = p < k && p != pv;
+      if (ok)
+        for (int32_t e = 0; e < ne; ++e)
+          if (cpart(e) == p) { ok = false; break; }
+#pragma unroll
+      for (int c = 0; c < NC; ++c) ok = ok && (long long)w[c] <= s.sl[r][c];
+      const unsigned m = __ballot_sync(0xffffffffu, ok);
+      if (m) return r * 32 + __ffs(m) - 1;
+    }
+  }
+  for (; q < ne; ++q) {
+    const int32_t g = cgain(q);
+    if (g <= thr) return -1;
+    const int32_t p = cpart(q);
+    if (__any_sync(0xffffffffu, lane_fits(s, lane, p, w))) return p;
+  }
+  return -1;
+}
+
+template <int MODE, int R, int NC>
+__global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __restrict__ nm_dev, MoverRecs r,
+                                                           int32_t k, const idx_t* __restrict__ cand_p,
+                                                           const idx_t* __restrict__ cand_g,
+                                                           long long* __restrict__ pw,
+                                                           const long long* __restrict__ feas_g,
+                                                           const long long* __restrict__ over_g,
+                                                           idx_t* __restrict__ d_out, int32_t* __restrict__ nmoves) {
+  __shared__ WalkBuf buf[2];
+  __shared__ int32_t dbuf[kWalkChunk];
+  const int32_t nm = *nm_dev;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  PartRegs<R, NC> s;
+  if (warp == 0) {
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+      const int32_t p = rr * 32 + lane;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const bool in = p < k;
+        const long long x = in ? pw[p * NC + c] : 0;
+        s.sl[rr][c] = in ? feas_g[p * NC + c] - x : LLONG_MIN / 2;
+        s.ov[rr][c] = in ? over_g[p * NC + c] - x : LLONG_MAX / 2;
+      }
+    }
+  }
+  if (nm > 0) walk_load(buf[0], r, 0, nm, NC, tid, blockDim.x);
+  __syncthreads();
+  int32_t moves = 0;
+  const int32_t nchunks = (int32_t)ceil_div(nm, kWalkChunk);
+  for (int32_t ch = 0; ch < nchunks; ++ch) {
+    const int32_t j0 = ch * kWalkChunk;
+    const int32_t cnt = min(kWalkChunk, nm - j0);
+    if (warp == 0) {
+      const WalkBuf& b = buf[ch & 1];
+      for (int32_t i = 0; i < cnt; ++i) {
+        int32_t w[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) w[c] = b.vw[i * kMaxCon + c];
+        int32_t d = b.known[i];
+        if (MODE == kCut && d == kFast) {
+          const int32_t c1 = b.cg[i * kInline] > 0 ? b.cp[i * kInline] : -1;
+          const int32_t c2 = b.cg[i * kInline + 1] > 0 ? b.cp[i * kInline + 1] : -1;
+          const bool f1 = __any_sync(0xffffffffu, lane_fits(s, lane, c1, w));
+          const bool f2 = __any_sync(0xffffffffu, lane_fits(s, lane, c2, w));
+          d = f1 ? c1 : (f2 ? c2 : -1);
+        } else if (d == kContended || d == kFast) {
+          d = reg_decide<MODE, R, NC>(s, lane, b, i, k, cand_p, cand_g, w);
+        }
+        if (lane == 0) dbuf[i] = d;
+        if (d >= 0) {
+          const int32_t pv = b.pv[i];
+#pragma unroll
+          for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              const long long dw = (long long)w[c];
+              const long long delta = (pv == rr * 32 + lane ? dw : 0) - (d == rr * 32 + lane ? dw : 0);
+              s.sl[rr][c] += delta;
+              s.ov[rr][c] += delta;
+            }
+          ++moves;
+        }
+      }
+      __syncwarp();
+      for (int32_t i = lane; i < cnt; i += 32) d_out[j0 + i] = dbuf[i];
+    } else if (ch + 1 < nchunks) {
+      walk_load(buf[(ch + 1) & 1], r, (ch + 1) * kWalkChunk, nm, NC, tid - 32, blockDim.x - 32);
+    }
+    __syncthreads();
+  }
+  if (warp == 0) {
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+      const int32_t p = rr * 32 + lane;
+      if (p < k)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) pw[p * NC + c] = feas_g[p * NC + c] - s.sl[rr][c];
+    }
+  }
   if (tid == 0) *nmoves = moves;
 }
 
@@ -549,11 +720,37 @@ static void launch_walk(int32_t nmax, const int32_t* nm_dev, const idx_t* movers
     k_walk_classify<<<blocks, 256, 0, st>>>(nm_dev, g.ncon, cand_p, cand_g, r, pw, feas, in_max, out_max);
     RMB_LAUNCH_CHECK();
   }
-  const size_t smem = K <= kWalkSmemParts ? sizeof(long long) * 3 * (size_t)K : 0;
-  RMB_CUDA(cudaFuncSetAttribute(k_walk<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(sizeof(long long) * 3 * kWalkSmemParts)));
   const int ph = profiler().begin(kProfDecide, st);
-  k_walk<MODE><<<1, kWalkThreads, smem, st>>>(nm_dev, r, g.ncon, k, cand_p, cand_g, pw, feas, over, d_out, nmoves);
+  const int ncon = g.ncon;
+#define RMB_WALK_REG(RR, NCC) \
+  k_walk_reg<MODE, RR, NCC><<<1, kWalkThreads, 0, st>>>(nm_dev, r, k, cand_p, cand_g, pw, feas, over, d_out, nmoves)
+  if (ncon <= 2 && k <= 256) {
+    const int rr = k <= 32 ? 1 : k <= 64 ? 2 : k <= 128 ? 4 : 8;
+    if (ncon == 1) {
+      if (rr == 1) RMB_WALK_REG(1, 1); else if (rr == 2) RMB_WALK_REG(2, 1);
+      else if (rr == 4) RMB_WALK_REG(4, 1); else RMB_WALK_REG(8, 1);
+    } else {
+      if (rr == 1) RMB_WALK_REG(1, 2); else if (rr == 2) RMB_WALK_REG(2, 2);
+      else if (rr == 4) RMB_WALK_REG(4, 2); else RMB_WALK_REG(8, 2);
+    }
+#undef RMB_WALK_REG
+  } else if (K <= kWalkSmemParts) {
+    static thread_local int attr_device = -1;  // attribute set on this device already
+    int dev = 0;
+    RMB_CUDA(cudaGetDevice(&dev));
+    if (attr_device != dev) {
+      RMB_CUDA(cudaFuncSetAttribute(k_walk<kRepair, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(sizeof(long long) * 3 * kWalkSmemParts)));
+      RMB_CUDA(cudaFuncSetAttribute(k_walk<kCut, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(sizeof(long long) * 3 * kWalkSmemParts)));
+      attr_device = dev;
+    }
+    k_walk<MODE, true><<<1, kWalkThreads, sizeof(long long) * 3 * (size_t)K, st>>>(
+        nm_dev, r, g.ncon, k, cand_p, cand_g, pw, feas, over, d_out, nmoves);
+  } else {
+    k_walk<MODE, false><<<1, kWalkThreads, 0, st>>>(nm_dev, r, g.ncon, k, cand_p, cand_g, pw, feas, over, d_out,
+                                                   nmoves);
+  }
   RMB_LAUNCH_CHECK();
   profiler().end(ph, st, 0.0);
   k_apply<<<blocks, 256, 0, st>>>(nm_dev, movers, d_out, const_cast<idx_t*>(part));
@@ -577,7 +774,8 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
   idx_t* cand_g = arena.alloc<idx_t>((size_t)g.m + 1);
   idx_t* movers = arena.alloc<idx_t>((size_t)g.n);
   idx_t* dec = arena.alloc<idx_t>((size_t)g.n);
-  int32_t* counters = arena.alloc<int32_t>(8);  // [0] nm, [2] moves
+  // Per pass: [2*pass] movers, [2*pass+1] moves.
+  int32_t* counters = arena.alloc<int32_t>(2 * ((size_t)rp.niter + 1));
   MoverRecs r;
   r.pv = arena.alloc<int32_t>((size_t)g.n);
   r.ne = arena.alloc<int32_t>((size_t)g.n);
@@ -590,36 +788,42 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
   int32_t* ghist = (nheavy > 0 && k > kGainHist) ? arena.alloc<int32_t>((size_t)k * 256 * 4) : nullptr;
   partition_weights_only(g, part, k, pw, st);
 
-  static const bool trace = std::getenv("RMETIS_B200_TRACE") != nullptr;
+  // The reference stops the cut passes at the first pass without a move
+  // (greedy.rs:184-186). Such a pass leaves part and pw unchanged, so every
+  // later pass would again find the same movers and make no move: running all
+  // niter passes gives the same result, and the whole level is queued without
+  // waiting for the host.
   for (int pass = 0; pass <= rp.niter; ++pass) {
     const int mode = pass == 0 ? kRepair : kCut;
-    const auto t_pass0 = std::chrono::steady_clock::now();
+    int32_t* nm_dev = counters + 2 * pass;
     if (mode == kRepair)
       launch_gain<kRepair>(g, part, k, pw, rp.over_thr, mover, ncand, wfrom, cand_p, cand_g, heavy, nheavy, ghist, st);
     else
       launch_gain<kCut>(g, part, k, pw, rp.over_thr, mover, ncand, wfrom, cand_p, cand_g, heavy, nheavy, ghist, st);
-    compact_flags(mover, g.n, movers, counters, arena, st);
+    compact_flags(mover, g.n, movers, nm_dev, arena, st);
     if (mode == kRepair)
-      launch_walk<kRepair>(g.n, counters, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r, pw, rp.feas_max,
-                           rp.over_thr, in_max, out_max, dec, counters + 2, st);
+      launch_walk<kRepair>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r, pw, rp.feas_max,
+                           rp.over_thr, in_max, out_max, dec, nm_dev + 1, st);
     else
-      launch_walk<kCut>(g.n, counters, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r, pw, rp.feas_max,
-                        rp.over_thr, in_max, out_max, dec, counters + 2, st);
-    RMB_CUDA(cudaMemcpyAsync(h_scratch, counters, 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+      launch_walk<kCut>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r, pw, rp.feas_max,
+                        rp.over_thr, in_max, out_max, dec, nm_dev + 1, st);
+  }
+  static const bool trace = std::getenv("RMETIS_B200_TRACE") != nullptr;
+  if (trace || rp.collect_stats) {
+    RMB_CUDA(cudaMemcpyAsync(h_scratch, counters, sizeof(int32_t) * 2 * ((size_t)rp.niter + 1),
+                             cudaMemcpyDeviceToHost, st));
     RMB_CUDA(cudaStreamSynchronize(st));
-    const int32_t nm = h_scratch[0];
-    const int32_t nmoves = h_scratch[2];
-    stats.passes += 1;
-    stats.movers += nm;
-    stats.moves += nmoves;
-    stats.decide_iters += 1;
-    if (trace) {
-      const double ms =
-          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_pass0).count();
-      std::fprintf(stderr, "refine n=%d m=%lld k=%d pass=%d mode=%d movers=%d moves=%d ms=%.3f\n", g.n,
-                   (long long)g.m, k, pass, mode, nm, nmoves, ms);
+    for (int pass = 0; pass <= rp.niter; ++pass) {
+      const int32_t nm = h_scratch[2 * pass], nmoves = h_scratch[2 * pass + 1];
+      stats.passes += 1;
+      stats.movers += nm;
+      stats.moves += nmoves;
+      stats.decide_iters += 1;
+      if (trace)
+        std::fprintf(stderr, "refine n=%d m=%lld k=%d pass=%d mode=%d movers=%d moves=%d\n", g.n, (long long)g.m, k,
+                     pass, pass == 0 ? 0 : 1, nm, nmoves);
+      if (pass > 0 && nmoves == 0) break;
     }
-    if (mode == kCut && nmoves == 0) break;
   }
   arena.reset_to(mk);
   return stats;
