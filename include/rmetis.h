@@ -176,6 +176,29 @@ RMETIS_API int RMETIS_GPU_GreedyRefine(idx_t n, idx_t ncon, const idx_t *xadj, c
                             const idx_t *adjwgt, idx_t *part, idx_t nparts, const double *targets,
                             const double *ubvec, idx_t niter, idx_t *cut, int64_t *stats);
 
+/* Edge cut and partition weights of a device-resident graph without any
+ * allocation, for callers that cannot allocate device memory at the point of
+ * the call (while recording a CUDA graph, under a host-owned fixed memory
+ * budget, or in a loop that must not synchronise the device). No counterpart
+ * in the reference: it is an additive variant of RMETIS_GPU_EdgeCut plus
+ * RMETIS_GPU_PartitionWeights.
+ * Inputs and outputs are device pointers on the current device: d_xadj[n+1],
+ * d_adjncy/d_adjwgt[nnz] (d_adjwgt and d_vwgt may be NULL for unit weights),
+ * d_part[n]; outputs *d_cut and d_pw[nparts*ncon]. The work is queued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream) and the call returns
+ * without waiting; outputs are ready once that stream has reached them.
+ * Scratch is a fixed array in device memory of the library (about 128 KiB per
+ * GPU, kept until exit): nparts*ncon above 16384 returns METIS_ERROR_INPUT with
+ * a message on stderr. The first call on a device looks up that array's device
+ * address, so make it before any stream capture. All calls share the array and
+ * each clears it first: calls that overlap on the GPU race and must be
+ * serialised by the caller. Out-of-range indices are skipped and make
+ * *d_cut = -1. */
+RMETIS_API int RMETIS_GPU_EdgeCutWeightsNoAlloc(idx_t n, idx_t ncon, int64_t nnz, const idx_t *d_xadj,
+                                                const idx_t *d_adjncy, const idx_t *d_adjwgt, const idx_t *d_vwgt,
+                                                const idx_t *d_part, idx_t nparts, idx_t *d_cut, idx_t *d_pw,
+                                                void *stream);
+
 #ifdef __cplusplus
 }
 #endif
