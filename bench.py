@@ -327,7 +327,7 @@ def main():
         value = world * m / (ms_max / 1000.0)
         e2e_value = world * m / e2e_max
         peak, peak_kind = load_peaks()
-        names = ["k_gain", "k_decide", "k_match_propose", "k_contract_thread", "k_cut", "k_grow"]
+        names = ["k_gain", "k_walk", "k_match_propose", "k_contract_thread", "k_cut", "k_grow"]
         dom = max(range(nprof), key=lambda i: ms_k[i] if bytes_k[i] > 0 else -1.0)
         avg_ms = ms_k[dom] / max(1, launches[dom])
         avg_bytes = bytes_k[dom] / max(1, launches[dom])

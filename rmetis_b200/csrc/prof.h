@@ -30,6 +30,11 @@ class Profiler {
   bool on = false;
   int begin(int id, cudaStream_t st);
   void end(int handle, cudaStream_t st, double bytes);
+  // Sets the algorithmic bytes of a recorded launch after the fact (for
+  // launches whose size is only known on the device when they are queued).
+  void set_bytes(int handle, double bytes) {
+    if (handle >= 0 && handle < (int)recs_.size()) recs_[handle].bytes = bytes;
+  }
   // Synchronises on the recorded events and adds them to the totals.
   void collect();
   void reset();

@@ -18,6 +18,7 @@
 // happens first, or that stays infeasible even if every potential move out
 // of it happens first (k_walk_classify). The walker only evaluates the rest.
 #include <chrono>
+#include <vector>
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
@@ -703,7 +704,7 @@ void gain_table(const DGraph& g, const idx_t* part, int k, idx_t* boundary, idx_
 }
 
 template <int MODE>
-static void launch_walk(int32_t nmax, const int32_t* nm_dev, const idx_t* movers, const DGraph& g, const idx_t* part,
+static int launch_walk(int32_t nmax, const int32_t* nm_dev, const idx_t* movers, const DGraph& g, const idx_t* part,
                         int k, const idx_t* ncand, const idx_t* wfrom, const idx_t* cand_p, const idx_t* cand_g,
                         const MoverRecs& r, long long* pw, const long long* feas, const long long* over,
                         long long* in_max, long long* out_max, idx_t* d_out, int32_t* nmoves, cudaStream_t st) {
@@ -755,6 +756,7 @@ static void launch_walk(int32_t nmax, const int32_t* nm_dev, const idx_t* movers
   profiler().end(ph, st, 0.0);
   k_apply<<<blocks, 256, 0, st>>>(nm_dev, movers, d_out, const_cast<idx_t*>(part));
   RMB_LAUNCH_CHECK();
+  return ph;
 }
 
 RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, const idx_t* heavy, int32_t nheavy,
@@ -793,6 +795,7 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
   // later pass would again find the same movers and make no move: running all
   // niter passes gives the same result, and the whole level is queued without
   // waiting for the host.
+  std::vector<int> walk_handles;
   for (int pass = 0; pass <= rp.niter; ++pass) {
     const int mode = pass == 0 ? kRepair : kCut;
     int32_t* nm_dev = counters + 2 * pass;
@@ -802,13 +805,23 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
       launch_gain<kCut>(g, part, k, pw, rp.over_thr, mover, ncand, wfrom, cand_p, cand_g, heavy, nheavy, ghist, st);
     compact_flags(mover, g.n, movers, nm_dev, arena, st);
     if (mode == kRepair)
-      launch_walk<kRepair>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r, pw, rp.feas_max,
-                           rp.over_thr, in_max, out_max, dec, nm_dev + 1, st);
+      walk_handles.push_back(launch_walk<kRepair>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r,
+                                                  pw, rp.feas_max, rp.over_thr, in_max, out_max, dec, nm_dev + 1, st));
     else
-      launch_walk<kCut>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r, pw, rp.feas_max,
-                        rp.over_thr, in_max, out_max, dec, nm_dev + 1, st);
+      walk_handles.push_back(launch_walk<kCut>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r, pw,
+                                               rp.feas_max, rp.over_thr, in_max, out_max, dec, nm_dev + 1, st));
   }
   static const bool trace = std::getenv("RMETIS_B200_TRACE") != nullptr;
+  if (profiler().on) {
+    // The walk reads one record per mover (pv, ne, w_from, offset, known,
+    // 4 inline candidates and gains, ncon weights) and writes its decision.
+    RMB_CUDA(cudaMemcpyAsync(h_scratch, counters, sizeof(int32_t) * 2 * ((size_t)rp.niter + 1),
+                             cudaMemcpyDeviceToHost, st));
+    RMB_CUDA(cudaStreamSynchronize(st));
+    const double rec_bytes = 4.0 * (5 + 2 * kInline + g.ncon) + 4.0;
+    for (int pass = 0; pass <= rp.niter; ++pass)
+      profiler().set_bytes(walk_handles[pass], rec_bytes * h_scratch[2 * pass]);
+  }
   if (trace || rp.collect_stats) {
     RMB_CUDA(cudaMemcpyAsync(h_scratch, counters, sizeof(int32_t) * 2 * ((size_t)rp.niter + 1),
                              cudaMemcpyDeviceToHost, st));
