@@ -497,6 +497,12 @@ int RMETIS_GPU_GreedyRefine(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t*
     rp.feas_max = d_feas;
     rp.over_thr = d_over;
     rp.collect_stats = stats != nullptr;
+    {
+      std::vector<long long> tot(ncon, 0);
+      for (int64_t v = 0; v < n; ++v)
+        for (int c = 0; c < ncon; ++c) tot[c] += vwgt ? vwgt[v * ncon + c] : 1;
+      rp.small_weights = weights_fit_int32(tot.data(), ncon, feas.data(), over.data(), K);
+    }
     RefineStats rs = greedy_refine(g, d_part, rp, d_heavy, nh, h.E.arena(), h.st(), h.E.host_scratch());
     unsigned long long* acc = h.E.arena().alloc<unsigned long long>(1);
     cut_and_weights(g, d_part, nparts, acc, nullptr, h.st());

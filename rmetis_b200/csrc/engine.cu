@@ -246,6 +246,14 @@ int Engine::partition_kway(const DGraph& g0, int nparts, const float* tpwgts, co
       for (int l = 0; l <= L; ++l) totals.push_back(level_total(l));
       thresholds(totals, k, ncon, tpwgts, ub, d_thr);
     }
+    // Host copy of the thresholds (still in the staging buffer) decides
+    // whether each level's walk can keep 32-bit slacks.
+    std::vector<bool> small(L + 1);
+    for (int l = 0; l <= L; ++l) {
+      std::vector<long long> tot;
+      for (int32_t t : level_total(l)) tot.push_back(t);
+      small[l] = weights_fit_int32(tot.data(), ncon, h_thr_ + 3 * K * (size_t)l, h_thr_ + 3 * K * (size_t)l + K, K);
+    }
     auto feas_of = [&](int l) { return d_thr + 3 * K * (size_t)l; };
     auto over_of = [&](int l) { return d_thr + 3 * K * (size_t)l + K; };
     long long* d_grow = d_thr + 3 * K * (size_t)L + 2 * K;
@@ -296,6 +304,7 @@ int Engine::partition_kway(const DGraph& g0, int nparts, const float* tpwgts, co
     rp.niter = o.niter;
     rp.feas_max = feas_of(L);
     rp.over_thr = over_of(L);
+    rp.small_weights = small[L];
     rp.collect_stats = trace != nullptr;
     {
       RefineStats rs = greedy_refine(cg, part, rp, heavy_lists[L], heavy_counts[L], arena_, st, h_scratch_);
@@ -310,6 +319,7 @@ int Engine::partition_kway(const DGraph& g0, int nparts, const float* tpwgts, co
       part = fpart;
       rp.feas_max = feas_of(i);
       rp.over_thr = over_of(i);
+      rp.small_weights = small[i];
       RefineStats rs = greedy_refine(fg, part, rp, heavy_lists[i], heavy_counts[i], arena_, st, h_scratch_);
       local.refine_passes += rs.passes;
       local.refine_moves += rs.moves;

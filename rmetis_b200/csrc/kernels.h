@@ -101,7 +101,22 @@ struct RefineParams {
   const long long* feas_max = nullptr;  // [k][ncon]: feasible iff pw + vw <= feas_max
   const long long* over_thr = nullptr;  // [k][ncon]: overweight iff pw > over_thr
   bool collect_stats = false;           // read the per-pass counts back (one sync)
+  // Set when every part weight (|pw| <= total < 2^28) and every threshold
+  // (|feas|, |over| < 2^29) is small: the walk may then keep 32-bit slacks.
+  bool small_weights = false;
 };
+
+// True when the totals and thresholds allow 32-bit slacks in the walk.
+inline bool weights_fit_int32(const long long* total, int ncon, const long long* feas, const long long* over,
+                              size_t K) {
+  for (int c = 0; c < ncon; ++c)
+    if (total[c] < 0 || total[c] >= (1LL << 28)) return false;
+  for (size_t i = 0; i < K; ++i) {
+    const long long lim = 1LL << 29;
+    if (feas[i] <= -lim || feas[i] >= lim || over[i] <= -lim || over[i] >= lim) return false;
+  }
+  return true;
+}
 
 struct RefineStats {
   int passes = 0;

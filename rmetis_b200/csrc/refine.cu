@@ -497,25 +497,25 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const int32_t* __restrict
 // negative. Cut-pass movers with at most two positive-gain candidates take a
 // branch-free path (both tests and votes at once, then a select). The other
 // warps stream mover records.
-template <int R, int NC>
+template <typename S, int R, int NC>
 struct PartRegs {
-  long long sl[R][NC];  // feas - pw
-  long long ov[R][NC];  // over - pw
+  S sl[R][NC];  // feas - pw
+  S ov[R][NC];  // over - pw
 };
 
-template <int R, int NC>
-__device__ __forceinline__ bool lane_fits(const PartRegs<R, NC>& s, int lane, int32_t p, const int32_t* w) {
+template <typename S, int R, int NC>
+__device__ __forceinline__ bool lane_fits(const PartRegs<S, R, NC>& s, int lane, int32_t p, const int32_t* w) {
   bool ok = p >= 0 && (p & 31) == lane;
   const int slot = p >> 5;
 #pragma unroll
   for (int r = 0; r < R; ++r)
 #pragma unroll
-    for (int c = 0; c < NC; ++c) ok = ok && (r != slot || (long long)w[c] <= s.sl[r][c]);
+    for (int c = 0; c < NC; ++c) ok = ok && (r != slot || (S)w[c] <= s.sl[r][c]);
   return ok;
 }
 
-template <int MODE, int R, int NC>
-__device__ __forceinline__ int32_t reg_decide(const PartRegs<R, NC>& s, int lane, const WalkBuf& b, int i,
+template <int MODE, typename S, int R, int NC>
+__device__ __forceinline__ int32_t reg_decide(const PartRegs<S, R, NC>& s, int lane, const WalkBuf& b, int i,
                                               int32_t k, const idx_t* __restrict__ cand_p,
                                               const idx_t* __restrict__ cand_g, const int32_t* w) {
   const int32_t pv = b.pv[i];
@@ -554,7 +554,7 @@ __device__ __forceinline__ int32_t reg_decide(const PartRegs<R, NC>& s, int lane
         for (int32_t e = 0; e < ne; ++e)
           if (cpart(e) == p) { ok = false; break; }
 #pragma unroll
-      for (int c = 0; c < NC; ++c) ok = ok && (long long)w[c] <= s.sl[r][c];
+      for (int c = 0; c < NC; ++c) ok = ok && (S)w[c] <= s.sl[r][c];
       const unsigned m = __ballot_sync(0xffffffffu, ok);
       if (m) return r * 32 + __ffs(m) - 1;
     }
@@ -568,7 +568,18 @@ __device__ __forceinline__ int32_t reg_decide(const PartRegs<R, NC>& s, int lane
   return -1;
 }
 
-template <int MODE, int R, int NC>
+// Register-resident walk for k <= 32*R parts and NC <= 2 constraints. Only
+// warp 0 walks: lane l holds, for parts l, l+32, ..., l+32*(R-1), the slack
+// to the feasibility threshold (feas - pw) and to the overweight threshold
+// (over - pw) in registers, as S (int32 when the host has checked that every
+// weight and threshold fits with margin, else int64). Every lane reads the
+// same mover record, so control flow stays uniform: a move into p is feasible
+// iff w <= slack[p] in p's lane (one compare and one vote), the source is
+// overweight iff its over-slack is negative. Cut-pass movers with at most two
+// positive-gain candidates take a branch-free path (both tests and votes at
+// once, then a select) and their record is fetched one mover ahead. The other
+// warps stream mover records.
+template <int MODE, typename S, int R, int NC>
 __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __restrict__ nm_dev, MoverRecs r,
                                                            int32_t k, const idx_t* __restrict__ cand_p,
                                                            const idx_t* __restrict__ cand_g,
@@ -580,7 +591,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
   __shared__ int32_t dbuf[kWalkChunk];
   const int32_t nm = *nm_dev;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  PartRegs<R, NC> s;
+  PartRegs<S, R, NC> s;
   if (warp == 0) {
 #pragma unroll
     for (int rr = 0; rr < R; ++rr) {
@@ -589,8 +600,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
       for (int c = 0; c < NC; ++c) {
         const bool in = p < k;
         const long long x = in ? pw[p * NC + c] : 0;
-        s.sl[rr][c] = in ? feas_g[p * NC + c] - x : LLONG_MIN / 2;
-        s.ov[rr][c] = in ? over_g[p * NC + c] - x : LLONG_MAX / 2;
+        // Parts beyond k are never feasible and never overweight.
+        s.sl[rr][c] = in ? (S)(feas_g[p * NC + c] - x) : (S)(-(1 << 30));
+        s.ov[rr][c] = in ? (S)(over_g[p * NC + c] - x) : (S)(1 << 30);
       }
     }
   }
@@ -603,29 +615,40 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
     const int32_t cnt = min(kWalkChunk, nm - j0);
     if (warp == 0) {
       const WalkBuf& b = buf[ch & 1];
+      auto c_of = [&](int i, int q) { return b.cg[i * kInline + q] > 0 ? b.cp[i * kInline + q] : -1; };
+      int32_t nk = b.known[0], npv = b.pv[0], nc1 = c_of(0, 0), nc2 = c_of(0, 1);
+      int32_t nw[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) nw[c] = b.vw[c];
       for (int32_t i = 0; i < cnt; ++i) {
+        const int32_t kn = nk, pv = npv, c1 = nc1, c2 = nc2;
         int32_t w[NC];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) w[c] = b.vw[i * kMaxCon + c];
-        int32_t d = b.known[i];
-        if (MODE == kCut && d == kFast) {
-          const int32_t c1 = b.cg[i * kInline] > 0 ? b.cp[i * kInline] : -1;
-          const int32_t c2 = b.cg[i * kInline + 1] > 0 ? b.cp[i * kInline + 1] : -1;
+        for (int c = 0; c < NC; ++c) w[c] = nw[c];
+        if (i + 1 < cnt) {
+          nk = b.known[i + 1];
+          npv = b.pv[i + 1];
+          nc1 = c_of(i + 1, 0);
+          nc2 = c_of(i + 1, 1);
+#pragma unroll
+          for (int c = 0; c < NC; ++c) nw[c] = b.vw[(i + 1) * kMaxCon + c];
+        }
+        int32_t d = kn;
+        if (MODE == kCut && kn == kFast) {
           const bool f1 = __any_sync(0xffffffffu, lane_fits(s, lane, c1, w));
           const bool f2 = __any_sync(0xffffffffu, lane_fits(s, lane, c2, w));
           d = f1 ? c1 : (f2 ? c2 : -1);
-        } else if (d == kContended || d == kFast) {
-          d = reg_decide<MODE, R, NC>(s, lane, b, i, k, cand_p, cand_g, w);
+        } else if (kn == kContended || kn == kFast) {
+          d = reg_decide<MODE, S, R, NC>(s, lane, b, i, k, cand_p, cand_g, w);
         }
         if (lane == 0) dbuf[i] = d;
         if (d >= 0) {
-          const int32_t pv = b.pv[i];
 #pragma unroll
           for (int rr = 0; rr < R; ++rr)
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
-              const long long dw = (long long)w[c];
-              const long long delta = (pv == rr * 32 + lane ? dw : 0) - (d == rr * 32 + lane ? dw : 0);
+              const S dw = (S)w[c];
+              const S delta = (pv == rr * 32 + lane ? dw : (S)0) - (d == rr * 32 + lane ? dw : (S)0);
               s.sl[rr][c] += delta;
               s.ov[rr][c] += delta;
             }
@@ -645,7 +668,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
       const int32_t p = rr * 32 + lane;
       if (p < k)
 #pragma unroll
-        for (int c = 0; c < NC; ++c) pw[p * NC + c] = feas_g[p * NC + c] - s.sl[rr][c];
+        for (int c = 0; c < NC; ++c) pw[p * NC + c] = feas_g[p * NC + c] - (long long)s.sl[rr][c];
     }
   }
   if (tid == 0) *nmoves = moves;
@@ -707,7 +730,8 @@ template <int MODE>
 static int launch_walk(int32_t nmax, const int32_t* nm_dev, const idx_t* movers, const DGraph& g, const idx_t* part,
                         int k, const idx_t* ncand, const idx_t* wfrom, const idx_t* cand_p, const idx_t* cand_g,
                         const MoverRecs& r, long long* pw, const long long* feas, const long long* over,
-                        long long* in_max, long long* out_max, idx_t* d_out, int32_t* nmoves, cudaStream_t st) {
+                        long long* in_max, long long* out_max, idx_t* d_out, int32_t* nmoves, bool small_weights,
+                        cudaStream_t st) {
   const int32_t K = k * g.ncon;
   const int blocks = grid_for(nmax, 256);
   if (MODE == kCut) {
@@ -723,17 +747,24 @@ static int launch_walk(int32_t nmax, const int32_t* nm_dev, const idx_t* movers,
   }
   const int ph = profiler().begin(kProfDecide, st);
   const int ncon = g.ncon;
-#define RMB_WALK_REG(RR, NCC) \
-  k_walk_reg<MODE, RR, NCC><<<1, kWalkThreads, 0, st>>>(nm_dev, r, k, cand_p, cand_g, pw, feas, over, d_out, nmoves)
+#define RMB_WALK_REG(ST, RR, NCC)                                                                     \
+  k_walk_reg<MODE, ST, RR, NCC><<<1, kWalkThreads, 0, st>>>(nm_dev, r, k, cand_p, cand_g, pw, feas, over, d_out, \
+                                                            nmoves)
+#define RMB_WALK_REG_R(ST, NCC)                       \
+  do {                                                \
+    if (rr == 1) RMB_WALK_REG(ST, 1, NCC);            \
+    else if (rr == 2) RMB_WALK_REG(ST, 2, NCC);       \
+    else if (rr == 4) RMB_WALK_REG(ST, 4, NCC);       \
+    else RMB_WALK_REG(ST, 8, NCC);                    \
+  } while (0)
   if (ncon <= 2 && k <= 256) {
     const int rr = k <= 32 ? 1 : k <= 64 ? 2 : k <= 128 ? 4 : 8;
-    if (ncon == 1) {
-      if (rr == 1) RMB_WALK_REG(1, 1); else if (rr == 2) RMB_WALK_REG(2, 1);
-      else if (rr == 4) RMB_WALK_REG(4, 1); else RMB_WALK_REG(8, 1);
+    if (small_weights) {
+      if (ncon == 1) RMB_WALK_REG_R(int32_t, 1); else RMB_WALK_REG_R(int32_t, 2);
     } else {
-      if (rr == 1) RMB_WALK_REG(1, 2); else if (rr == 2) RMB_WALK_REG(2, 2);
-      else if (rr == 4) RMB_WALK_REG(4, 2); else RMB_WALK_REG(8, 2);
+      if (ncon == 1) RMB_WALK_REG_R(long long, 1); else RMB_WALK_REG_R(long long, 2);
     }
+#undef RMB_WALK_REG_R
 #undef RMB_WALK_REG
   } else if (K <= kWalkSmemParts) {
     static thread_local int attr_device = -1;  // attribute set on this device already
@@ -806,10 +837,12 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
     compact_flags(mover, g.n, movers, nm_dev, arena, st);
     if (mode == kRepair)
       walk_handles.push_back(launch_walk<kRepair>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r,
-                                                  pw, rp.feas_max, rp.over_thr, in_max, out_max, dec, nm_dev + 1, st));
+                                                  pw, rp.feas_max, rp.over_thr, in_max, out_max, dec, nm_dev + 1,
+                                                  rp.small_weights, st));
     else
       walk_handles.push_back(launch_walk<kCut>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r, pw,
-                                               rp.feas_max, rp.over_thr, in_max, out_max, dec, nm_dev + 1, st));
+                                               rp.feas_max, rp.over_thr, in_max, out_max, dec, nm_dev + 1,
+                                               rp.small_weights, st));
   }
   static const bool trace = std::getenv("RMETIS_B200_TRACE") != nullptr;
   if (profiler().on) {

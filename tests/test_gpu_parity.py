@@ -285,3 +285,14 @@ def test_pipeline_replay_bit_exact(rmb, oracle):
         assert rc == 1
         assert obj == res.objval
         assert (part == res.part).all()
+
+
+def test_greedy_refine_large_weights(rmb, oracle):
+    """Totals above 2^28 take the 64-bit slack path of the walk."""
+    x, a, _, w = G.grid3d(14, 12, 10, weights_seed=4)
+    n = len(x) - 1
+    v = np.random.default_rng(5).integers(200_000, 400_000, n).astype(np.int32)
+    assert v.astype(np.int64).sum() > (1 << 28)
+    k = 9
+    part = np.random.default_rng(6).integers(0, k, n).astype(np.int32)
+    _refine_case(rmb, oracle, x, a, v, w, part, k, [1.03])
