@@ -514,10 +514,73 @@ __device__ __forceinline__ bool lane_fits(const PartRegs<S, R, NC>& s, int lane,
   return ok;
 }
 
+// Whether a move of weight w into part p (each lane its own p; p < 0 never)
+// fits: the slack of p sits in lane p & 31, slot p >> 5, so every lane
+// gathers the slacks of its p with one shuffle per slot. All lanes call it.
+template <typename S, int R, int NC>
+__device__ __forceinline__ bool gather_fits(const PartRegs<S, R, NC>& s, int32_t p, const int32_t* w) {
+  const int src = p & 31, slot = p >> 5;
+  bool ok = p >= 0;
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const S x = __shfl_sync(0xffffffffu, s.sl[r][c], src);
+      if (slot == r && (S)w[c] > x) ok = false;
+    }
+  return ok;
+}
+
+// Explicit candidates q0.. of one mover, 32 at a time: lane t takes
+// candidate q0 + t (coalesced loads), and the first lane in candidate order
+// whose candidate ends the scan decides. The scan ends at a candidate whose
+// gain is <= stop_gain (returns -2 - q: the caller goes on elsewhere from q),
+// at one whose gain is <= thr (returns -1), or at a feasible one (returns its
+// part); running out returns -2 - ne.
+template <typename S, int R, int NC>
+__device__ __forceinline__ int32_t coop_scan(const PartRegs<S, R, NC>& s, int lane, const WalkBuf& b, int i,
+                                             int32_t q0, int32_t ne, int32_t st, int32_t stop_gain, int32_t thr,
+                                             const idx_t* __restrict__ cand_p, const idx_t* __restrict__ cand_g,
+                                             const int32_t* w) {
+  for (int32_t base = q0; base < ne; base += 32) {
+    const int32_t q = base + lane;
+    const bool valid = q < ne;
+    int32_t g = 0, p = -1;
+    if (valid) {
+      g = q < kInline ? b.cg[i * kInline + q] : __ldg(&cand_g[st + q]);
+      p = q < kInline ? b.cp[i * kInline + q] : __ldg(&cand_p[st + q]);
+    }
+    const bool stop = valid && g <= stop_gain;
+    const bool below = valid && g <= thr;
+    const bool fits = gather_fits(s, valid ? p : -1, w);
+    const unsigned m = __ballot_sync(0xffffffffu, stop || below || fits);
+    if (m) {
+      const int l = __ffs(m) - 1;
+      const bool l_stop = __shfl_sync(0xffffffffu, stop, l);
+      const bool l_below = __shfl_sync(0xffffffffu, below, l);
+      const int32_t l_p = __shfl_sync(0xffffffffu, p, l);
+      if (l_stop) return -2 - (base + l);
+      if (l_below) return -1;
+      return l_p;
+    }
+  }
+  return -2 - ne;
+}
+
+// The decision of one mover in the register walk (greedy.rs:64-107 repair,
+// :131-164 cut), in the reference's candidate order: explicit candidates with
+// gain above the non-adjacent gain ig = -w_from, then the non-adjacent parts
+// by id, then the explicit ones at or below ig; the first feasible one with
+// gain above the pass threshold, or -1. The first kInline candidates come
+// from the shared-memory record one at a time; longer lists (a vertex next to
+// many parts) are scanned 32 candidates per step, and membership in the
+// candidate list for the non-adjacent step comes from a shared bitmap `ebits`
+// (R words, zero between calls).
 template <int MODE, typename S, int R, int NC>
 __device__ __forceinline__ int32_t reg_decide(const PartRegs<S, R, NC>& s, int lane, const WalkBuf& b, int i,
                                               int32_t k, const idx_t* __restrict__ cand_p,
-                                              const idx_t* __restrict__ cand_g, const int32_t* w) {
+                                              const idx_t* __restrict__ cand_g, const int32_t* w,
+                                              unsigned* ebits) {
   const int32_t pv = b.pv[i];
   if (MODE == kRepair) {
     bool over = false;
@@ -535,34 +598,69 @@ __device__ __forceinline__ int32_t reg_decide(const PartRegs<S, R, NC>& s, int l
   const int32_t ne = b.ne[i];
   const int32_t st = b.coff[i];
   const int32_t ig = (int32_t)(0u - (uint32_t)b.wf[i]);
-  auto cpart = [&](int32_t q) { return q < kInline ? b.cp[i * kInline + q] : cand_p[st + q]; };
-  auto cgain = [&](int32_t q) { return q < kInline ? b.cg[i * kInline + q] : cand_g[st + q]; };
+  const int32_t nin = ne < kInline ? ne : kInline;
   int32_t q = 0;
-  for (; q < ne; ++q) {
-    const int32_t g = cgain(q);
+  for (; q < nin; ++q) {
+    const int32_t g = b.cg[i * kInline + q];
     if (g <= ig) break;
     if (g <= thr) return -1;
-    const int32_t p = cpart(q);
+    const int32_t p = b.cp[i * kInline + q];
     if (__any_sync(0xffffffffu, lane_fits(s, lane, p, w))) return p;
   }
+  if (q == kInline && ne > kInline) {
+    const int32_t r1 = coop_scan(s, lane, b, i, q, ne, st, ig, thr, cand_p, cand_g, w);
+    if (r1 >= -1) return r1;
+    q = -2 - r1;
+  }
   if (ig > thr) {
+    if (ne <= kInline) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int32_t p = r * 32 + lane;
-      bool ok = p < k && p != pv;
-      if (ok)
+      for (int r = 0; r < R; ++r) {
+        const int32_t p = r * 32 + lane;
+        bool ok = p < k && p != pv;
         for (int32_t e = 0; e < ne; ++e)
-          if (cpart(e) == p) { ok = false; break; }
+          if (b.cp[i * kInline + e] == p) ok = false;
 #pragma unroll
-      for (int c = 0; c < NC; ++c) ok = ok && (S)w[c] <= s.sl[r][c];
-      const unsigned m = __ballot_sync(0xffffffffu, ok);
-      if (m) return r * 32 + __ffs(m) - 1;
+        for (int c = 0; c < NC; ++c) ok = ok && (S)w[c] <= s.sl[r][c];
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        if (m) return r * 32 + __ffs(m) - 1;
+      }
+    } else {
+      for (int32_t base = 0; base < ne; base += 32) {
+        const int32_t e = base + lane;
+        if (e < ne) {
+          const int32_t p = e < kInline ? b.cp[i * kInline + e] : __ldg(&cand_p[st + e]);
+          atomicOr(&ebits[p >> 5], 1u << (p & 31));
+        }
+      }
+      __syncwarp();
+      int32_t found = -1;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int32_t p = r * 32 + lane;
+        bool ok = found < 0 && p < k && p != pv && !((ebits[r] >> lane) & 1u);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) ok = ok && (S)w[c] <= s.sl[r][c];
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        if (m && found < 0) found = r * 32 + __ffs(m) - 1;
+      }
+      __syncwarp();
+      if (lane < R) ebits[lane] = 0u;
+      __syncwarp();
+      if (found >= 0) return found;
     }
+  } else if (q < ne) {
+    // The candidate at q has gain <= ig <= thr, and the rest are lower.
+    return -1;
+  }
+  if (ne > kInline) {
+    const int32_t r3 = coop_scan(s, lane, b, i, q, ne, st, INT_MIN, thr, cand_p, cand_g, w);
+    return r3 >= -1 ? r3 : -1;
   }
   for (; q < ne; ++q) {
-    const int32_t g = cgain(q);
+    const int32_t g = b.cg[i * kInline + q];
     if (g <= thr) return -1;
-    const int32_t p = cpart(q);
+    const int32_t p = b.cp[i * kInline + q];
     if (__any_sync(0xffffffffu, lane_fits(s, lane, p, w))) return p;
   }
   return -1;
@@ -589,8 +687,10 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
                                                            idx_t* __restrict__ d_out, int32_t* __restrict__ nmoves) {
   __shared__ WalkBuf buf[2];
   __shared__ int32_t dbuf[kWalkChunk];
+  __shared__ unsigned ebits[R];
   const int32_t nm = *nm_dev;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid < R) ebits[tid] = 0u;
   PartRegs<S, R, NC> s;
   if (warp == 0) {
 #pragma unroll
@@ -639,7 +739,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
           const bool f2 = __any_sync(0xffffffffu, lane_fits(s, lane, c2, w));
           d = f1 ? c1 : (f2 ? c2 : -1);
         } else if (kn == kContended || kn == kFast) {
-          d = reg_decide<MODE, S, R, NC>(s, lane, b, i, k, cand_p, cand_g, w);
+          d = reg_decide<MODE, S, R, NC>(s, lane, b, i, k, cand_p, cand_g, w, ebits);
         }
         if (lane == 0) dbuf[i] = d;
         if (d >= 0) {

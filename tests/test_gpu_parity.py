@@ -296,3 +296,55 @@ def test_greedy_refine_large_weights(rmb, oracle):
     k = 9
     part = np.random.default_rng(6).integers(0, k, n).astype(np.int32)
     _refine_case(rmb, oracle, x, a, v, w, part, k, [1.03])
+
+
+@pytest.mark.parametrize("k,ub,start", [(128, 1.03, "random"), (256, 1.03, "random"), (256, 1.01, "skewed"),
+                                        (200, 1.05, "skewed")])
+def test_greedy_refine_many_candidates(rmb, oracle, k, ub, start):
+    """R-MAT hubs touch many parts: candidate lists far longer than the
+    walk's inline slots, and (skewed start) repair moves to parts the vertex
+    has no edge to."""
+    x, a = G.rmat(12, seed=5)
+    n = len(x) - 1
+    rng = np.random.default_rng(k)
+    if start == "random":
+        part = rng.integers(0, k, n).astype(np.int32)
+    else:
+        part = np.minimum((np.arange(n) * k * 3) // (4 * n), k - 1).astype(np.int32)
+        flip = rng.random(n) < 0.3
+        part[flip] = rng.integers(0, k, flip.sum())
+    stats = _refine_case(rmb, oracle, x, a, None, None, part, k, [ub])
+    assert stats[1] > 0
+
+
+def test_greedy_refine_many_candidates_two_constraints(rmb, oracle):
+    x, a = G.rmat(11, seed=9)
+    n = len(x) - 1
+    v = np.random.default_rng(1).integers(1, 9, 2 * n).astype(np.int32)
+    w = G.symmetric_edge_weights(x, a, np.random.default_rng(2), 1, 10)
+    k = 160
+    part = np.random.default_rng(3).integers(0, k, n).astype(np.int32)
+    _refine_case(rmb, oracle, x, a, v, w, part, k, [1.05, 1.1], ncon=2)
+
+
+def test_greedy_refine_many_candidates_large_weights(rmb, oracle):
+    x, a = G.rmat(11, seed=10)
+    n = len(x) - 1
+    v = np.random.default_rng(4).integers(200_000, 400_000, n).astype(np.int32)
+    k = 96
+    part = np.random.default_rng(5).integers(0, k, n).astype(np.int32)
+    _refine_case(rmb, oracle, x, a, v, None, part, k, [1.03])
+
+
+def test_pipeline_replay_rmat_k256(rmb, oracle):
+    """Skewed graph, k=256: coarsening stops early (isolated vertices never
+    match), grow leaves many vertices to the lightest-part rule."""
+    from tests.conftest import greedy_options
+    x, a = G.rmat(13, seed=3)
+    n = len(x) - 1
+    g = rmb.Graph(n, 1, x, a)
+    res, mats, seeds, _ = rmb.part_graph_kway_trace(g, 256, options=rmb.Options(rtype=rmb.RType.Greedy, seed=4))
+    rc, part, obj = oracle.part_graph_kway(x, a, 256, options=greedy_options(seed=4), script=(mats, seeds))
+    assert rc == 1
+    assert obj == res.objval
+    assert (part == res.part).all()
