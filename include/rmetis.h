@@ -96,10 +96,44 @@ RMETIS_API int RMETIS_GPU_PartGraphKwayDevice(const idx_t *nvtxs, const idx_t *n
 RMETIS_API int RMETIS_GPU_SetStream(void *stream);
 
 /* Engine knobs without a METIS option slot: grown partitions per attempt
- * (lowest cut kept), matching rounds per level, and whether a graph without
+ * (lowest cut kept), matching rounds per level, whether a graph without
  * vertex weights gets summed coarse weights (1) or the reference's unit coarse
- * weights (0, default). Values < 0 leave a knob unchanged. */
-RMETIS_API int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weights);
+ * weights (0, default), and whether ncuts > 1 attempts run concurrently on the
+ * device's worker pool (1, default) or one after another (0); both give the
+ * same result. Values < 0 leave a knob unchanged. */
+RMETIS_API int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weights,
+                                    int parallel_attempts);
+
+/* Many graphs in one call (no counterpart in the reference, which partitions
+ * one graph per call). Host arrays of the concatenated batch: graph g has
+ * n_g = vtx_off[g+1]-vtx_off[g] vertices and m_g = edge_off[g+1]-edge_off[g]
+ * CSR entries; its xadj (n_g+1 local offsets) starts at xadj[vtx_off[g]+g],
+ * its adjncy/adjwgt (local vertex ids) at edge_off[g], its vwgt at
+ * vtx_off[g]*ncon, its part at part[vtx_off[g]]. nparts[g] per graph; ncon,
+ * ubvec and options are shared. The batch is uploaded once and the graphs are
+ * partitioned concurrently on the device's worker pool; each result equals
+ * the one of a separate RMETIS_PartGraphKway call. status[g] gets each graph's
+ * return code; the call returns METIS_OK or the first failing code. */
+RMETIS_API int RMETIS_GPU_PartGraphKwayBatch(idx_t ngraphs, idx_t ncon, const int64_t *vtx_off,
+                                             const int64_t *edge_off, const idx_t *xadj, const idx_t *adjncy,
+                                             const idx_t *vwgt, const idx_t *adjwgt, const idx_t *nparts,
+                                             const real_t *ubvec, const idx_t *options, idx_t *objval,
+                                             idx_t *part, idx_t *status);
+
+/* Asynchronous requests for a serving loop (no counterpart in the reference).
+ * Same arguments as RMETIS_PartGraphKway without vsize; returns a ticket > 0,
+ * or a negative METIS error code. The request starts on the device's worker
+ * pool once its estimated device-memory footprint fits in the pool's budget
+ * next to the requests running; xadj, adjncy, vwgt, adjwgt, part and objval
+ * must stay valid until RMETIS_GPU_WaitKway returns. Poll: 0 pending, 1 done
+ * (the ticket stays valid). Wait: blocks, returns the request's code and
+ * releases the ticket. */
+RMETIS_API int64_t RMETIS_GPU_SubmitKway(const idx_t *nvtxs, const idx_t *ncon, const idx_t *xadj,
+                                         const idx_t *adjncy, const idx_t *vwgt, const idx_t *adjwgt,
+                                         const idx_t *nparts, const real_t *tpwgts, const real_t *ubvec,
+                                         const idx_t *options, idx_t *objval, idx_t *part);
+RMETIS_API int RMETIS_GPU_PollKway(int64_t ticket);
+RMETIS_API int RMETIS_GPU_WaitKway(int64_t ticket);
 
 /* Per-launch CUDA-event timing of the hot kernels (off by default).
  * RMETIS_GPU_GetProfile fills, per kernel id (0 gain, 1 decide, 2 propose,

@@ -361,5 +361,104 @@ def part_graph_kway_trace(graph: Graph, nparts: int, tpwgts=None, ubvec=None, op
     return PartitionResult(part=part, objval=int(obj.value)), matchings, seeds, stats
 
 
-def set_tuning(grow_trials: int = -1, match_rounds: int = -1, summed_unit_weights: int = -1):
-    _raise_for(_lib.load().RMETIS_GPU_SetTuning(grow_trials, match_rounds, summed_unit_weights), "set_tuning")
+def set_tuning(grow_trials: int = -1, match_rounds: int = -1, summed_unit_weights: int = -1,
+               parallel_attempts: int = -1):
+    """Engine knobs without an options slot (-1 leaves a knob unchanged)."""
+    _raise_for(_lib.load().RMETIS_GPU_SetTuning(grow_trials, match_rounds, summed_unit_weights, parallel_attempts),
+               "set_tuning")
+
+
+def part_graph_kway_batch(graphs, nparts, ubvec=None, options: Options | None = None):
+    """Partition many graphs in one call: the batch is uploaded once and the
+    graphs run concurrently on the device's worker pool. Returns one
+    PartitionResult per graph, each equal to part_graph_kway's for that graph.
+    `nparts` is an int or one value per graph; all graphs share ncon and
+    either all have vertex (edge) weights or none has."""
+    options = options or Options()
+    graphs = list(graphs)
+    G = len(graphs)
+    if G == 0:
+        return []
+    ncon = graphs[0].ncon
+    if any(g.ncon != ncon for g in graphs):
+        raise InputError("all graphs of a batch need the same ncon")
+    nps = np.full(G, nparts, np.int32) if np.isscalar(nparts) else np.ascontiguousarray(nparts, dtype=np.int32)
+    if len(nps) != G:
+        raise InputError("nparts needs one value per graph")
+    for g, k in zip(graphs, nps):
+        if k < 2 or k > g.nvtxs:
+            raise InputError(f"nparts={k} is outside [2, nvtxs={g.nvtxs}]")
+    have_vw = {g.vwgt is not None for g in graphs}
+    have_ew = {g.adjwgt is not None for g in graphs}
+    if len(have_vw) > 1 or len(have_ew) > 1:
+        raise InputError("either every graph of a batch has vertex (edge) weights or none has")
+    vtx_off = np.zeros(G + 1, np.int64)
+    edge_off = np.zeros(G + 1, np.int64)
+    vtx_off[1:] = np.cumsum([g.nvtxs for g in graphs])
+    edge_off[1:] = np.cumsum([len(g.adjncy) for g in graphs])
+    xadj = np.concatenate([g.xadj for g in graphs]).astype(np.int32)
+    adjncy = np.concatenate([g.adjncy for g in graphs]).astype(np.int32)
+    vwgt = np.concatenate([g.vwgt for g in graphs]).astype(np.int32) if have_vw.pop() else None
+    adjwgt = np.concatenate([g.adjwgt for g in graphs]).astype(np.int32) if have_ew.pop() else None
+    ub = None if ubvec is None else np.ascontiguousarray(ubvec, dtype=np.float32)
+    part = np.zeros(int(vtx_off[-1]), np.int32)
+    obj = np.zeros(G, np.int32)
+    status = np.zeros(G, np.int32)
+    opts = options.c_array()
+    rc = _lib.load().RMETIS_GPU_PartGraphKwayBatch(G, ncon, _p(vtx_off, I64P), _p(edge_off, I64P), _p(xadj),
+                                                   _p(adjncy), _p(vwgt), _p(adjwgt), _p(nps), _p(ub, F32P),
+                                                   _p(opts), _p(obj), _p(part), _p(status))
+    _raise_for(rc, "part_graph_kway_batch")
+    return [PartitionResult(part=part[vtx_off[i]:vtx_off[i + 1]].copy(), objval=int(obj[i])) for i in range(G)]
+
+
+class KwayRequest:
+    """An asynchronous k-way request on the device's worker pool (see
+    submit_kway). It holds the host arrays the worker reads and writes until
+    wait() returns."""
+
+    def __init__(self, ticket, keep, part, obj):
+        self._ticket = ticket
+        self._keep = keep
+        self._part = part
+        self._obj = obj
+        self._result = None
+
+    def done(self) -> bool:
+        if self._result is not None:
+            return True
+        rc = _lib.load().RMETIS_GPU_PollKway(self._ticket)
+        if rc < 0:
+            _raise_for(rc, "poll")
+        return rc == 1
+
+    def wait(self) -> PartitionResult:
+        if self._result is None:
+            rc = _lib.load().RMETIS_GPU_WaitKway(self._ticket)
+            self._keep = None
+            _raise_for(rc, "submit_kway")
+            self._result = PartitionResult(part=self._part, objval=int(self._obj.value))
+        return self._result
+
+
+def submit_kway(graph: Graph, nparts: int, tpwgts=None, ubvec=None, options: Options | None = None) -> KwayRequest:
+    """Queue a k-way partition on the device's worker pool and return at once.
+    Requests start in submission order as their estimated memory footprint
+    fits the pool's budget; the result equals part_graph_kway's."""
+    options = options or Options()
+    if nparts < 2:
+        raise InputError(f"nparts must be >= 2, got {nparts}")
+    if nparts > graph.nvtxs:
+        raise InputError(f"nparts={nparts} > nvtxs={graph.nvtxs}")
+    opts = options.c_array()
+    part = np.zeros(graph.nvtxs, dtype=np.int32)
+    obj = ctypes.c_int32(0)
+    nv = ctypes.c_int32(graph.nvtxs); nc = ctypes.c_int32(graph.ncon); npr = ctypes.c_int32(nparts)
+    tp = None if tpwgts is None else np.ascontiguousarray(tpwgts, dtype=np.float32)
+    ub = None if ubvec is None else np.ascontiguousarray(ubvec, dtype=np.float32)
+    t = _lib.load().RMETIS_GPU_SubmitKway(ctypes.byref(nv), ctypes.byref(nc), _p(graph.xadj), _p(graph.adjncy),
+                                          _p(graph.vwgt), _p(graph.adjwgt), ctypes.byref(npr), _p(tp, F32P),
+                                          _p(ub, F32P), _p(opts), ctypes.byref(obj), _p(part))
+    if t <= 0:
+        _raise_for(int(t), "submit_kway")
+    return KwayRequest(t, (graph, opts, nv, nc, npr, tp, ub), part, obj)

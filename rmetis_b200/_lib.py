@@ -20,7 +20,7 @@ SIGNATURES = {
     "RMETIS_PartGraphKway": [I32P, I32P, I32P, I32P, I32P, I32P, I32P, I32P, F32P, F32P, I32P, I32P, I32P],
     "RMETIS_GPU_PartGraphKwayDevice": [I32P, I32P, VP, VP, VP, VP, I32P, F32P, F32P, I32P, I32P, VP],
     "RMETIS_GPU_SetStream": [VP],
-    "RMETIS_GPU_SetTuning": [ctypes.c_int, ctypes.c_int, ctypes.c_int],
+    "RMETIS_GPU_SetTuning": [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int],
     "RMETIS_GPU_SetProfiling": [ctypes.c_int],
     "RMETIS_GPU_GetProfile": [I64P, F64P, F64P, ctypes.c_int],
     "RMETIS_GPU_PartGraphKwayTrace": [I32P, I32P, I32P, I32P, I32P, I32P, I32P, F32P, F32P, I32P, I32P, I32P,
@@ -38,7 +38,15 @@ SIGNATURES = {
                                 F64P, ctypes.c_int32, I32P, I64P],
     "RMETIS_GPU_EdgeCutWeightsNoAlloc": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, VP, VP, VP, VP, VP,
                                          ctypes.c_int32, VP, VP, VP],
+    "RMETIS_GPU_PartGraphKwayBatch": [ctypes.c_int32, ctypes.c_int32, I64P, I64P, I32P, I32P, I32P, I32P, I32P,
+                                      F32P, I32P, I32P, I32P, I32P],
+    "RMETIS_GPU_SubmitKway": [I32P, I32P, I32P, I32P, I32P, I32P, I32P, F32P, F32P, I32P, I32P, I32P],
+    "RMETIS_GPU_PollKway": [ctypes.c_int64],
+    "RMETIS_GPU_WaitKway": [ctypes.c_int64],
 }
+
+# Return types other than int.
+RESTYPES = {"RMETIS_GPU_SubmitKway": ctypes.c_int64}
 
 _lib = None
 
@@ -55,6 +63,6 @@ def load() -> ctypes.CDLL:
         for name, args in SIGNATURES.items():
             fn = getattr(lib, name)
             fn.argtypes = args
-            fn.restype = ctypes.c_int
+            fn.restype = RESTYPES.get(name, ctypes.c_int)
         _lib = lib
     return _lib

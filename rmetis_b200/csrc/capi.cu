@@ -1,7 +1,10 @@
 // extern "C" boundary: the reference's C ABI (src/ffi/c_api.rs) plus the GPU
 // extensions declared in include/rmetis.h.
+#include <algorithm>
+#include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -35,6 +38,7 @@ struct Tuning {
   int grow_trials = 32;
   int match_rounds = 24;
   int summed_unit_weights = 0;
+  int parallel_attempts = 1;
 };
 Tuning& tuning() {
   static Tuning t;
@@ -45,6 +49,7 @@ void apply_tuning(KwayOptions& o) {
   o.grow_trials = tuning().grow_trials;
   o.match_rounds = tuning().match_rounds;
   o.summed_unit_weights = tuning().summed_unit_weights;
+  o.parallel_attempts = tuning().parallel_attempts;
 }
 
 template <typename F>
@@ -78,10 +83,11 @@ void download(Engine& E, T* h, const T* d, size_t count) {
 // The shared body of the host- and device-pointer entry points.
 int kway_common(Engine& E, int32_t n, int32_t nc, int32_t np, const idx_t* d_xadj, const idx_t* d_adj, int64_t ne,
                 const idx_t* d_vwgt, const idx_t* d_adjwgt, const real_t* tpwgts, const real_t* ubvec,
-                const idx_t* options, idx_t* objval, idx_t* d_part, KwayTrace* trace) {
-  KwayOptions o = parse_options(options);
+                const idx_t* options, idx_t* objval, idx_t* d_part, KwayTrace* trace,
+                const KwayOptions* preset = nullptr) {
+  KwayOptions o = preset ? *preset : parse_options(options);
   if (o.rtype != 1) throw Error(METIS_ERROR_INPUT, "RType Fm is not on the GPU path; select Greedy");
-  apply_tuning(o);
+  if (!preset) apply_tuning(o);
   DGraph g;
   g.n = n;
   g.m = ne;
@@ -244,10 +250,11 @@ int RMETIS_GPU_SetStream(void* stream) {
   });
 }
 
-int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weights) {
+int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weights, int parallel_attempts) {
   if (grow_trials >= 0) tuning().grow_trials = grow_trials > 0 ? grow_trials : 1;
   if (match_rounds >= 0) tuning().match_rounds = match_rounds > 0 ? match_rounds : 1;
   if (summed_unit_weights >= 0) tuning().summed_unit_weights = summed_unit_weights ? 1 : 0;
+  if (parallel_attempts >= 0) tuning().parallel_attempts = parallel_attempts ? 1 : 0;
   return METIS_OK;
 }
 
@@ -272,6 +279,157 @@ int RMETIS_GPU_GetProfile(int64_t* launches, double* ms, double* bytes, int max_
     if (max_ids > (int)kProfCount && launches) launches[kProfCount] = launch_counter();
     return (int)kProfCount;
   });
+}
+
+int RMETIS_GPU_PartGraphKwayBatch(idx_t ngraphs, idx_t ncon, const int64_t* vtx_off, const int64_t* edge_off,
+                                  const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt, const idx_t* adjwgt,
+                                  const idx_t* nparts, const real_t* ubvec, const idx_t* options, idx_t* objval,
+                                  idx_t* part, idx_t* status) {
+  return guarded([&] {
+    if (ngraphs <= 0 || ncon <= 0 || !vtx_off || !edge_off || !xadj || !adjncy || !nparts || !part || !objval ||
+        !status)
+      return METIS_ERROR_INPUT;
+    if (vtx_off[0] != 0 || edge_off[0] != 0) return METIS_ERROR_INPUT;
+    for (idx_t g = 0; g < ngraphs; ++g) {
+      const int64_t n = vtx_off[g + 1] - vtx_off[g], m = edge_off[g + 1] - edge_off[g];
+      if (n <= 0 || n > INT32_MAX || m < 0 || m > INT32_MAX) return METIS_ERROR_INPUT;
+      const idx_t* x = xadj + vtx_off[g] + g;
+      if (x[0] != 0 || x[n] != m) return METIS_ERROR_INPUT;
+    }
+    KwayOptions o = parse_options(options);
+    if (o.rtype != 1) return METIS_ERROR_INPUT;
+    apply_tuning(o);
+    o.parallel_attempts = 0;  // the graphs already run concurrently
+    const int64_t ntot = vtx_off[ngraphs], mtot = edge_off[ngraphs];
+    Engine& E = engine_for_current_device();
+    std::lock_guard<std::mutex> lk(E.mu);
+    Arena::Mark mk = E.arena().mark();
+    struct Rewind {
+      Engine& E;
+      Arena::Mark m;
+      ~Rewind() { E.arena().reset_to(m); }
+    } rw{E, mk};
+    // One upload of the concatenated batch; the workers read it in place.
+    idx_t* d_xadj = upload(E, xadj, (size_t)(ntot + ngraphs));
+    idx_t* d_adj = upload(E, adjncy, (size_t)mtot);
+    idx_t* d_vwgt = upload(E, vwgt, (size_t)ntot * ncon);
+    idx_t* d_adjwgt = upload(E, adjwgt, (size_t)mtot);
+    idx_t* d_part = E.arena().alloc<idx_t>((size_t)ntot);
+    RMB_CUDA(cudaStreamSynchronize(E.stream()));
+    int dev = 0;
+    RMB_CUDA(cudaGetDevice(&dev));
+    WorkerPool& pool = pool_for_device(dev);
+    std::vector<std::future<int>> fut;
+    std::vector<int32_t> objs(ngraphs, 0);
+    for (idx_t g = 0; g < ngraphs; ++g) {
+      const int64_t v0 = vtx_off[g], e0 = edge_off[g];
+      const int32_t n = (int32_t)(vtx_off[g + 1] - v0);
+      const int64_t m = edge_off[g + 1] - e0;
+      const int32_t k = nparts[g];
+      int32_t* obj_g = &objs[g];
+      fut.push_back(pool.submit(footprint_bytes(n, m, std::max(k, 2), ncon), [=](Engine& W) {
+        DGraph gr;
+        gr.n = n;
+        gr.m = m;
+        gr.ncon = ncon;
+        gr.xadj = d_xadj + v0 + g;
+        gr.adjncy = d_adj + e0;
+        gr.adjwgt = d_adjwgt ? d_adjwgt + e0 : nullptr;
+        gr.vwgt = d_vwgt ? d_vwgt + v0 * ncon : nullptr;
+        if (k < 2 || k > n) return (int)METIS_ERROR_INPUT;
+        if (validate_device(gr, W.arena(), W.stream(), W.host_scratch()) != 0) return (int)METIS_ERROR_INPUT;
+        return W.partition_kway(gr, k, nullptr, ubvec, o, d_part + v0, obj_g, nullptr);
+      }));
+    }
+    int rc = METIS_OK;
+    for (idx_t g = 0; g < ngraphs; ++g) {
+      status[g] = fut[g].get();
+      objval[g] = objs[g];
+      if (status[g] != METIS_OK && rc == METIS_OK) rc = status[g];
+    }
+    download(E, part, d_part, (size_t)ntot);
+    RMB_CUDA(cudaStreamSynchronize(E.stream()));
+    return rc;
+  });
+}
+
+namespace {
+struct Tickets {
+  std::mutex mu;
+  int64_t next = 1;
+  std::map<int64_t, std::shared_future<int>> pending;
+};
+Tickets& tickets() {
+  static Tickets t;
+  return t;
+}
+}  // namespace
+
+int64_t RMETIS_GPU_SubmitKway(const idx_t* nvtxs, const idx_t* ncon, const idx_t* xadj, const idx_t* adjncy,
+                              const idx_t* vwgt, const idx_t* adjwgt, const idx_t* nparts, const real_t* tpwgts,
+                              const real_t* ubvec, const idx_t* options, idx_t* objval, idx_t* part) {
+  try {
+    if (!nvtxs || !ncon || !xadj || !adjncy || !nparts || !part) return METIS_ERROR_INPUT;
+    const int32_t n = *nvtxs, nc = *ncon, np = *nparts;
+    if (n <= 0 || nc <= 0 || np < 2) return METIS_ERROR_INPUT;
+    if (xadj[0] != 0 || xadj[n] < 0) return METIS_ERROR_INPUT;
+    const int64_t ne = xadj[n];
+    KwayOptions o = parse_options(options);
+    if (o.rtype != 1) return METIS_ERROR_INPUT;
+    apply_tuning(o);
+    o.parallel_attempts = 0;
+    // tpwgts and ubvec are copied now; the CSR arrays, part and objval are
+    // read and written by the worker until the request completes.
+    std::vector<real_t> tp, ub;
+    if (tpwgts) tp.assign(tpwgts, tpwgts + (size_t)np * nc);
+    if (ubvec) ub.assign(ubvec, ubvec + nc);
+    int dev = 0;
+    RMB_CUDA(cudaGetDevice(&dev));
+    WorkerPool& pool = pool_for_device(dev);
+    std::shared_future<int> f =
+        pool.submit(footprint_bytes(n, ne, np, nc), [=](Engine& W) {
+              Arena::Mark mk = W.arena().mark();
+              idx_t* d_xadj = upload(W, xadj, (size_t)n + 1);
+              idx_t* d_adj = upload(W, adjncy, (size_t)ne);
+              idx_t* d_vwgt = upload(W, vwgt, (size_t)n * nc);
+              idx_t* d_adjwgt = upload(W, adjwgt, (size_t)ne);
+              idx_t* d_part = W.arena().alloc<idx_t>((size_t)n);
+              const int rc = kway_common(W, n, nc, np, d_xadj, d_adj, ne, d_vwgt, d_adjwgt,
+                                         tp.empty() ? nullptr : tp.data(), ub.empty() ? nullptr : ub.data(), nullptr,
+                                         objval, d_part, nullptr, &o);
+              download(W, part, d_part, (size_t)n);
+              RMB_CUDA(cudaStreamSynchronize(W.stream()));
+              W.arena().reset_to(mk);
+              return rc;
+            }).share();
+    std::lock_guard<std::mutex> lk(tickets().mu);
+    const int64_t id = tickets().next++;
+    tickets().pending.emplace(id, f);
+    return id;
+  } catch (const rmb::Error& e) {
+    return e.code;
+  } catch (...) {
+    return METIS_ERROR;
+  }
+}
+
+int RMETIS_GPU_PollKway(int64_t ticket) {
+  std::lock_guard<std::mutex> lk(tickets().mu);
+  auto it = tickets().pending.find(ticket);
+  if (it == tickets().pending.end()) return METIS_ERROR_INPUT;
+  return it->second.wait_for(std::chrono::seconds(0)) == std::future_status::ready ? 1 : 0;
+}
+
+int RMETIS_GPU_WaitKway(int64_t ticket) {
+  std::shared_future<int> f;
+  {
+    std::lock_guard<std::mutex> lk(tickets().mu);
+    auto it = tickets().pending.find(ticket);
+    if (it == tickets().pending.end()) return METIS_ERROR_INPUT;
+    f = it->second;
+    tickets().pending.erase(it);
+  }
+  return f.get();
 }
 
 int RMETIS_GPU_PartGraphKwayTrace(const idx_t* nvtxs, const idx_t* ncon, const idx_t* xadj, const idx_t* adjncy,

@@ -2,6 +2,8 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include <stdint.h>
 
 #include <cstdio>
@@ -28,7 +30,7 @@ struct Error : public std::runtime_error {
   } while (0)
 
 // Every kernel launch is followed by RMB_LAUNCH_CHECK(), which also counts it.
-long long& launch_counter();
+std::atomic<long long>& launch_counter();
 #define RMB_LAUNCH_CHECK()          \
   do {                              \
     RMB_CUDA(cudaGetLastError());   \

@@ -1,5 +1,6 @@
 // Host orchestration of the multilevel k-way pipeline
 // (src/partition/kway.rs:20-162 and src/coarsen/mod.rs:36-71).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -18,8 +19,8 @@ Profiler& profiler() {
   return p;
 }
 
-long long& launch_counter() {
-  static long long c = 0;
+std::atomic<long long>& launch_counter() {
+  static std::atomic<long long> c{0};
   return c;
 }
 
@@ -36,6 +37,7 @@ cudaEvent_t Profiler::get() {
 
 int Profiler::begin(int id, cudaStream_t st) {
   if (!on) return -1;
+  std::lock_guard<std::mutex> lk(mu_);
   Rec r{id, get(), get(), 0.0};
   RMB_CUDA(cudaEventRecord(r.a, st));
   recs_.push_back(r);
@@ -44,11 +46,13 @@ int Profiler::begin(int id, cudaStream_t st) {
 
 void Profiler::end(int h, cudaStream_t st, double bytes) {
   if (h < 0) return;
+  std::lock_guard<std::mutex> lk(mu_);
   recs_[h].bytes = bytes;
   RMB_CUDA(cudaEventRecord(recs_[h].b, st));
 }
 
 void Profiler::collect() {
+  std::lock_guard<std::mutex> lk(mu_);
   for (auto& r : recs_) {
     RMB_CUDA(cudaEventSynchronize(r.b));
     float ms = 0.f;
@@ -64,6 +68,7 @@ void Profiler::collect() {
 
 void Profiler::reset() {
   collect();
+  std::lock_guard<std::mutex> lk(mu_);
   totals = ProfTotals{};
 }
 
@@ -95,7 +100,8 @@ void threshold_values(double t, double ub, long long* feas, long long* over, lon
 // ---------------------------------------------------------------------------
 // Engine
 // ---------------------------------------------------------------------------
-Engine::Engine() {
+Engine::Engine(bool is_worker) : is_worker_(is_worker) {
+  RMB_CUDA(cudaGetDevice(&device_));
   RMB_CUDA(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
   stream_ = own_stream_;
   RMB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_scratch_), 4096));
@@ -151,9 +157,7 @@ int Engine::partition_kway(const DGraph& g0, int nparts, const float* tpwgts, co
   for (int c = 0; c < ncon; ++c) ub[c] = ubvec ? (double)ubvec[c] : 1.0 + (double)o.ufactor / 1000.0;
 
   Arena::Mark call_mark = arena_.mark();
-  const size_t K = (size_t)k * ncon;
   long long* d_tot = arena_.alloc<long long>((size_t)ncon);
-  unsigned long long* d_cut = arena_.alloc<unsigned long long>(1);
 
   // Total weight of the input (i32 with wrap-around, like the reference).
   std::vector<int32_t> total0(ncon, g0.n);
@@ -168,18 +172,79 @@ int Engine::partition_kway(const DGraph& g0, int nparts, const float* tpwgts, co
     }
   }
 
-  const size_t limit = std::max<size_t>((size_t)20 * k, 20);         // coarsen/mod.rs:43
+  std::random_device rd;
+  std::vector<uint64_t> seeds(o.ncuts);
+  for (int a = 0; a < o.ncuts; ++a)                                 // kway.rs:55-61
+    seeds[a] = o.seed == 0 ? (((uint64_t)rd() << 32) ^ (uint64_t)rd()) : o.seed + (uint64_t)a;
+
   bool have_best = false;
   int32_t best_obj = 0;
-  std::random_device rd;
+  if (o.ncuts > 1 && o.parallel_attempts && !is_worker_ && !trace) {
+    // Attempts are independent (the reference stripes them over MPI ranks,
+    // kway.rs:54): run them on the worker pool, each into its own buffer, and
+    // keep the first attempt with the lowest cut (strict <, kway.rs:96-98).
+    WorkerPool& pool = pool_for_device(device_);
+    std::vector<idx_t*> parts(o.ncuts);
+    for (int a = 0; a < o.ncuts; ++a) parts[a] = arena_.alloc<idx_t>((size_t)g0.n);
+    RMB_CUDA(cudaStreamSynchronize(st));  // the input is complete before other streams read it
+    std::vector<int32_t> objs(o.ncuts, 0);
+    std::vector<std::future<int>> fut;
+    const size_t fp = footprint_bytes(g0.n, g0.m, k, ncon);
+    for (int a = 0; a < o.ncuts; ++a) {
+      fut.push_back(pool.submit(fp, [&, a](Engine& e) {
+        e.run_attempt(g0, k, tpwgts, ub, total0, o, seeds[a], parts[a], &objs[a], nullptr);
+        return 1;
+      }));
+    }
+    int rc = 1;
+    for (auto& f : fut) {
+      const int r = f.get();
+      if (r != 1 && rc == 1) rc = r;
+    }
+    if (rc != 1) {
+      arena_.reset_to(call_mark);
+      throw Error(rc, "an attempt failed");
+    }
+    int best = 0;
+    for (int a = 1; a < o.ncuts; ++a)
+      if (objs[a] < objs[best]) best = a;
+    best_obj = objs[best];
+    RMB_CUDA(cudaMemcpyAsync(part_out, parts[best], sizeof(idx_t) * g0.n, cudaMemcpyDeviceToDevice, st));
+    RMB_CUDA(cudaStreamSynchronize(st));
+  } else {
+    for (int a = 0; a < o.ncuts; ++a) {                                 // kway.rs:54
+      Arena::Mark att_mark = arena_.mark();
+      idx_t* part = arena_.alloc<idx_t>((size_t)g0.n);
+      KwayTrace local;
+      int32_t obj = 0;
+      run_attempt(g0, k, tpwgts, ub, total0, o, seeds[a], part, &obj, trace ? &local : nullptr);
+      if (!have_best || obj < best_obj) {                               // kway.rs:96-98
+        best_obj = obj;
+        have_best = true;
+        RMB_CUDA(cudaMemcpyAsync(part_out, part, sizeof(idx_t) * g0.n, cudaMemcpyDeviceToDevice, st));
+        if (trace) *trace = std::move(local);
+      }
+      RMB_CUDA(cudaStreamSynchronize(st));
+      arena_.reset_to(att_mark);
+    }
+  }
+  arena_.reset_to(call_mark);
+  if (objval) *objval = best_obj;
+  if (profiler().on) profiler().collect();
+  return 1;
+}
 
-  for (int attempt = 0; attempt < o.ncuts; ++attempt) {              // kway.rs:54
-    Arena::Mark att_mark = arena_.mark();
-    uint64_t seed64;
-    if (o.seed == 0) seed64 = ((uint64_t)rd() << 32) ^ (uint64_t)rd();
-    else seed64 = o.seed + (uint64_t)attempt;
-    KwayTrace local;
-
+void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std::vector<double>& ub,
+                         const std::vector<int32_t>& total0, const KwayOptions& o, uint64_t seed64, idx_t* part_out,
+                         int32_t* objval, KwayTrace* trace) {
+  cudaStream_t st = stream_;
+  const int ncon = g0.ncon;
+  const size_t K = (size_t)k * ncon;
+  const size_t limit = std::max<size_t>((size_t)20 * k, 20);         // coarsen/mod.rs:43
+  Arena::Mark att_mark = arena_.mark();
+  unsigned long long* d_cut = arena_.alloc<unsigned long long>(1);
+  KwayTrace local;
+  {
     // ---- coarsening (coarsen/mod.rs:36-71) ----
     std::vector<DGraph> levels{g0};
     std::vector<idx_t*> cmaps;
@@ -329,23 +394,14 @@ int Engine::partition_kway(const DGraph& g0, int nparts, const float* tpwgts, co
     // ---- objective (kway.rs:94-98) ----
     cut_and_weights(g0, part, k, d_cut, nullptr, st);
     unsigned long long cut_raw = 0;
+    RMB_CUDA(cudaMemcpyAsync(part_out, part, sizeof(idx_t) * g0.n, cudaMemcpyDeviceToDevice, st));
     RMB_CUDA(cudaMemcpyAsync(h_scratch_ + 32, d_cut, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     RMB_CUDA(cudaStreamSynchronize(st));
     std::memcpy(&cut_raw, h_scratch_ + 32, sizeof(cut_raw));
-    const int32_t obj = (int32_t)(uint32_t)cut_raw / 2;
-    if (!have_best || obj < best_obj) {
-      best_obj = obj;
-      have_best = true;
-      RMB_CUDA(cudaMemcpyAsync(part_out, part, sizeof(idx_t) * g0.n, cudaMemcpyDeviceToDevice, st));
-      if (trace) *trace = std::move(local);
-    }
-    RMB_CUDA(cudaStreamSynchronize(st));
-    arena_.reset_to(att_mark);
+    *objval = (int32_t)(uint32_t)cut_raw / 2;
+    if (trace) *trace = std::move(local);
   }
-  arena_.reset_to(call_mark);
-  if (objval) *objval = best_obj;
-  if (profiler().on) profiler().collect();
-  return 1;
+  arena_.reset_to(att_mark);
 }
 
 Engine& engine_for_current_device() {

@@ -3,7 +3,13 @@
 
 #include <cuda_runtime.h>
 
+#include <condition_variable>
+#include <deque>
+#include <functional>
+#include <future>
+#include <memory>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "arena.h"
@@ -25,6 +31,7 @@ struct KwayOptions {
   int grow_trials = 32;       // grown partitions per attempt; the lowest cut is kept
   int match_rounds = 24;     // proposal rounds per coarsening level (upper bound)
   int summed_unit_weights = 0;  // 1: a graph without vwgt gets summed coarse weights
+  int parallel_attempts = 1;    // 1: ncuts > 1 attempts run concurrently on the worker pool
 };
 
 // Per-kernel-family device time, measured with CUDA events on the engine's
@@ -47,7 +54,8 @@ struct KwayTrace {
 
 class Engine {
  public:
-  Engine();
+  // A worker engine (one per pool thread) never hands work to the pool.
+  explicit Engine(bool is_worker = false);
   ~Engine();
 
   // The whole k-way partition of a device-resident graph. part_out is a
@@ -55,6 +63,13 @@ class Engine {
   // Returns 1 (METIS_OK) or throws rmb::Error.
   int partition_kway(const DGraph& g, int nparts, const float* tpwgts, const float* ubvec, const KwayOptions& o,
                      idx_t* part_out, int32_t* objval, KwayTrace* trace);
+
+  // One attempt (kway.rs:62-98) with seed seed64: coarsen, grow, refine and
+  // project; writes the partition to part_out (device, g.n) and its cut to
+  // *objval. g must be complete before this engine's stream reads it.
+  void run_attempt(const DGraph& g, int k, const float* tpwgts, const std::vector<double>& ub,
+                   const std::vector<int32_t>& total0, const KwayOptions& o, uint64_t seed64, idx_t* part_out,
+                   int32_t* objval, KwayTrace* trace);
 
   void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
   cudaStream_t stream() const { return stream_; }
@@ -75,6 +90,8 @@ class Engine {
 
   struct Timer;
   Arena arena_;
+  bool is_worker_ = false;
+  int device_ = 0;
   cudaStream_t own_stream_ = nullptr;
   cudaStream_t stream_ = nullptr;
   int32_t* h_scratch_ = nullptr;   // pinned
@@ -86,6 +103,48 @@ class Engine {
 
 // One engine per device, created on first use.
 Engine& engine_for_current_device();
+
+// Device memory one partition of a graph of n vertices, m CSR entries, k
+// parts and ncon constraints may hold at once (input, hierarchy, refinement
+// and grow scratch), rounded up: the admission estimate of the pool.
+size_t footprint_bytes(int64_t n, int64_t m, int k, int ncon);
+
+// Worker threads on one device, each with its own Engine (stream, workspace,
+// pinned staging), running submitted jobs concurrently. Jobs start in
+// submission order when their footprint fits in the budget next to the jobs
+// running (a job larger than the whole budget runs alone). A job's return
+// value (or the code of the rmb::Error it throws) completes its future; the
+// worker's workspace is rewound after every job.
+class WorkerPool {
+ public:
+  WorkerPool(int device, int nworkers, size_t budget_bytes);
+  ~WorkerPool();
+  std::future<int> submit(size_t footprint, std::function<int(Engine&)> fn);
+  int workers() const { return (int)threads_.size(); }
+  size_t budget() const { return budget_; }
+  void set_budget(size_t b);
+
+ private:
+  struct Job {
+    size_t footprint;
+    std::function<int(Engine&)> fn;
+    std::promise<int> prom;
+  };
+  void worker_main(int idx);
+  int device_;
+  std::vector<std::thread> threads_;
+  std::deque<std::unique_ptr<Job>> queue_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  size_t budget_;
+  size_t in_use_ = 0;
+  int running_ = 0;
+  bool stop_ = false;
+};
+
+// The pool of a device, created on first use: RMETIS_B200_WORKERS threads
+// (default 8) and a budget of RMETIS_B200_POOL_BYTES (default 150 GB).
+WorkerPool& pool_for_device(int device);
 
 // Host-side threshold form of the reference's f64 tests:
 //   feasible   (pw + vw) as f64 <= t * ub   <=>  pw + vw <= feas

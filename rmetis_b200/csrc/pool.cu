@@ -1,0 +1,123 @@
+// Worker pool: concurrent partitions on one device (the attempts of one call,
+// the graphs of a batch, asynchronous requests).
+#include <algorithm>
+#include <cstdlib>
+#include <mutex>
+
+#include "engine.h"
+
+namespace rmb {
+
+size_t footprint_bytes(int64_t n, int64_t m, int k, int ncon) {
+  // Input (xadj, adjncy, adjwgt, vwgt), the coarse hierarchy (about 1.5x the
+  // input), refinement scratch per level (mover records, candidates, flags)
+  // and the grow trials on the coarsest graph; rounded up generously.
+  const int64_t input = 4 * (n + 1) + 8 * m + 4 * n * ncon;
+  const int64_t hierarchy = input * 3 / 2 + 16 * n;
+  const int64_t refine = 88 * n + 8 * m + 24 * (int64_t)k * ncon;
+  const int64_t grow = 32 * (16 * std::max<int64_t>(20 * (int64_t)k, 20) * 4);
+  return (size_t)(input + hierarchy + refine + grow + ((int64_t)64 << 20));
+}
+
+WorkerPool::WorkerPool(int device, int nworkers, size_t budget_bytes) : device_(device), budget_(budget_bytes) {
+  for (int i = 0; i < nworkers; ++i) threads_.emplace_back([this, i] { worker_main(i); });
+}
+
+WorkerPool::~WorkerPool() {
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    stop_ = true;
+  }
+  cv_.notify_all();
+  for (auto& t : threads_)
+    if (t.joinable()) t.join();
+}
+
+void WorkerPool::set_budget(size_t b) {
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    budget_ = b;
+  }
+  cv_.notify_all();
+}
+
+std::future<int> WorkerPool::submit(size_t footprint, std::function<int(Engine&)> fn) {
+  auto job = std::make_unique<Job>();
+  job->footprint = footprint;
+  job->fn = std::move(fn);
+  std::future<int> f = job->prom.get_future();
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    queue_.push_back(std::move(job));
+  }
+  cv_.notify_all();
+  return f;
+}
+
+void WorkerPool::worker_main(int idx) {
+  (void)idx;
+  cudaSetDevice(device_);
+  std::unique_ptr<Engine> engine;
+  try {
+    engine = std::make_unique<Engine>(/*is_worker=*/true);
+  } catch (...) {
+    engine.reset();  // every job this thread takes then fails with METIS_ERROR
+  }
+  for (;;) {
+    std::unique_ptr<Job> job;
+    {
+      std::unique_lock<std::mutex> lk(mu_);
+      // Admission in submission order: the head starts when its footprint
+      // fits next to the running jobs, or when nothing runs.
+      cv_.wait(lk, [&] {
+        if (stop_) return true;
+        if (queue_.empty()) return false;
+        const size_t fp = queue_.front()->footprint;
+        return running_ == 0 || in_use_ + fp <= budget_;
+      });
+      if (stop_) return;
+      job = std::move(queue_.front());
+      queue_.pop_front();
+      in_use_ += job->footprint;
+      ++running_;
+    }
+    int rc = -4;
+    if (engine) {
+      try {
+        rc = job->fn(*engine);
+      } catch (const Error& e) {
+        rc = e.code;
+      } catch (const std::bad_alloc&) {
+        rc = -3;
+      } catch (...) {
+        rc = -4;
+      }
+      // A failed job must not leave its workspace half used.
+      engine->arena().rewind();
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      in_use_ -= job->footprint;
+      --running_;
+    }
+    cv_.notify_all();
+    job->prom.set_value(rc);
+  }
+}
+
+WorkerPool& pool_for_device(int device) {
+  static std::mutex m;
+  static std::vector<WorkerPool*> pools;
+  std::lock_guard<std::mutex> lk(m);
+  if ((int)pools.size() <= device) pools.resize(device + 1, nullptr);
+  if (!pools[device]) {
+    int n = 8;
+    if (const char* e = std::getenv("RMETIS_B200_WORKERS")) n = std::max(1, std::atoi(e));
+    size_t budget = (size_t)150 << 30;
+    if (const char* e = std::getenv("RMETIS_B200_POOL_BYTES")) budget = (size_t)std::strtoull(e, nullptr, 10);
+    pools[device] = new WorkerPool(device, n, budget);  // lives until process exit
+  }
+  return *pools[device];
+}
+
+}  // namespace rmb

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <vector>
 
 namespace rmb {
@@ -33,6 +34,7 @@ class Profiler {
   // Sets the algorithmic bytes of a recorded launch after the fact (for
   // launches whose size is only known on the device when they are queued).
   void set_bytes(int handle, double bytes) {
+    std::lock_guard<std::mutex> lk(mu_);
     if (handle >= 0 && handle < (int)recs_.size()) recs_[handle].bytes = bytes;
   }
   // Synchronises on the recorded events and adds them to the totals.
@@ -47,6 +49,7 @@ class Profiler {
     double bytes;
   };
   std::vector<Rec> recs_;
+  std::mutex mu_;  // worker threads record launches concurrently
   std::vector<cudaEvent_t> pool_;
   cudaEvent_t get();
 };

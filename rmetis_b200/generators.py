@@ -151,6 +151,44 @@ def rmat(scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19, seed: int = 
     return xadj, adjncy
 
 
+def rmat_device(scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19, seed: int = 22, device="cuda"):
+    """R-MAT built on a CUDA device with torch (a seeded torch.Generator on that
+    device), for scales whose host-side sort and dedup take minutes. Same
+    construction as rmat(): symmetrised, self-loops and duplicates removed,
+    isolated vertices kept, neighbours ascending. The random stream differs
+    from rmat()'s numpy one, so the two give different graphs for one seed.
+    Returns host numpy (xadj, adjncy)."""
+    import torch
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    n = 1 << scale
+    ne = edge_factor * n
+    src = torch.zeros(ne, dtype=torch.int64, device=device)
+    dst = torch.zeros(ne, dtype=torch.int64, device=device)
+    ab = a + b
+    c_norm = c / (1.0 - ab)
+    a_norm = a / ab
+    for bit in range(scale):
+        ii = torch.rand(ne, generator=gen, device=device) > ab
+        thr = torch.where(ii, torch.tensor(c_norm, device=device), torch.tensor(a_norm, device=device))
+        jj = torch.rand(ne, generator=gen, device=device) > thr
+        src |= ii.to(torch.int64) << bit
+        dst |= jj.to(torch.int64) << bit
+        del ii, jj, thr
+    keep = src != dst
+    src, dst = src[keep], dst[keep]
+    key = torch.unique(torch.cat([src * n + dst, dst * n + src]), sorted=True)
+    del src, dst, keep
+    s2 = key // n
+    adjncy = (key % n).to(torch.int32)
+    xadj = torch.zeros(n + 1, dtype=torch.int64, device=device)
+    xadj[1:] = torch.cumsum(torch.bincount(s2, minlength=n), 0)
+    out = xadj.to(torch.int32).cpu().numpy(), adjncy.cpu().numpy()
+    del key, s2, adjncy, xadj
+    torch.cuda.empty_cache()
+    return out
+
+
 def rgg2d(n: int, seed, mean_degree: float = 10.0):
     """2D random geometric graph: points U[0,1]^2, radius r = sqrt(mean_degree
     / (pi n)); edge weight 1 + floor(10 * (1 - d / r)). Returns (xadj, adjncy,

@@ -13,7 +13,7 @@ from tests.conftest import ROOT, greedy_options
 
 def header_symbols():
     text = open(os.path.join(ROOT, "include", "rmetis.h")).read()
-    return sorted(set(re.findall(r"RMETIS_API\s+int\s+(RMETIS_\w+)\s*\(", text)))
+    return sorted(set(re.findall(r"RMETIS_API\s+(?:int|int64_t)\s+(RMETIS_\w+)\s*\(", text)))
 
 
 def test_header_declares_drop_in_symbols():
