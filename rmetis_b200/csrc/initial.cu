@@ -131,31 +131,86 @@ __global__ void __launch_bounds__(32) k_grow(const idx_t* __restrict__ xadj, con
     any_active = active > 0;
   }
 
-  // Leftovers (disconnected or unreachable): lightest part on constraint 0.
-  for (int32_t b = 0; b < n; b += 32) {
-    const int32_t v = b + lane;
-    unsigned un = __ballot_sync(FULL, v < n && part[v] == -1);
-    while (un) {
-      const int i = __ffs(un) - 1;
-      un &= un - 1;
-      const int32_t vv = b + i;
-      long long best = LLONG_MAX;
-      int32_t bp = INT32_MAX;
-      for (int32_t p = lane; p < k; p += 32) {
-        const long long x = pw[(int64_t)p * ncon];
-        if (x < best) { best = x; bp = p; }
-      }
+  // Leftovers (disconnected or unreachable): lightest part on constraint 0,
+  // first minimum, in ascending vertex order.
+  if (!HAS_VW && k <= 1024) {
+    // Unit weights: the leftovers fill the parts level by level. At level L
+    // the parts whose weight before this phase is <= L each take one leftover,
+    // in id order, and then the level rises by one; parts join as L reaches
+    // their weight. Lane l keeps the bitmap word of parts 32l..32l+31.
+    long long L = LLONG_MAX;
+    for (int32_t p = lane; p < k; p += 32) L = min(L, pw[(int64_t)p * ncon]);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const long long ob = __shfl_xor_sync(FULL, best, o);
-        const int32_t op = __shfl_xor_sync(FULL, bp, o);
-        if (ob < best || (ob == best && op < bp)) { best = ob; bp = op; }
+    for (int o = 16; o > 0; o >>= 1) L = min(L, __shfl_xor_sync(FULL, L, o));
+    unsigned act = 0;
+    long long nxt = LLONG_MAX;  // smallest weight of this lane's parts not yet active
+    auto activate = [&]() {
+      nxt = LLONG_MAX;
+      for (int bb = 0; bb < 32; ++bb) {
+        const int32_t p = lane * 32 + bb;
+        if (p < k && !((act >> bb) & 1u)) {
+          const long long x = pw[(int64_t)p * ncon];
+          if (x <= L) act |= 1u << bb;
+          else nxt = min(nxt, x);
+        }
       }
-      if (lane == 0) {
-        part[vv] = bp;
-        for (int c = 0; c < ncon; ++c) pw[(int64_t)bp * ncon + c] += HAS_VW ? vwgt[(int64_t)vv * ncon + c] : 1;
+    };
+    activate();
+    int32_t cursor = 0;  // parts below cursor have had their turn at level L
+    for (int32_t b = 0; b < n; b += 32) {
+      const int32_t v = b + lane;
+      unsigned un = __ballot_sync(FULL, v < n && part[v] == -1);
+      while (un) {
+        const int i = __ffs(un) - 1;
+        un &= un - 1;
+        const int32_t w0 = lane * 32;
+        unsigned mask = w0 + 31 < cursor ? 0u : (w0 >= cursor ? act : act & (~0u << (cursor & 31)));
+        unsigned m = __ballot_sync(FULL, mask != 0u);
+        if (m == 0u) {
+          // Level L is done: every active part now weighs L + 1.
+          ++L;
+          cursor = 0;
+          long long g = nxt;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) g = min(g, __shfl_xor_sync(FULL, g, o));
+          if (g <= L) activate();
+          mask = act;
+          m = __ballot_sync(FULL, mask != 0u);
+        }
+        const int wl = __ffs(m) - 1;
+        const unsigned word = __shfl_sync(FULL, mask, wl);
+        const int32_t p = wl * 32 + __ffs(word) - 1;
+        if (lane == 0) part[b + i] = p;
+        cursor = p + 1;
       }
       __syncwarp();
+    }
+  } else {
+    for (int32_t b = 0; b < n; b += 32) {
+      const int32_t v = b + lane;
+      unsigned un = __ballot_sync(FULL, v < n && part[v] == -1);
+      while (un) {
+        const int i = __ffs(un) - 1;
+        un &= un - 1;
+        const int32_t vv = b + i;
+        long long best = LLONG_MAX;
+        int32_t bp = INT32_MAX;
+        for (int32_t p = lane; p < k; p += 32) {
+          const long long x = pw[(int64_t)p * ncon];
+          if (x < best) { best = x; bp = p; }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const long long ob = __shfl_xor_sync(FULL, best, o);
+          const int32_t op = __shfl_xor_sync(FULL, bp, o);
+          if (ob < best || (ob == best && op < bp)) { best = ob; bp = op; }
+        }
+        if (lane == 0) {
+          part[vv] = bp;
+          for (int c = 0; c < ncon; ++c) pw[(int64_t)bp * ncon + c] += HAS_VW ? vwgt[(int64_t)vv * ncon + c] : 1;
+        }
+        __syncwarp();
+      }
     }
   }
   __syncwarp();

@@ -205,6 +205,7 @@ constexpr int kWalkChunk = 256;     // mover records per shared-memory chunk
 constexpr int kWalkThreads = 256;   // warp 0 walks, the other warps stream records
 constexpr int32_t kContended = -2;  // decision not known before the walk (general path)
 constexpr int32_t kFast = -3;       // not known; at most two candidates, cut pass
+constexpr int32_t kLong = -4;       // not known; cut pass, more candidates than the inline slots
 constexpr int kWalkSmemParts = 4096;  // [k][ncon] entries kept in shared memory
 
 struct MoverRecs {  // structure of arrays, nm entries each
@@ -226,7 +227,7 @@ __global__ void k_walk_prep(const int32_t* __restrict__ nm_dev, const idx_t* __r
                             const idx_t* __restrict__ xadj, const idx_t* __restrict__ ncand,
                             const idx_t* __restrict__ wfrom, const idx_t* __restrict__ cand_p,
                             const idx_t* __restrict__ cand_g, MoverRecs r, long long* __restrict__ in_max,
-                            long long* __restrict__ out_max) {
+                            long long* __restrict__ out_max, int32_t* __restrict__ long_flag) {
   const int32_t nm = *nm_dev;
   RMB_GRID_STRIDE(j, nm) {
     const int32_t v = movers[j];
@@ -234,7 +235,12 @@ __global__ void k_walk_prep(const int32_t* __restrict__ nm_dev, const idx_t* __r
     const int32_t s = xadj[v];
     const int32_t ne = ncand[v];
     r.pv[j] = pv;
-    if (MODE != kCut) r.known[j] = kContended;
+    if (MODE != kCut) {
+      r.known[j] = kContended;
+      // Count the movers with long candidate lists (one atomic per warp).
+      const unsigned lm = __ballot_sync(__activemask(), ne > kInline);
+      if (lm && (threadIdx.x & 31) == __ffs(lm) - 1) atomicAdd(long_flag, __popc(lm));
+    }
     r.ne[j] = ne;
     r.wf[j] = wfrom[v];
     r.coff[j] = s;
@@ -262,7 +268,7 @@ __global__ void k_walk_prep(const int32_t* __restrict__ nm_dev, const idx_t* __r
 __global__ void k_walk_classify(const int32_t* __restrict__ nm_dev, int32_t ncon, const idx_t* __restrict__ cand_p,
                                 const idx_t* __restrict__ cand_g, MoverRecs r, const long long* __restrict__ pw0,
                                 const long long* __restrict__ feas, const long long* __restrict__ in_max,
-                                const long long* __restrict__ out_max) {
+                                const long long* __restrict__ out_max, int32_t* __restrict__ long_flag) {
   const int32_t nm = *nm_dev;
   RMB_GRID_STRIDE(j, nm) {
     const int32_t ne = r.ne[j];
@@ -298,6 +304,10 @@ __global__ void k_walk_classify(const int32_t* __restrict__ nm_dev, int32_t ncon
         if (npos <= 2) known = kFast;
       }
     }
+    if (known == kContended && ne > kInline) known = kLong;
+    // Count the kLong movers (one atomic per warp).
+    const unsigned lm = __ballot_sync(__activemask(), known == kLong);
+    if (lm && (threadIdx.x & 31) == __ffs(lm) - 1) atomicAdd(long_flag, __popc(lm));
     r.known[j] = known;
   }
 }
@@ -438,7 +448,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const int32_t* __restrict
         const int i = i0 + lane;
         const bool valid = i < cnt;
         const int32_t known = valid ? b.known[i] : -1;
-        const bool open = valid && (known == kContended || known == kFast);
+        const bool open = valid && (known == kContended || known == kFast || known == kLong);
         const int32_t pv = valid ? b.pv[i] : -1;
         for (int c = 0; c < ncon; ++c) win_vw[lane * kMaxCon + c] = valid ? b.vw[i * kMaxCon + c] : 0;
         win_pv[lane] = pv;
@@ -514,45 +524,58 @@ __device__ __forceinline__ bool lane_fits(const PartRegs<S, R, NC>& s, int lane,
   return ok;
 }
 
-// Whether a move of weight w into part p (each lane its own p; p < 0 never)
-// fits: the slack of p sits in lane p & 31, slot p >> 5, so every lane
-// gathers the slacks of its p with one shuffle per slot. All lanes call it.
-template <typename S, int R, int NC>
-__device__ __forceinline__ bool gather_fits(const PartRegs<S, R, NC>& s, int32_t p, const int32_t* w) {
-  const int src = p & 31, slot = p >> 5;
-  bool ok = p >= 0;
-#pragma unroll
-  for (int r = 0; r < R; ++r)
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      const S x = __shfl_sync(0xffffffffu, s.sl[r][c], src);
-      if (slot == r && (S)w[c] > x) ok = false;
+// First 32 candidates of a mover (lane q holds candidate q, or p = -1 past
+// the end): from the shared-memory record for q < kInline, else from the
+// global candidate arrays.
+struct CandChunk {
+  int32_t g, p;
+};
+__device__ __forceinline__ CandChunk first_chunk(const WalkBuf& b, int i, int lane, const idx_t* __restrict__ cand_p,
+                                                 const idx_t* __restrict__ cand_g) {
+  CandChunk c{0, -1};
+  const int32_t ne = b.ne[i];
+  if (lane < ne) {
+    if (lane < kInline) {
+      c.g = b.cg[i * kInline + lane];
+      c.p = b.cp[i * kInline + lane];
+    } else {
+      const int32_t st = b.coff[i];
+      c.g = __ldg(&cand_g[st + lane]);
+      c.p = __ldg(&cand_p[st + lane]);
     }
-  return ok;
+  }
+  return c;
 }
 
 // Explicit candidates q0.. of one mover, 32 at a time: lane t takes
-// candidate q0 + t (coalesced loads), and the first lane in candidate order
-// whose candidate ends the scan decides. The scan ends at a candidate whose
-// gain is <= stop_gain (returns -2 - q: the caller goes on elsewhere from q),
-// at one whose gain is <= thr (returns -1), or at a feasible one (returns its
-// part); running out returns -2 - ne.
-template <typename S, int R, int NC>
-__device__ __forceinline__ int32_t coop_scan(const PartRegs<S, R, NC>& s, int lane, const WalkBuf& b, int i,
-                                             int32_t q0, int32_t ne, int32_t st, int32_t stop_gain, int32_t thr,
+// candidate q0 + t, tests it against the shared copy of the part slacks, and
+// the first lane in candidate order whose candidate ends the scan decides.
+// The scan ends at a candidate whose gain is <= stop_gain (returns -2 - q:
+// the caller goes on elsewhere from q), at one whose gain is <= thr (returns
+// -1), or at a feasible one (returns its part); running out returns -2 - ne.
+// `pre` holds candidates 0..31 already loaded (used when q0 == 0).
+template <typename S, int NC>
+__device__ __forceinline__ int32_t coop_scan(const S* sslack, int lane, const WalkBuf& b, int i, int32_t q0,
+                                             int32_t ne, int32_t stop_gain, int32_t thr,
                                              const idx_t* __restrict__ cand_p, const idx_t* __restrict__ cand_g,
-                                             const int32_t* w) {
+                                             const int32_t* w, const CandChunk& pre) {
+  const int32_t st = b.coff[i];
   for (int32_t base = q0; base < ne; base += 32) {
     const int32_t q = base + lane;
     const bool valid = q < ne;
     int32_t g = 0, p = -1;
-    if (valid) {
+    if (base == 0) {
+      g = pre.g;
+      p = pre.p;
+    } else if (valid) {
       g = q < kInline ? b.cg[i * kInline + q] : __ldg(&cand_g[st + q]);
       p = q < kInline ? b.cp[i * kInline + q] : __ldg(&cand_p[st + q]);
     }
     const bool stop = valid && g <= stop_gain;
     const bool below = valid && g <= thr;
-    const bool fits = gather_fits(s, valid ? p : -1, w);
+    bool fits = valid;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) fits = fits && (S)w[c] <= sslack[(valid ? p : 0) * NC + c];
     const unsigned m = __ballot_sync(0xffffffffu, stop || below || fits);
     if (m) {
       const int l = __ffs(m) - 1;
@@ -571,16 +594,18 @@ __device__ __forceinline__ int32_t coop_scan(const PartRegs<S, R, NC>& s, int la
 // :131-164 cut), in the reference's candidate order: explicit candidates with
 // gain above the non-adjacent gain ig = -w_from, then the non-adjacent parts
 // by id, then the explicit ones at or below ig; the first feasible one with
-// gain above the pass threshold, or -1. The first kInline candidates come
-// from the shared-memory record one at a time; longer lists (a vertex next to
-// many parts) are scanned 32 candidates per step, and membership in the
-// candidate list for the non-adjacent step comes from a shared bitmap `ebits`
-// (R words, zero between calls).
+// gain above the pass threshold, or -1. Explicit candidates are tested 32 at
+// a time against the shared slack copy `sslack`; membership in the candidate
+// list for the non-adjacent step comes from the inline slots, or for longer
+// lists from a shared bitmap `ebits` (R words, zero between calls).
+// The decision of one mover when no mover of the pass has more candidates
+// than the inline slots (the same order as reg_decide; a longer list, which
+// the walk's flag rules out, would still be read correctly from global
+// memory one candidate at a time).
 template <int MODE, typename S, int R, int NC>
-__device__ __forceinline__ int32_t reg_decide(const PartRegs<S, R, NC>& s, int lane, const WalkBuf& b, int i,
-                                              int32_t k, const idx_t* __restrict__ cand_p,
-                                              const idx_t* __restrict__ cand_g, const int32_t* w,
-                                              unsigned* ebits) {
+__device__ __forceinline__ int32_t lean_decide(const PartRegs<S, R, NC>& s, int lane, const WalkBuf& b, int i,
+                                               int32_t k, const idx_t* __restrict__ cand_p,
+                                              const idx_t* __restrict__ cand_g, const int32_t* w) {
   const int32_t pv = b.pv[i];
   if (MODE == kRepair) {
     bool over = false;
@@ -598,22 +623,70 @@ __device__ __forceinline__ int32_t reg_decide(const PartRegs<S, R, NC>& s, int l
   const int32_t ne = b.ne[i];
   const int32_t st = b.coff[i];
   const int32_t ig = (int32_t)(0u - (uint32_t)b.wf[i]);
-  const int32_t nin = ne < kInline ? ne : kInline;
+  auto cpart = [&](int32_t q) { return q < kInline ? b.cp[i * kInline + q] : cand_p[st + q]; };
+  auto cgain = [&](int32_t q) { return q < kInline ? b.cg[i * kInline + q] : cand_g[st + q]; };
   int32_t q = 0;
-  for (; q < nin; ++q) {
-    const int32_t g = b.cg[i * kInline + q];
+  for (; q < ne; ++q) {
+    const int32_t g = cgain(q);
     if (g <= ig) break;
     if (g <= thr) return -1;
-    const int32_t p = b.cp[i * kInline + q];
+    const int32_t p = cpart(q);
     if (__any_sync(0xffffffffu, lane_fits(s, lane, p, w))) return p;
   }
-  if (q == kInline && ne > kInline) {
-    const int32_t r1 = coop_scan(s, lane, b, i, q, ne, st, ig, thr, cand_p, cand_g, w);
-    if (r1 >= -1) return r1;
-    q = -2 - r1;
-  }
   if (ig > thr) {
-    if (ne <= kInline) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int32_t p = r * 32 + lane;
+      bool ok = p < k && p != pv;
+      if (ok)
+        for (int32_t e = 0; e < ne; ++e)
+          if (cpart(e) == p) { ok = false; break; }
+#pragma unroll
+      for (int c = 0; c < NC; ++c) ok = ok && (S)w[c] <= s.sl[r][c];
+      const unsigned m = __ballot_sync(0xffffffffu, ok);
+      if (m) return r * 32 + __ffs(m) - 1;
+    }
+  }
+  for (; q < ne; ++q) {
+    const int32_t g = cgain(q);
+    if (g <= thr) return -1;
+    const int32_t p = cpart(q);
+    if (__any_sync(0xffffffffu, lane_fits(s, lane, p, w))) return p;
+  }
+  return -1;
+}
+
+template <int MODE, typename S, int R, int NC>
+__device__ __forceinline__ int32_t reg_decide(const PartRegs<S, R, NC>& s, int lane,
+                                              const WalkBuf& b, int i, int32_t k, const idx_t* __restrict__ cand_p,
+                                              const idx_t* __restrict__ cand_g, const int32_t* w, unsigned* ebits,
+                                              const CandChunk* pre, S* sslack, bool& dirty) {
+  const int32_t pv = b.pv[i];
+  if (MODE == kRepair) {
+    bool over = false;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+        if (pv == r * 32 + lane && s.ov[r][c] < 0) over = true;
+    if (!__any_sync(0xffffffffu, over)) return -1;
+  }
+  const int32_t thr = (MODE == kRepair) ? INT_MIN : 0;
+  const int32_t ne = b.ne[i];
+  const int32_t st = b.coff[i];
+  const int32_t ig = (int32_t)(0u - (uint32_t)b.wf[i]);
+  if (ne <= kInline) {
+    // Short list, all in the shared-memory record: one candidate at a time
+    // against the owner lane's register slack.
+    int32_t q = 0;
+    for (; q < ne; ++q) {
+      const int32_t g = b.cg[i * kInline + q];
+      if (g <= ig) break;
+      if (g <= thr) return -1;
+      const int32_t p = b.cp[i * kInline + q];
+      if (__any_sync(0xffffffffu, lane_fits(s, lane, p, w))) return p;
+    }
+    if (ig > thr) {
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const int32_t p = r * 32 + lane;
@@ -625,7 +698,35 @@ __device__ __forceinline__ int32_t reg_decide(const PartRegs<S, R, NC>& s, int l
         const unsigned m = __ballot_sync(0xffffffffu, ok);
         if (m) return r * 32 + __ffs(m) - 1;
       }
-    } else {
+    }
+    for (; q < ne; ++q) {
+      const int32_t g = b.cg[i * kInline + q];
+      if (g <= thr) return -1;
+      const int32_t p = b.cp[i * kInline + q];
+      if (__any_sync(0xffffffffu, lane_fits(s, lane, p, w))) return p;
+    }
+    return -1;
+  }
+  // Long list: 32 candidates per step against the shared slack copy, brought
+  // up to date first if a move happened since it was last written. kLong
+  // movers of the cut pass come with their first 32 candidates prefetched.
+  const CandChunk pc = pre ? *pre : first_chunk(b, i, lane, cand_p, cand_g);
+  if (dirty) {
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) sslack[(r * 32 + lane) * NC + c] = s.sl[r][c];
+    __syncwarp();
+    dirty = false;
+  }
+  int32_t q;
+  {
+    const int32_t r1 = coop_scan<S, NC>(sslack, lane, b, i, 0, ne, ig, thr, cand_p, cand_g, w, pc);
+    if (r1 >= -1) return r1;
+    q = -2 - r1;
+  }
+  if (ig > thr) {
+    {
       for (int32_t base = 0; base < ne; base += 32) {
         const int32_t e = base + lane;
         if (e < ne) {
@@ -653,17 +754,92 @@ __device__ __forceinline__ int32_t reg_decide(const PartRegs<S, R, NC>& s, int l
     // The candidate at q has gain <= ig <= thr, and the rest are lower.
     return -1;
   }
-  if (ne > kInline) {
-    const int32_t r3 = coop_scan(s, lane, b, i, q, ne, st, INT_MIN, thr, cand_p, cand_g, w);
-    return r3 >= -1 ? r3 : -1;
+  if (q >= ne) return -1;
+  const int32_t r3 = coop_scan<S, NC>(sslack, lane, b, i, q, ne, INT_MIN, thr, cand_p, cand_g, w, pc);
+  return r3 >= -1 ? r3 : -1;
+}
+
+
+// The chunk loop of k_walk_reg. LONG: many movers of the pass have more
+// candidates than the inline slots, so the long-list decision (shared slack
+// copy, candidates 32 at a time, prefetch) is compiled in; without it every
+// mover takes the short decision, which reads long lists one candidate at a
+// time. Both give the same decisions.
+template <int MODE, typename S, int R, int NC, bool LONG>
+__device__ __forceinline__ void walk_chunks(int32_t nm, const MoverRecs& r, int32_t k,
+                                            const idx_t* __restrict__ cand_p, const idx_t* __restrict__ cand_g,
+                                            idx_t* __restrict__ d_out, WalkBuf* buf, int32_t* dbuf, unsigned* ebits,
+                                            S* sslack, PartRegs<S, R, NC>& s, int32_t& moves, int tid, int lane,
+                                            int warp) {
+  bool dirty = false;  // a move since sslack was last written
+  const int32_t nchunks = (int32_t)ceil_div(nm, kWalkChunk);
+  for (int32_t ch = 0; ch < nchunks; ++ch) {
+    const int32_t j0 = ch * kWalkChunk;
+    const int32_t cnt = min(kWalkChunk, nm - j0);
+    if (warp == 0) {
+      const WalkBuf& b = buf[ch & 1];
+      auto c_of = [&](int i, int q) { return b.cg[i * kInline + q] > 0 ? b.cp[i * kInline + q] : -1; };
+      // kContended and kLong movers take the general decision (in the repair
+      // pass every mover is kContended, and most leave at the overweight
+      // test); the first candidates of a kLong mover are loaded one mover
+      // ahead.
+      int32_t nk = b.known[0], npv = b.pv[0], nc1 = c_of(0, 0), nc2 = c_of(0, 1);
+      int32_t nw[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) nw[c] = b.vw[c];
+      CandChunk npre{0, -1};
+      if (LONG && MODE == kCut && nk == kLong) npre = first_chunk(b, 0, lane, cand_p, cand_g);
+      for (int32_t i = 0; i < cnt; ++i) {
+        const int32_t kn = nk, pv = npv, c1 = nc1, c2 = nc2;
+        int32_t w[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) w[c] = nw[c];
+        CandChunk pre = npre;
+        if (i + 1 < cnt) {
+          nk = b.known[i + 1];
+          npv = b.pv[i + 1];
+          nc1 = c_of(i + 1, 0);
+          nc2 = c_of(i + 1, 1);
+#pragma unroll
+          for (int c = 0; c < NC; ++c) nw[c] = b.vw[(i + 1) * kMaxCon + c];
+          if (LONG && MODE == kCut && nk == kLong) npre = first_chunk(b, i + 1, lane, cand_p, cand_g);
+        }
+        int32_t d = kn;
+        if (MODE == kCut && kn == kFast) {
+          const bool f1 = __any_sync(0xffffffffu, lane_fits(s, lane, c1, w));
+          const bool f2 = __any_sync(0xffffffffu, lane_fits(s, lane, c2, w));
+          d = f1 ? c1 : (f2 ? c2 : -1);
+        } else if (kn <= kContended && kn != kFast) {  // kContended or kLong (this form keeps the
+                                                        // common kFast path short)
+          if (LONG)
+            d = reg_decide<MODE, S, R, NC>(s, lane, b, i, k, cand_p, cand_g, w, ebits,
+                                           MODE == kCut && kn == kLong ? &pre : nullptr, sslack, dirty);
+          else
+            d = lean_decide<MODE, S, R, NC>(s, lane, b, i, k, cand_p, cand_g, w);
+        }
+        if (lane == 0) dbuf[i] = d;
+        if (d >= 0) {
+#pragma unroll
+          for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              const S dw = (S)w[c];
+              const int32_t p = rr * 32 + lane;
+              const S delta = (pv == p ? dw : (S)0) - (d == p ? dw : (S)0);
+              s.sl[rr][c] += delta;
+              s.ov[rr][c] += delta;
+            }
+          dirty = true;
+          ++moves;
+        }
+      }
+      __syncwarp();
+      for (int32_t i = lane; i < cnt; i += 32) d_out[j0 + i] = dbuf[i];
+    } else if (ch + 1 < nchunks) {
+      walk_load(buf[(ch + 1) & 1], r, (ch + 1) * kWalkChunk, nm, NC, tid - 32, blockDim.x - 32);
+    }
+    __syncthreads();
   }
-  for (; q < ne; ++q) {
-    const int32_t g = b.cg[i * kInline + q];
-    if (g <= thr) return -1;
-    const int32_t p = b.cp[i * kInline + q];
-    if (__any_sync(0xffffffffu, lane_fits(s, lane, p, w))) return p;
-  }
-  return -1;
 }
 
 // Register-resident walk for k <= 32*R parts and NC <= 2 constraints. Only
@@ -684,11 +860,16 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
                                                            long long* __restrict__ pw,
                                                            const long long* __restrict__ feas_g,
                                                            const long long* __restrict__ over_g,
-                                                           idx_t* __restrict__ d_out, int32_t* __restrict__ nmoves) {
+                                                           idx_t* __restrict__ d_out, int32_t* __restrict__ nmoves,
+                                                           int32_t* __restrict__ long_flag) {
   __shared__ WalkBuf buf[2];
   __shared__ int32_t dbuf[kWalkChunk];
   __shared__ unsigned ebits[R];
+  __shared__ S sslack[32 * R * NC];  // copy of the feasibility slacks for the long-list scans
   const int32_t nm = *nm_dev;
+  // The long-list version of the loop pays off when long lists are common
+  // (count from k_walk_prep / k_walk_classify); both versions decide alike.
+  const bool any_long = (long long)*long_flag * 16 > (long long)nm;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid < R) ebits[tid] = 0u;
   PartRegs<S, R, NC> s;
@@ -703,65 +884,19 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
         // Parts beyond k are never feasible and never overweight.
         s.sl[rr][c] = in ? (S)(feas_g[p * NC + c] - x) : (S)(-(1 << 30));
         s.ov[rr][c] = in ? (S)(over_g[p * NC + c] - x) : (S)(1 << 30);
+        sslack[p * NC + c] = s.sl[rr][c];
       }
     }
   }
   if (nm > 0) walk_load(buf[0], r, 0, nm, NC, tid, blockDim.x);
   __syncthreads();
   int32_t moves = 0;
-  const int32_t nchunks = (int32_t)ceil_div(nm, kWalkChunk);
-  for (int32_t ch = 0; ch < nchunks; ++ch) {
-    const int32_t j0 = ch * kWalkChunk;
-    const int32_t cnt = min(kWalkChunk, nm - j0);
-    if (warp == 0) {
-      const WalkBuf& b = buf[ch & 1];
-      auto c_of = [&](int i, int q) { return b.cg[i * kInline + q] > 0 ? b.cp[i * kInline + q] : -1; };
-      int32_t nk = b.known[0], npv = b.pv[0], nc1 = c_of(0, 0), nc2 = c_of(0, 1);
-      int32_t nw[NC];
-#pragma unroll
-      for (int c = 0; c < NC; ++c) nw[c] = b.vw[c];
-      for (int32_t i = 0; i < cnt; ++i) {
-        const int32_t kn = nk, pv = npv, c1 = nc1, c2 = nc2;
-        int32_t w[NC];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) w[c] = nw[c];
-        if (i + 1 < cnt) {
-          nk = b.known[i + 1];
-          npv = b.pv[i + 1];
-          nc1 = c_of(i + 1, 0);
-          nc2 = c_of(i + 1, 1);
-#pragma unroll
-          for (int c = 0; c < NC; ++c) nw[c] = b.vw[(i + 1) * kMaxCon + c];
-        }
-        int32_t d = kn;
-        if (MODE == kCut && kn == kFast) {
-          const bool f1 = __any_sync(0xffffffffu, lane_fits(s, lane, c1, w));
-          const bool f2 = __any_sync(0xffffffffu, lane_fits(s, lane, c2, w));
-          d = f1 ? c1 : (f2 ? c2 : -1);
-        } else if (kn == kContended || kn == kFast) {
-          d = reg_decide<MODE, S, R, NC>(s, lane, b, i, k, cand_p, cand_g, w, ebits);
-        }
-        if (lane == 0) dbuf[i] = d;
-        if (d >= 0) {
-#pragma unroll
-          for (int rr = 0; rr < R; ++rr)
-#pragma unroll
-            for (int c = 0; c < NC; ++c) {
-              const S dw = (S)w[c];
-              const S delta = (pv == rr * 32 + lane ? dw : (S)0) - (d == rr * 32 + lane ? dw : (S)0);
-              s.sl[rr][c] += delta;
-              s.ov[rr][c] += delta;
-            }
-          ++moves;
-        }
-      }
-      __syncwarp();
-      for (int32_t i = lane; i < cnt; i += 32) d_out[j0 + i] = dbuf[i];
-    } else if (ch + 1 < nchunks) {
-      walk_load(buf[(ch + 1) & 1], r, (ch + 1) * kWalkChunk, nm, NC, tid - 32, blockDim.x - 32);
-    }
-    __syncthreads();
-  }
+  if (any_long)
+    walk_chunks<MODE, S, R, NC, true>(nm, r, k, cand_p, cand_g, d_out, buf, dbuf, ebits, sslack, s, moves, tid, lane,
+                                      warp);
+  else
+    walk_chunks<MODE, S, R, NC, false>(nm, r, k, cand_p, cand_g, d_out, buf, dbuf, ebits, sslack, s, moves, tid,
+                                       lane, warp);
   if (warp == 0) {
 #pragma unroll
     for (int rr = 0; rr < R; ++rr) {
@@ -771,7 +906,10 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
         for (int c = 0; c < NC; ++c) pw[p * NC + c] = feas_g[p * NC + c] - (long long)s.sl[rr][c];
     }
   }
-  if (tid == 0) *nmoves = moves;
+  if (tid == 0) {
+    *nmoves = moves;
+    *long_flag = 0;  // every thread read it before the first barrier
+  }
 }
 
 // Apply the pass's moves together (greedy.rs:111-119, :168-181).
@@ -831,7 +969,7 @@ static int launch_walk(int32_t nmax, const int32_t* nm_dev, const idx_t* movers,
                         int k, const idx_t* ncand, const idx_t* wfrom, const idx_t* cand_p, const idx_t* cand_g,
                         const MoverRecs& r, long long* pw, const long long* feas, const long long* over,
                         long long* in_max, long long* out_max, idx_t* d_out, int32_t* nmoves, bool small_weights,
-                        cudaStream_t st) {
+                        int32_t* long_flag, cudaStream_t st) {
   const int32_t K = k * g.ncon;
   const int blocks = grid_for(nmax, 256);
   if (MODE == kCut) {
@@ -839,17 +977,18 @@ static int launch_walk(int32_t nmax, const int32_t* nm_dev, const idx_t* movers,
     RMB_CUDA(cudaMemsetAsync(out_max, 0, sizeof(long long) * (size_t)K, st));
   }
   k_walk_prep<MODE><<<blocks, 256, 0, st>>>(nm_dev, movers, part, g.vwgt, g.ncon, g.xadj, ncand, wfrom, cand_p,
-                                            cand_g, r, in_max, out_max);
+                                            cand_g, r, in_max, out_max, long_flag);
   RMB_LAUNCH_CHECK();
   if (MODE == kCut) {
-    k_walk_classify<<<blocks, 256, 0, st>>>(nm_dev, g.ncon, cand_p, cand_g, r, pw, feas, in_max, out_max);
+    k_walk_classify<<<blocks, 256, 0, st>>>(nm_dev, g.ncon, cand_p, cand_g, r, pw, feas, in_max, out_max,
+                                            long_flag);
     RMB_LAUNCH_CHECK();
   }
   const int ph = profiler().begin(kProfDecide, st);
   const int ncon = g.ncon;
 #define RMB_WALK_REG(ST, RR, NCC)                                                                     \
   k_walk_reg<MODE, ST, RR, NCC><<<1, kWalkThreads, 0, st>>>(nm_dev, r, k, cand_p, cand_g, pw, feas, over, d_out, \
-                                                            nmoves)
+                                                            nmoves, long_flag)
 #define RMB_WALK_REG_R(ST, NCC)                       \
   do {                                                \
     if (rr == 1) RMB_WALK_REG(ST, 1, NCC);            \
@@ -909,6 +1048,10 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
   idx_t* dec = arena.alloc<idx_t>((size_t)g.n);
   // Per pass: [2*pass] movers, [2*pass+1] moves.
   int32_t* counters = arena.alloc<int32_t>(2 * ((size_t)rp.niter + 1));
+  // Number of a pass's movers with more candidates than the inline slots,
+  // counted by prep/classify; the register walk reads and clears it.
+  int32_t* long_flag = arena.alloc<int32_t>(1);
+  RMB_CUDA(cudaMemsetAsync(long_flag, 0, sizeof(int32_t), st));
   MoverRecs r;
   r.pv = arena.alloc<int32_t>((size_t)g.n);
   r.ne = arena.alloc<int32_t>((size_t)g.n);
@@ -938,11 +1081,11 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
     if (mode == kRepair)
       walk_handles.push_back(launch_walk<kRepair>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r,
                                                   pw, rp.feas_max, rp.over_thr, in_max, out_max, dec, nm_dev + 1,
-                                                  rp.small_weights, st));
+                                                  rp.small_weights, long_flag, st));
     else
       walk_handles.push_back(launch_walk<kCut>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r, pw,
                                                rp.feas_max, rp.over_thr, in_max, out_max, dec, nm_dev + 1,
-                                               rp.small_weights, st));
+                                               rp.small_weights, long_flag, st));
   }
   static const bool trace = std::getenv("RMETIS_B200_TRACE") != nullptr;
   if (profiler().on) {

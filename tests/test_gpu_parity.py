@@ -348,3 +348,47 @@ def test_pipeline_replay_rmat_k256(rmb, oracle):
     assert rc == 1
     assert obj == res.objval
     assert (part == res.part).all()
+
+
+@pytest.mark.parametrize("k", [7, 64, 200, 1024, 1100])
+def test_grow_leftovers_unweighted(rmb, oracle, k):
+    """Thousands of isolated vertices (R-MAT) go to the lightest part one by
+    one (src/initial/grow.rs:88-100); unweighted graphs take the level-by-level
+    form of that rule up to k = 1024 and the plain argmin above it."""
+    from rmetis_b200 import functions as F
+    x, a = G.rmat(12, seed=7)
+    n = len(x) - 1
+    assert (np.diff(x) == 0).sum() > 500
+    t = oracle.compute_target_weights(n, 1, None, k)
+    seeds = np.stack([np.random.default_rng(40 + i).choice(n, k, replace=False) for i in range(3)]).astype(np.int32)
+    parts, _ = F.grow_partition(rmb.Graph(n, 1, x, a), k, t, seeds)
+    for i in range(3):
+        ref, _ = oracle.grow_partition(x, a, k, t, seeds=seeds[i])
+        assert (parts[i] == ref).all()
+
+
+def test_grow_leftovers_skewed_levels(rmb, oracle):
+    """Parts of very different weights before the leftovers: the levels pass
+    many part weights before every part takes part."""
+    from rmetis_b200 import functions as F
+    # a long path, a few short paths and many isolated vertices
+    xs, as_ = [], []
+    off = 0
+    sizes = [3000, 40, 25, 5] + [1] * 4000
+    for sz in sizes:
+        if sz == 1:
+            xs.append(np.array([0], np.int64)); as_.append(np.zeros(0, np.int64))
+        else:
+            px, pa = G.path(sz)
+            xs.append(px[:-1].astype(np.int64)); as_.append(pa.astype(np.int64) + off)
+        off += sz
+    nnz = np.cumsum([0] + [len(q) for q in as_])
+    x = np.concatenate([xs[i] + nnz[i] for i in range(len(xs))] + [np.array([nnz[-1]])]).astype(np.int32)
+    a = np.concatenate(as_).astype(np.int32)
+    n = len(x) - 1
+    k = 24
+    t = oracle.compute_target_weights(n, 1, None, k)
+    seeds = np.array([[0, 1500, 2999, 3000, 3040, 3065] + list(range(3070, 3088))], np.int32)
+    parts, _ = F.grow_partition(rmb.Graph(n, 1, x, a), k, t, seeds)
+    ref, _ = oracle.grow_partition(x, a, k, t, seeds=seeds[0])
+    assert (parts[0] == ref).all()
