@@ -14,6 +14,19 @@ shard within one graph); value = N * m / max-over-ranks step time.
 
 --impl reference times the oracle (CPU restatement of the reference) on the
 host cores instead; rank 0 only.
+
+Further workloads (one JSON line each, same keys):
+  --workload rmat_seeds  R-MAT scale 22 (--scale), k=256, ncuts=16: the 16
+                         attempts concurrently on the device's worker pool vs
+                         one after another (the plain path), attempts/s.
+  --workload rgg_batch   512 uneven 2D RGGs (--graphs), ncon=2, k in
+                         {2..64}, ufactor=50: one batched call vs plain calls
+                         one graph at a time, graphs/s.
+  --workload serving     Poisson arrivals (--rates, --requests) of 2D grid /
+                         3D grid / RGG requests, n log-uniform in [1e4, 2e6],
+                         k in {2..128}, through the asynchronous API; p50/p99
+                         latency and throughput vs the plain path serving the
+                         same arrivals one request at a time.
 """
 from __future__ import annotations
 
@@ -45,6 +58,7 @@ WORKLOADS = {
     "grid2d_64": (lambda: G.grid2d(64, 64) + (None, None), 8, 1,
                   "2D 5-point grid 64x64, unit weights, nparts=8, Shem+Greedy, ufactor=30, ncuts=1, seed=1"),
 }
+EXTRA_WORKLOADS = ("rmat_seeds", "rgg_batch", "serving")
 CPU_SAMPLE = {
     "grid3d_128": (lambda: G.grid3d(64, weights_seed=7), "3D 7-point grid 64^3 (same weight laws), nparts=64"),
     "grid2d_64": (lambda: G.grid2d(64, 64) + (None, None), "2D grid 64x64, nparts=8"),
@@ -193,13 +207,381 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+# ---------------------------------------------------------------------------
+# Batched seeds, batched graphs and the serving stream
+# ---------------------------------------------------------------------------
+def _setup_device():
+    import torch
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    return torch, torch.device("cuda", local_rank), local_rank
+
+
+def _device_call(lib, torch, dev, x, a, v, w, k, opts, ncon=1):
+    """A closure running one RMETIS_GPU_PartGraphKwayDevice call on
+    device-resident copies of the graph; returns (call, part tensor, objval)."""
+    I32P = ctypes.POINTER(ctypes.c_int32)
+    t = lambda arr: None if arr is None else torch.from_numpy(np.ascontiguousarray(arr, np.int32)).to(dev)
+    dx, da, dv, dw = t(x), t(a), t(v), t(w)
+    n = len(x) - 1
+    dpart = torch.empty(n, dtype=torch.int32, device=dev)
+    nv, nc, npr = ctypes.c_int32(n), ctypes.c_int32(ncon), ctypes.c_int32(k)
+    obj = ctypes.c_int32(0)
+    op = opts.ctypes.data_as(I32P)
+    ptr = lambda tt: None if tt is None else tt.data_ptr()
+
+    def call():
+        rc = lib.RMETIS_GPU_PartGraphKwayDevice(ctypes.byref(nv), ctypes.byref(nc), ptr(dx), ptr(da), ptr(dv),
+                                                ptr(dw), ctypes.byref(npr), None, None, op, ctypes.byref(obj),
+                                                ptr(dpart))
+        if rc != 1:
+            raise RuntimeError(f"RMETIS_GPU_PartGraphKwayDevice returned {rc}")
+    return call, dpart, obj
+
+
+def _timed(torch, stream, fn, reps):
+    """Device time of fn() per call (CUDA events on the caller's stream; the
+    call returns only when all its work, on any stream, is done)."""
+    out = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def run_rmat_seeds(args):
+    """R-MAT, k=256, 16 attempts (seed 1+attempt), best cut kept."""
+    torch, dev, local_rank = _setup_device()
+    import rmetis_b200 as rmb
+    lib = rmb._lib.load()
+    k, ncuts, seed = 256, 16, 1
+    t0 = time.perf_counter()
+    x, a = G.rmat_device(args.scale, seed=22)
+    gen_s = time.perf_counter() - t0
+    n, m = len(x) - 1, len(a)
+    stream = torch.cuda.current_stream(dev)
+    assert lib.RMETIS_GPU_SetStream(stream.cuda_stream) == 1
+    call16, dpart16, obj16 = _device_call(lib, torch, dev, x, a, None, None, k, kway_options(seed, ncuts=ncuts))
+    warm = max(1, min(args.warmup, 2))
+    reps = max(1, min(args.steps, 3))
+    rmb.set_tuning(parallel_attempts=1)
+    for _ in range(warm):
+        call16()
+    sampler = ClockSampler(gpu_id_for(local_rank))
+    sampler.start()
+    tw0 = time.time()
+    batched = _timed(torch, stream, call16, reps)
+    tw1 = time.time()
+    sampler.stop()
+    best_batched = (int(obj16.value), dpart16.cpu().numpy().copy())
+    # The plain path: the same 16 attempts one after another.
+    rmb.set_tuning(parallel_attempts=0)
+    plain = _timed(torch, stream, call16, 1)
+    rmb.set_tuning(parallel_attempts=1)
+    same = int(obj16.value) == best_batched[0] and bool((dpart16.cpu().numpy() == best_batched[1]).all())
+    # One attempt, profiled, for the roofline of the dominant kernel.
+    call1, _, obj1 = _device_call(lib, torch, dev, x, a, None, None, k, kway_options(seed, ncuts=1))
+    call1()
+    prof = _profile_one(lib, torch, call1)
+    # e2e: the drop-in C ABI with pinned host buffers, 16 attempts.
+    e2e_ms = _host_call_ms(lib, torch, x, a, None, None, k, kway_options(seed, ncuts=ncuts))
+    ms = float(np.mean(batched))
+    line = {
+        "metric": "k-way attempt-edges/s (batched seeds, best of 16)", "value": ncuts * m / (ms / 1e3),
+        "unit": "edges/s", "n_gpus": 1, "steps": reps, "warmup": warm, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": f"R-MAT scale {args.scale} (a,b,c=.57,.19,.19, edge factor 16, torch seed 22, "
+                               "symmetrised, deduplicated), unit weights, nparts=256, ncuts=16 (seed 1+attempt), "
+                               "Shem+Greedy, ufactor=30", "name": "rmat_seeds", "n": n, "m": m,
+                   "generation_s": round(gen_s, 1), "l2": "inputs larger than L2"},
+        "objval": int(obj16.value), "objval_first_attempt": int(obj1.value),
+        "attempts_per_s": ncuts / (ms / 1e3),
+        "plain_gpu": {"ms": plain[0], "attempts_per_s": ncuts / (plain[0] / 1e3), "same_result": same},
+        "speedup_vs_plain_gpu": plain[0] / ms,
+        "e2e": {"value": ncuts * m / (e2e_ms / 1e3), "unit": "edges/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(4 * (len(x) + len(a))), "d2h_bytes_per_step": int(4 * n + 4)},
+        "roofline": prof["roofline"], "kernels_one_attempt": prof["kernels"],
+        "gpu_launches": prof["launches"],
+        "clocks": sampler.summary(tw0, tw1),
+    }
+    if not args.no_cpu_baseline:
+        # The oracle's cost on R-MAT grows with sum(deg^2) (row merges) and
+        # k*deg (gains); one attempt on a scale-16 graph of the same law.
+        from oracle import oracle as O
+        xs, as_ = G.rmat_device(16, seed=22)
+        t0 = time.perf_counter()
+        rc, _, cobj = O.part_graph_kway(xs, as_, k, options=kway_options(seed))
+        dt = time.perf_counter() - t0
+        assert rc == 1
+        line["cpu_baseline"] = {"value": len(as_) / dt, "unit": "edges/s (attempt-edges)", "cores": 1,
+                                "kind": "port", "sample": f"R-MAT scale 16 (n={len(xs) - 1}, m={len(as_)}), "
+                                f"k=256, 1 attempt, {dt:.2f} s, cut {cobj}"}
+    print(json.dumps(line))
+
+
+def _profile_one(lib, torch, call):
+    """Per-kernel CUDA-event totals of one call, and the roofline of the kernel
+    with the most device time among those with counted bytes."""
+    nprof = 6
+    launches = (ctypes.c_int64 * (nprof + 1))()
+    ms_k = (ctypes.c_double * nprof)()
+    bytes_k = (ctypes.c_double * nprof)()
+    lib.RMETIS_GPU_GetProfile(launches, ms_k, bytes_k, nprof + 1)
+    l0 = [launches[i] for i in range(nprof + 1)]
+    m0 = [ms_k[i] for i in range(nprof)]
+    b0 = [bytes_k[i] for i in range(nprof)]
+    lib.RMETIS_GPU_SetProfiling(1)
+    call()
+    torch.cuda.synchronize()
+    lib.RMETIS_GPU_GetProfile(launches, ms_k, bytes_k, nprof + 1)
+    lib.RMETIS_GPU_SetProfiling(0)
+    names = ["k_gain", "k_walk", "k_match_propose", "k_contract_thread", "k_cut", "k_grow"]
+    L = [launches[i] - l0[i] for i in range(nprof)]
+    M = [ms_k[i] - m0[i] for i in range(nprof)]
+    B = [bytes_k[i] - b0[i] for i in range(nprof)]
+    dom = max(range(nprof), key=lambda i: M[i] if B[i] > 0 else -1.0)
+    avg_ms = M[dom] / max(1, L[dom])
+    avg_b = B[dom] / max(1, L[dom])
+    peak, kind = load_peaks()
+    ach = (avg_b / (avg_ms / 1e3)) / 1e9 if avg_ms > 0 else 0.0
+    return {"roofline": {"bound": "hbm", "kernel": names[dom], "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "peak_source": kind, "traffic": None, "bytes_per_launch": avg_b,
+                         "ms_per_launch": avg_ms},
+            "kernels": {names[i]: {"launches": int(L[i]), "ms": round(M[i], 3)} for i in range(nprof)},
+            "launches": int(launches[nprof] - l0[nprof])}
+
+
+def _host_call_ms(lib, torch, x, a, v, w, k, opts, ncon=1, reps=1):
+    I32P = ctypes.POINTER(ctypes.c_int32)
+    pin = lambda arr: None if arr is None else torch.from_numpy(np.ascontiguousarray(arr, np.int32)).pin_memory()
+    hx, ha, hv, hw = pin(x), pin(a), pin(v), pin(w)
+    n = len(x) - 1
+    hpart = torch.empty(n, dtype=torch.int32).pin_memory()
+    hp = lambda tt: None if tt is None else ctypes.cast(tt.data_ptr(), I32P)
+    nv, nc, npr, obj = ctypes.c_int32(n), ctypes.c_int32(ncon), ctypes.c_int32(k), ctypes.c_int32(0)
+    op = opts.ctypes.data_as(I32P)
+    out = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        rc = lib.RMETIS_PartGraphKway(ctypes.byref(nv), ctypes.byref(nc), hp(hx), hp(ha), hp(hv), None, hp(hw),
+                                      ctypes.byref(npr), None, None, op, ctypes.byref(obj), hp(hpart))
+        out.append((time.perf_counter() - t0) * 1e3)
+        if rc != 1:
+            raise RuntimeError(f"RMETIS_PartGraphKway returned {rc}")
+    return float(np.mean(out))
+
+
+def _rgg_batch_graphs(count):
+    """Graph i: n log-uniform in [1e3, 2e5], k from {2,4,...,64}, vertex
+    weights U{1..8} on 2 constraints (numpy default_rng([4, i])), points and
+    edges from the device generator seeded by the same stream."""
+    out = []
+    for i in range(count):
+        rng = np.random.default_rng([4, i])
+        n = int(np.exp(rng.uniform(np.log(1e3), np.log(2e5))))
+        k = int(rng.choice([2, 4, 8, 16, 32, 64]))
+        x, a, w = G.rgg2d_device(n, int(rng.integers(1 << 31)), 10.0)
+        v = rng.integers(1, 9, size=2 * n).astype(np.int32)
+        out.append((x, a, v, w, k))
+    return out
+
+
+def run_rgg_batch(args):
+    torch, dev, local_rank = _setup_device()
+    import rmetis_b200 as rmb
+    t0 = time.perf_counter()
+    specs = _rgg_batch_graphs(args.graphs)
+    gen_s = time.perf_counter() - t0
+    graphs = [rmb.Graph(len(x) - 1, 2, x, a, vwgt=v, adjwgt=w, validate=False) for x, a, v, w, _ in specs]
+    ks = [k for *_, k in specs]
+    n_tot = sum(g.nvtxs for g in graphs)
+    m_tot = sum(len(g.adjncy) for g in graphs)
+    o = rmb.Options(rtype=rmb.RType.Greedy, seed=1, ufactor=50)
+    warm = max(1, min(args.warmup, 2))
+    reps = max(1, min(args.steps, 3))
+    for _ in range(warm):
+        rmb.part_graph_kway_batch(graphs, ks, options=o)
+    sampler = ClockSampler(gpu_id_for(local_rank))
+    sampler.start()
+    tw0 = time.time()
+    bt = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = rmb.part_graph_kway_batch(graphs, ks, options=o)
+        bt.append(time.perf_counter() - t0)
+    tw1 = time.time()
+    sampler.stop()
+    # The plain path: the same graphs one call after another.
+    t0 = time.perf_counter()
+    plain = [rmb.part_graph_kway(g, kk, options=o) for g, kk in zip(graphs, ks)]
+    pt = time.perf_counter() - t0
+    same = all(r.objval == p.objval and bool((r.part == p.part).all()) for r, p in zip(res, plain))
+    b = float(np.mean(bt))
+    line = {
+        "metric": "k-way graphs/s (batched uneven graphs)", "value": args.graphs / b, "unit": "graphs/s",
+        "n_gpus": 1, "steps": reps, "warmup": warm, "ms_per_step": b * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": f"{args.graphs} 2D RGGs, n log-uniform [1e3, 2e5], mean degree 10, "
+                               "edge w = 1+floor(10(1-d/r)), ncon=2 vwgt U{1..8}, k from {2,..,64}, ufactor=50, "
+                               "Shem+Greedy, seed 1", "name": "rgg_batch", "n_total": n_tot, "m_total": m_tot,
+                   "generation_s": round(gen_s, 1),
+                   "timing": "host wall clock around the whole batched call (one upload, all graphs, results "
+                             "back on the host)"},
+        "edges_per_s": m_tot / b,
+        "plain_gpu": {"s": pt, "graphs_per_s": args.graphs / pt, "same_result": same},
+        "speedup_vs_plain_gpu": pt / b,
+        "e2e": {"value": args.graphs / b, "unit": "graphs/s", "ms_per_step": b * 1e3,
+                "h2d_bytes_per_step": int(4 * (sum(len(s[0]) + len(s[1]) + len(s[2]) + len(s[3]) for s in specs))),
+                "d2h_bytes_per_step": int(4 * n_tot + 8 * args.graphs)},
+        "clocks": sampler.summary(tw0, tw1),
+    }
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        sample = specs[:32]
+        t0 = time.perf_counter()
+        for x, a, v, w, kk in sample:
+            rc, _, _ = O.part_graph_kway(x, a, kk, vwgt=v, adjwgt=w, ncon=2, options=kway_options(1, ufactor=50))
+            assert rc == 1
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": len(sample) / dt, "unit": "graphs/s", "cores": 1, "kind": "port",
+                                "sample": f"the first {len(sample)} graphs of the batch, 1 thread, {dt:.2f} s"}
+    print(json.dumps(line))
+
+
+def _serving_templates(count=24):
+    """Graph templates of the serving stream: 2D grid, 3D grid, 2D RGG (1:1:1),
+    n log-uniform in [1e4, 2e6], unit or U{1..10} edge weights
+    (numpy default_rng(5))."""
+    rng = np.random.default_rng(5)
+    out = []
+    for i in range(count):
+        kind = i % 3
+        n = int(np.exp(rng.uniform(np.log(1e4), np.log(2e6))))
+        weighted = bool(rng.integers(2))
+        if kind == 0:
+            side = max(2, int(round(np.sqrt(n))))
+            x, a = G.grid2d(side, side)
+            w = G.grid_weighted((side, side), seed=int(rng.integers(1 << 30)), wmax=10)[2] if weighted else None
+            name = f"grid2d {side}x{side}"
+        elif kind == 1:
+            side = max(2, int(round(n ** (1 / 3))))
+            x, a, _, w = G.grid3d(side, weights_seed=int(rng.integers(1 << 30)))
+            w = w if weighted else None
+            name = f"grid3d {side}^3"
+        else:
+            x, a, w = G.rgg2d_device(n, int(rng.integers(1 << 31)), 10.0)
+            w = w if weighted else None
+            name = f"rgg n={n}"
+        out.append((name, x, a, w))
+    return out
+
+
+def run_serving(args):
+    torch, dev, local_rank = _setup_device()
+    import rmetis_b200 as rmb
+    t0 = time.perf_counter()
+    templates = _serving_templates()
+    gen_s = time.perf_counter() - t0
+    graphs = [rmb.Graph(len(x) - 1, 1, x, a, adjwgt=w, validate=False) for _, x, a, w in templates]
+    rates = [float(r) for r in args.rates.split(",")]
+    R = args.requests
+    rng = np.random.default_rng(55)
+    # Requests: template, k in {2..128}, seed; the same list for every rate.
+    req_t = rng.integers(0, len(graphs), R)
+    req_k = rng.integers(2, 129, R)
+    req_s = rng.integers(1, 1 << 30, R)
+    opts = [rmb.Options(rtype=rmb.RType.Greedy, seed=int(s)) for s in req_s]
+    # Plain path service times: one request at a time.
+    for g in graphs[:3]:
+        rmb.part_graph_kway(g, 8, options=opts[0])
+    service = np.zeros(R)
+    plain_obj = {}
+    for i in range(R):
+        t0 = time.perf_counter()
+        r = rmb.part_graph_kway(graphs[req_t[i]], int(req_k[i]), options=opts[i])
+        service[i] = time.perf_counter() - t0
+        plain_obj[i] = r.objval
+    results = []
+    sampler = ClockSampler(gpu_id_for(local_rank))
+    sampler.start()
+    tw0 = time.time()
+    for rate in rates:
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, R))
+        # Continuous batching: requests are submitted as they arrive and run
+        # concurrently on the worker pool.
+        done_at = np.zeros(R)
+        pending = {}
+        mismatches = 0
+        start = time.perf_counter()
+        nxt = 0
+        while nxt < R or pending:
+            now = time.perf_counter() - start
+            while nxt < R and arrivals[nxt] <= now:
+                pending[nxt] = rmb.submit_kway(graphs[req_t[nxt]], int(req_k[nxt]), options=opts[nxt])
+                nxt += 1
+            for i in [i for i, q in pending.items() if q.done()]:
+                done_at[i] = time.perf_counter() - start
+                res = pending.pop(i).wait()
+                mismatches += int(res.objval != plain_obj[i])
+            if nxt < R and not pending:
+                time.sleep(max(0.0, min(0.002, arrivals[nxt] - (time.perf_counter() - start))))
+            else:
+                time.sleep(0.0002)
+        lat = (done_at - arrivals) * 1e3
+        # The plain path on the same arrivals: FIFO, one request at a time.
+        finish = np.zeros(R)
+        prev = 0.0
+        for i in range(R):
+            prev = max(prev, arrivals[i]) + service[i]
+            finish[i] = prev
+        plat = (finish - arrivals) * 1e3
+        results.append({"rate": rate, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                        "throughput": R / (done_at.max() - arrivals[0]),
+                        "plain_p50_ms": float(np.percentile(plat, 50)),
+                        "plain_p99_ms": float(np.percentile(plat, 99)),
+                        "plain_throughput": R / (finish.max() - arrivals[0]),
+                        "results_equal_plain": mismatches == 0})
+    tw1 = time.time()
+    sampler.stop()
+    best = max(results, key=lambda r: r["throughput"])
+    line = {
+        "metric": "serving throughput (req/s) and p50/p99 latency (ms)", "value": best["throughput"],
+        "unit": "requests/s", "n_gpus": 1, "steps": len(rates), "warmup": 1,
+        "ms_per_step": float(np.mean(service)) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": f"{R} requests per rate, Poisson arrivals at {args.rates} req/s, 24 graph "
+                               "templates (2D grid / 3D grid / RGG 1:1:1, n log-uniform [1e4, 2e6], unit or "
+                               "U{1..10} edge weights), k U{2..128}, ncuts=1, Shem+Greedy",
+                   "name": "serving", "generation_s": round(gen_s, 1),
+                   "pool": {"workers": int(os.environ.get("RMETIS_B200_WORKERS", "8")),
+                            "budget_bytes": int(os.environ.get("RMETIS_B200_POOL_BYTES", str(150 << 30)))}},
+        "rates": results,
+        "plain_mean_service_ms": float(np.mean(service)) * 1e3,
+        "e2e": {"value": best["throughput"], "unit": "requests/s", "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": None},
+        "clocks": sampler.summary(tw0, tw1),
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="grid3d_128", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="grid3d_128", choices=list(WORKLOADS) + list(EXTRA_WORKLOADS))
+    ap.add_argument("--scale", type=int, default=22, help="rmat_seeds: R-MAT scale")
+    ap.add_argument("--graphs", type=int, default=512, help="rgg_batch: number of graphs")
+    ap.add_argument("--requests", type=int, default=1000, help="serving: requests per arrival rate")
+    ap.add_argument("--rates", default="50,100,200,500", help="serving: arrival rates, requests/s")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
@@ -208,6 +590,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload in EXTRA_WORKLOADS:
+        {"rmat_seeds": run_rmat_seeds, "rgg_batch": run_rgg_batch, "serving": run_serving}[args.workload](args)
         return
 
     import torch

@@ -229,6 +229,52 @@ def rgg2d(n: int, seed, mean_degree: float = 10.0):
     return xadj, adjncy, adjwgt, pts
 
 
+def rgg2d_device(n: int, seed: int, mean_degree: float = 10.0, device="cuda"):
+    """rgg2d() built on a CUDA device with torch (seeded torch.Generator), for
+    batches of many graphs: points U[0,1]^2, radius r = sqrt(mean_degree /
+    (pi n)), edge weight 1 + floor(10 * (1 - d / r)), neighbours ascending.
+    Returns host numpy (xadj, adjncy, adjwgt)."""
+    import torch
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    pts = torch.rand((n, 2), generator=gen, device=device, dtype=torch.float64)
+    r = float(np.sqrt(mean_degree / (np.pi * n)))
+    cells = max(1, int(1.0 / r))
+    cxy = torch.clamp((pts * cells).to(torch.int64), max=cells - 1)
+    cell = cxy[:, 1] * cells + cxy[:, 0]
+    order = torch.argsort(cell, stable=True)
+    cell_sorted = cell[order]
+    ar = torch.arange(cells * cells, device=device)
+    starts = torch.searchsorted(cell_sorted, ar)
+    ends = torch.searchsorted(cell_sorted, ar, right=True)
+    srcs, dsts, ws = [], [], []
+    idx_all = torch.arange(n, device=device)
+    for dy in (-1, 0, 1):
+        for dx in (-1, 0, 1):
+            ncx = cxy[:, 0] + dx
+            ncy = cxy[:, 1] + dy
+            ok = (ncx >= 0) & (ncx < cells) & (ncy >= 0) & (ncy < cells)
+            idx = idx_all[ok]
+            nc = ncy[ok] * cells + ncx[ok]
+            st = starts[nc]
+            cnt = ends[nc] - st
+            rep = torch.repeat_interleave(idx, cnt)
+            base = torch.repeat_interleave(st - (torch.cumsum(cnt, 0) - cnt), cnt)
+            cand = order[base + torch.arange(int(cnt.sum()), device=device)]
+            d = torch.sqrt(((pts[rep] - pts[cand]) ** 2).sum(dim=1))
+            m = (d < r) & (rep != cand)
+            srcs.append(rep[m]); dsts.append(cand[m])
+            ws.append(1 + torch.floor(10.0 * (1.0 - d[m] / r)).to(torch.int64))
+    src = torch.cat(srcs); dst = torch.cat(dsts); w = torch.cat(ws)
+    key = src * n + dst
+    o = torch.argsort(key)
+    src, dst, w = src[o], dst[o], w[o]
+    xadj = torch.zeros(n + 1, dtype=torch.int64, device=device)
+    xadj[1:] = torch.cumsum(torch.bincount(src, minlength=n), 0)
+    return (xadj.to(torch.int32).cpu().numpy(), dst.to(torch.int32).cpu().numpy(),
+            w.to(torch.int32).cpu().numpy())
+
+
 def path(n: int):
     src = np.concatenate([np.arange(n - 1), np.arange(1, n)])
     dst = np.concatenate([np.arange(1, n), np.arange(n - 1)])
