@@ -208,6 +208,18 @@ constexpr int32_t kFast = -3;       // not known; at most two candidates, cut pa
 constexpr int32_t kLong = -4;       // not known; cut pass, more candidates than the inline slots
 constexpr int kWalkSmemParts = 4096;  // [k][ncon] entries kept in shared memory
 
+// What the walk writes: each mover's new part straight into part (the moves
+// of a pass apply together after its decisions, greedy.rs:111-119,
+// :168-181; the walk itself reads only the records), and the cleared
+// in/out bounds that the next pass's prep accumulates into.
+struct WalkOut {
+  const idx_t* movers;  // [nm] vertex of each mover record
+  idx_t* part;
+  long long* in_max;    // [k][ncon]
+  long long* out_max;   // [k][ncon]
+  int32_t K;            // k * ncon
+};
+
 struct MoverRecs {  // structure of arrays, nm entries each
   int32_t* pv;
   int32_t* ne;
@@ -417,7 +429,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const int32_t* __restrict
                                                        const idx_t* __restrict__ cand_g, long long* __restrict__ pw,
                                                        const long long* __restrict__ feas_g,
                                                        const long long* __restrict__ over_g,
-                                                       idx_t* __restrict__ d_out, int32_t* __restrict__ nmoves) {
+                                                       WalkOut wo, int32_t* __restrict__ nmoves) {
   extern __shared__ long long sparts[];
   __shared__ WalkBuf buf[2];
   __shared__ int32_t win_d[32], win_pv[32], win_vw[32 * kMaxCon];
@@ -476,7 +488,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const int32_t* __restrict
           if (!changed) break;
         }
         if (valid) {
-          d_out[j0 + i] = d;
+          if (d >= 0) wo.part[wo.movers[j0 + i]] = d;
           if (d >= 0) {
             for (int c = 0; c < ncon; ++c) {
               const long long w = win_vw[lane * kMaxCon + c];
@@ -495,6 +507,11 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const int32_t* __restrict
   }
   if (SMEM)
     for (int32_t x = tid; x < K; x += blockDim.x) pw[x] = sparts[x];
+  // The next cut pass's prep accumulates into cleared bounds.
+  for (int32_t x = tid; x < wo.K; x += blockDim.x) {
+    wo.in_max[x] = 0;
+    wo.out_max[x] = 0;
+  }
   if (tid == 0) *nmoves = moves;
 }
 
@@ -768,7 +785,7 @@ __device__ __forceinline__ int32_t reg_decide(const PartRegs<S, R, NC>& s, int l
 template <int MODE, typename S, int R, int NC, bool LONG>
 __device__ __forceinline__ void walk_chunks(int32_t nm, const MoverRecs& r, int32_t k,
                                             const idx_t* __restrict__ cand_p, const idx_t* __restrict__ cand_g,
-                                            idx_t* __restrict__ d_out, WalkBuf* buf, int32_t* dbuf, unsigned* ebits,
+                                            const WalkOut& wo, WalkBuf* buf, int32_t* dbuf, unsigned* ebits,
                                             S* sslack, PartRegs<S, R, NC>& s, int32_t& moves, int tid, int lane,
                                             int warp) {
   bool dirty = false;  // a move since sslack was last written
@@ -834,7 +851,8 @@ __device__ __forceinline__ void walk_chunks(int32_t nm, const MoverRecs& r, int3
         }
       }
       __syncwarp();
-      for (int32_t i = lane; i < cnt; i += 32) d_out[j0 + i] = dbuf[i];
+      for (int32_t i = lane; i < cnt; i += 32)
+        if (dbuf[i] >= 0) wo.part[wo.movers[j0 + i]] = dbuf[i];
     } else if (ch + 1 < nchunks) {
       walk_load(buf[(ch + 1) & 1], r, (ch + 1) * kWalkChunk, nm, NC, tid - 32, blockDim.x - 32);
     }
@@ -860,7 +878,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
                                                            long long* __restrict__ pw,
                                                            const long long* __restrict__ feas_g,
                                                            const long long* __restrict__ over_g,
-                                                           idx_t* __restrict__ d_out, int32_t* __restrict__ nmoves,
+                                                           WalkOut wo, int32_t* __restrict__ nmoves,
                                                            int32_t* __restrict__ long_flag) {
   __shared__ WalkBuf buf[2];
   __shared__ int32_t dbuf[kWalkChunk];
@@ -892,10 +910,10 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
   __syncthreads();
   int32_t moves = 0;
   if (any_long)
-    walk_chunks<MODE, S, R, NC, true>(nm, r, k, cand_p, cand_g, d_out, buf, dbuf, ebits, sslack, s, moves, tid, lane,
+    walk_chunks<MODE, S, R, NC, true>(nm, r, k, cand_p, cand_g, wo, buf, dbuf, ebits, sslack, s, moves, tid, lane,
                                       warp);
   else
-    walk_chunks<MODE, S, R, NC, false>(nm, r, k, cand_p, cand_g, d_out, buf, dbuf, ebits, sslack, s, moves, tid,
+    walk_chunks<MODE, S, R, NC, false>(nm, r, k, cand_p, cand_g, wo, buf, dbuf, ebits, sslack, s, moves, tid,
                                        lane, warp);
   if (warp == 0) {
 #pragma unroll
@@ -906,21 +924,17 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
         for (int c = 0; c < NC; ++c) pw[p * NC + c] = feas_g[p * NC + c] - (long long)s.sl[rr][c];
     }
   }
+  // The next cut pass's prep accumulates into cleared bounds.
+  for (int32_t x = tid; x < wo.K; x += blockDim.x) {
+    wo.in_max[x] = 0;
+    wo.out_max[x] = 0;
+  }
   if (tid == 0) {
     *nmoves = moves;
     *long_flag = 0;  // every thread read it before the first barrier
   }
 }
 
-// Apply the pass's moves together (greedy.rs:111-119, :168-181).
-__global__ void k_apply(const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
-                        const idx_t* __restrict__ d, idx_t* __restrict__ part) {
-  const int32_t nm = *nm_dev;
-  RMB_GRID_STRIDE(j, nm) {
-    const int32_t dd = d[j];
-    if (dd >= 0) part[movers[j]] = dd;
-  }
-}
 
 // ---------------------------------------------------------------------------
 // Host side
@@ -968,14 +982,12 @@ template <int MODE>
 static int launch_walk(int32_t nmax, const int32_t* nm_dev, const idx_t* movers, const DGraph& g, const idx_t* part,
                         int k, const idx_t* ncand, const idx_t* wfrom, const idx_t* cand_p, const idx_t* cand_g,
                         const MoverRecs& r, long long* pw, const long long* feas, const long long* over,
-                        long long* in_max, long long* out_max, idx_t* d_out, int32_t* nmoves, bool small_weights,
+                        long long* in_max, long long* out_max, int32_t* nmoves, bool small_weights,
                         int32_t* long_flag, cudaStream_t st) {
   const int32_t K = k * g.ncon;
   const int blocks = grid_for(nmax, 256);
-  if (MODE == kCut) {
-    RMB_CUDA(cudaMemsetAsync(in_max, 0, sizeof(long long) * (size_t)K, st));
-    RMB_CUDA(cudaMemsetAsync(out_max, 0, sizeof(long long) * (size_t)K, st));
-  }
+  // in_max/out_max are zero here: cleared once per level and by every walk.
+  WalkOut wo{movers, const_cast<idx_t*>(part), in_max, out_max, K};
   k_walk_prep<MODE><<<blocks, 256, 0, st>>>(nm_dev, movers, part, g.vwgt, g.ncon, g.xadj, ncand, wfrom, cand_p,
                                             cand_g, r, in_max, out_max, long_flag);
   RMB_LAUNCH_CHECK();
@@ -987,7 +999,7 @@ static int launch_walk(int32_t nmax, const int32_t* nm_dev, const idx_t* movers,
   const int ph = profiler().begin(kProfDecide, st);
   const int ncon = g.ncon;
 #define RMB_WALK_REG(ST, RR, NCC)                                                                     \
-  k_walk_reg<MODE, ST, RR, NCC><<<1, kWalkThreads, 0, st>>>(nm_dev, r, k, cand_p, cand_g, pw, feas, over, d_out, \
+  k_walk_reg<MODE, ST, RR, NCC><<<1, kWalkThreads, 0, st>>>(nm_dev, r, k, cand_p, cand_g, pw, feas, over, wo, \
                                                             nmoves, long_flag)
 #define RMB_WALK_REG_R(ST, NCC)                       \
   do {                                                \
@@ -1017,15 +1029,13 @@ static int launch_walk(int32_t nmax, const int32_t* nm_dev, const idx_t* movers,
       attr_device = dev;
     }
     k_walk<MODE, true><<<1, kWalkThreads, sizeof(long long) * 3 * (size_t)K, st>>>(
-        nm_dev, r, g.ncon, k, cand_p, cand_g, pw, feas, over, d_out, nmoves);
+        nm_dev, r, g.ncon, k, cand_p, cand_g, pw, feas, over, wo, nmoves);
   } else {
-    k_walk<MODE, false><<<1, kWalkThreads, 0, st>>>(nm_dev, r, g.ncon, k, cand_p, cand_g, pw, feas, over, d_out,
+    k_walk<MODE, false><<<1, kWalkThreads, 0, st>>>(nm_dev, r, g.ncon, k, cand_p, cand_g, pw, feas, over, wo,
                                                    nmoves);
   }
   RMB_LAUNCH_CHECK();
   profiler().end(ph, st, 0.0);
-  k_apply<<<blocks, 256, 0, st>>>(nm_dev, movers, d_out, const_cast<idx_t*>(part));
-  RMB_LAUNCH_CHECK();
   return ph;
 }
 
@@ -1045,13 +1055,14 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
   idx_t* cand_p = arena.alloc<idx_t>((size_t)g.m + 1);
   idx_t* cand_g = arena.alloc<idx_t>((size_t)g.m + 1);
   idx_t* movers = arena.alloc<idx_t>((size_t)g.n);
-  idx_t* dec = arena.alloc<idx_t>((size_t)g.n);
   // Per pass: [2*pass] movers, [2*pass+1] moves.
   int32_t* counters = arena.alloc<int32_t>(2 * ((size_t)rp.niter + 1));
   // Number of a pass's movers with more candidates than the inline slots,
   // counted by prep/classify; the register walk reads and clears it.
   int32_t* long_flag = arena.alloc<int32_t>(1);
   RMB_CUDA(cudaMemsetAsync(long_flag, 0, sizeof(int32_t), st));
+  RMB_CUDA(cudaMemsetAsync(in_max, 0, sizeof(long long) * (size_t)K, st));
+  RMB_CUDA(cudaMemsetAsync(out_max, 0, sizeof(long long) * (size_t)K, st));
   MoverRecs r;
   r.pv = arena.alloc<int32_t>((size_t)g.n);
   r.ne = arena.alloc<int32_t>((size_t)g.n);
@@ -1080,11 +1091,11 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
     compact_flags(mover, g.n, movers, nm_dev, arena, st);
     if (mode == kRepair)
       walk_handles.push_back(launch_walk<kRepair>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r,
-                                                  pw, rp.feas_max, rp.over_thr, in_max, out_max, dec, nm_dev + 1,
+                                                  pw, rp.feas_max, rp.over_thr, in_max, out_max, nm_dev + 1,
                                                   rp.small_weights, long_flag, st));
     else
       walk_handles.push_back(launch_walk<kCut>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r, pw,
-                                               rp.feas_max, rp.over_thr, in_max, out_max, dec, nm_dev + 1,
+                                               rp.feas_max, rp.over_thr, in_max, out_max, nm_dev + 1,
                                                rp.small_weights, long_flag, st));
   }
   static const bool trace = std::getenv("RMETIS_B200_TRACE") != nullptr;

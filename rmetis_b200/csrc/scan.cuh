@@ -119,6 +119,50 @@ __global__ void k_tile_scan(Load load, Store store, int64_t n, const T* tile_off
   }
 }
 
+// Small inputs: the whole scan in one block (tiles of 1024 x 8 items in
+// order, with a running carry), one launch instead of three.
+constexpr int kScanSmallThreads = 1024;
+constexpr int kScanSmallTile = kScanSmallThreads * kScanItems;
+constexpr int64_t kScanSmallMax = 2 * kScanSmallTile;
+
+template <typename T, typename Load, typename Store>
+__global__ void __launch_bounds__(kScanSmallThreads) k_scan_small(Load load, Store store, int64_t n, T* total_out) {
+  __shared__ T sw[32];
+  __shared__ T tile[kScanSmallTile];
+  T carry = 0;
+  for (int64_t base = 0; base < n; base += kScanSmallTile) {
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+      const int64_t j = base + (int64_t)i * kScanSmallThreads + threadIdx.x;
+      tile[i * kScanSmallThreads + threadIdx.x] = (j < n) ? load(j) : T(0);
+    }
+    __syncthreads();
+    T vals[kScanItems];
+    T s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+      vals[i] = tile[threadIdx.x * kScanItems + i];
+      s += vals[i];
+    }
+    T tot;
+    T run = carry + block_exclusive_scan<T>(s, sw, &tot);
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+      tile[threadIdx.x * kScanItems + i] = run;
+      run += vals[i];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+      const int64_t j = base + (int64_t)i * kScanSmallThreads + threadIdx.x;
+      if (j < n) store(j, tile[i * kScanSmallThreads + threadIdx.x]);
+    }
+    carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && total_out) *total_out = carry;
+}
+
 template <typename T>
 struct LoadArr {
   const T* p;
@@ -135,6 +179,11 @@ struct StoreArr {
 // is released on return.
 template <typename T, typename Load, typename Store>
 void exclusive_scan(Load load, Store store, int64_t n, T* total_dev, Arena& arena, cudaStream_t st) {
+  if (n <= kScanSmallMax) {
+    k_scan_small<T, Load, Store><<<1, kScanSmallThreads, 0, st>>>(load, store, n, total_dev);
+    RMB_LAUNCH_CHECK();
+    return;
+  }
   Arena::Mark mk = arena.mark();
   int64_t ntiles = ceil_div(n, kScanTile);
   if (ntiles < 1) ntiles = 1;

@@ -126,3 +126,24 @@ def test_async_error_codes(rmb):
     lib = rmb._lib.load()
     assert lib.RMETIS_GPU_WaitKway(123456789) == -2
     assert lib.RMETIS_GPU_PollKway(123456789) == -2
+
+
+def test_ranks_path_single_rank_equals_plain(rmb):
+    """The rank-striped best-of-ncuts with one rank runs every attempt there
+    and equals the plain call's best of ncuts."""
+    import socket
+    import torch.distributed as dist
+    from rmetis_b200 import distributed as D
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        x, a, v, w = G.grid3d(18, weights_seed=6)
+        g = graph_of(rmb, x, a, v, w)
+        res = D.part_graph_kway_ranks(g, 12, options=greedy(21, 4))
+        plain = rmb.part_graph_kway(g, 12, options=greedy(21, 4))
+        assert res.objval == plain.objval
+        np.testing.assert_array_equal(res.part, plain.part)
+    finally:
+        dist.destroy_process_group()
