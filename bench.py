@@ -59,6 +59,8 @@ WORKLOADS = {
                   "2D 5-point grid 64x64, unit weights, nparts=8, Shem+Greedy, ufactor=30, ncuts=1, seed=1"),
 }
 EXTRA_WORKLOADS = ("rmat_seeds", "rgg_batch", "serving")
+# Kernel families of RMETIS_GPU_GetProfile, in its slot order.
+PROF_NAMES = ["k_gain", "k_walk", "k_match_propose", "k_contract_thread", "k_cut", "k_grow", "k_refine_level"]
 CPU_SAMPLE = {
     "grid3d_128": (lambda: G.grid3d(64, weights_seed=7), "3D 7-point grid 64^3 (same weight laws), nparts=64"),
     "grid2d_64": (lambda: G.grid2d(64, 64) + (None, None), "2D grid 64x64, nparts=8"),
@@ -328,7 +330,7 @@ def run_rmat_seeds(args):
 def _profile_one(lib, torch, call):
     """Per-kernel CUDA-event totals of one call, and the roofline of the kernel
     with the most device time among those with counted bytes."""
-    nprof = 6
+    nprof = len(PROF_NAMES)
     launches = (ctypes.c_int64 * (nprof + 1))()
     ms_k = (ctypes.c_double * nprof)()
     bytes_k = (ctypes.c_double * nprof)()
@@ -341,7 +343,7 @@ def _profile_one(lib, torch, call):
     torch.cuda.synchronize()
     lib.RMETIS_GPU_GetProfile(launches, ms_k, bytes_k, nprof + 1)
     lib.RMETIS_GPU_SetProfiling(0)
-    names = ["k_gain", "k_walk", "k_match_propose", "k_contract_thread", "k_cut", "k_grow"]
+    names = PROF_NAMES
     L = [launches[i] - l0[i] for i in range(nprof)]
     M = [ms_k[i] - m0[i] for i in range(nprof)]
     B = [bytes_k[i] - b0[i] for i in range(nprof)]
@@ -637,7 +639,7 @@ def main():
         step_device()
     torch.cuda.synchronize()
 
-    nprof = 6
+    nprof = len(PROF_NAMES)
     launches = (ctypes.c_int64 * (nprof + 1))()
     ms_k = (ctypes.c_double * nprof)()
     bytes_k = (ctypes.c_double * nprof)()
@@ -712,7 +714,7 @@ def main():
         value = world * m / (ms_max / 1000.0)
         e2e_value = world * m / e2e_max
         peak, peak_kind = load_peaks()
-        names = ["k_gain", "k_walk", "k_match_propose", "k_contract_thread", "k_cut", "k_grow"]
+        names = PROF_NAMES
         dom = max(range(nprof), key=lambda i: ms_k[i] if bytes_k[i] > 0 else -1.0)
         avg_ms = ms_k[dom] / max(1, launches[dom])
         avg_bytes = bytes_k[dom] / max(1, launches[dom])

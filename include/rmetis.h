@@ -98,11 +98,13 @@ RMETIS_API int RMETIS_GPU_SetStream(void *stream);
 /* Engine knobs without a METIS option slot: grown partitions per attempt
  * (lowest cut kept), matching rounds per level, whether a graph without
  * vertex weights gets summed coarse weights (1) or the reference's unit coarse
- * weights (0, default), and whether ncuts > 1 attempts run concurrently on the
- * device's worker pool (1, default) or one after another (0); both give the
- * same result. Values < 0 leave a knob unchanged. */
+ * weights (0, default), whether ncuts > 1 attempts run concurrently on the
+ * device's worker pool (1, default) or one after another (0), and the largest
+ * level (vertices) whose refinement runs in one single-block launch (default
+ * 2048, 0 = never); the last two never change a result. Values < 0 leave a
+ * knob unchanged. */
 RMETIS_API int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weights,
-                                    int parallel_attempts);
+                                    int parallel_attempts, int fused_max_n);
 
 /* Many graphs in one call (no counterpart in the reference, which partitions
  * one graph per call). Host arrays of the concatenated batch: graph g has

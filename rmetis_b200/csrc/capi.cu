@@ -39,6 +39,7 @@ struct Tuning {
   int match_rounds = 24;
   int summed_unit_weights = 0;
   int parallel_attempts = 1;
+  int fused_max_n = 2048;
 };
 Tuning& tuning() {
   static Tuning t;
@@ -50,6 +51,7 @@ void apply_tuning(KwayOptions& o) {
   o.match_rounds = tuning().match_rounds;
   o.summed_unit_weights = tuning().summed_unit_weights;
   o.parallel_attempts = tuning().parallel_attempts;
+  o.fused_max_n = tuning().fused_max_n;
 }
 
 template <typename F>
@@ -250,11 +252,13 @@ int RMETIS_GPU_SetStream(void* stream) {
   });
 }
 
-int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weights, int parallel_attempts) {
+int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weights, int parallel_attempts,
+                         int fused_max_n) {
   if (grow_trials >= 0) tuning().grow_trials = grow_trials > 0 ? grow_trials : 1;
   if (match_rounds >= 0) tuning().match_rounds = match_rounds > 0 ? match_rounds : 1;
   if (summed_unit_weights >= 0) tuning().summed_unit_weights = summed_unit_weights ? 1 : 0;
   if (parallel_attempts >= 0) tuning().parallel_attempts = parallel_attempts ? 1 : 0;
+  if (fused_max_n >= 0) tuning().fused_max_n = fused_max_n;
   return METIS_OK;
 }
 
@@ -655,6 +659,7 @@ int RMETIS_GPU_GreedyRefine(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t*
     rp.feas_max = d_feas;
     rp.over_thr = d_over;
     rp.collect_stats = stats != nullptr;
+    rp.fused_max_n = tuning().fused_max_n;
     {
       std::vector<long long> tot(ncon, 0);
       for (int64_t v = 0; v < n; ++v)

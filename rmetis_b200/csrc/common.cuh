@@ -50,6 +50,17 @@ __host__ __device__ inline uint64_t mix64(uint64_t z) {
 }
 
 // Grid-stride loop helper.
+// The loop set of a kernel body: every thread of the grid, or the threads of
+// one block (a body run by a single block inside a fused kernel).
+struct Lanes {
+  int64_t first, stride;
+};
+__device__ inline Lanes grid_lanes() {
+  return {(int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x};
+}
+__device__ inline Lanes block_lanes() { return {(int64_t)threadIdx.x, (int64_t)blockDim.x}; }
+#define RMB_FOR(i, n, L) for (int64_t i = (L).first; i < (int64_t)(n); i += (L).stride)
+
 #define RMB_GRID_STRIDE(i, n) \
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)(n); i += (int64_t)gridDim.x * blockDim.x)
 

@@ -370,6 +370,7 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
     rp.feas_max = feas_of(L);
     rp.over_thr = over_of(L);
     rp.small_weights = small[L];
+    rp.fused_max_n = o.fused_max_n;
     rp.collect_stats = trace != nullptr;
     {
       RefineStats rs = greedy_refine(cg, part, rp, heavy_lists[L], heavy_counts[L], arena_, st, h_scratch_);

@@ -227,17 +227,6 @@ void boundary_flags(const DGraph& g, const idx_t* part, idx_t* flag, cudaStream_
 // ---------------------------------------------------------------------------
 // Flag compaction
 // ---------------------------------------------------------------------------
-struct LoadNonZero {
-  const idx_t* f;
-  __device__ idx_t operator()(int64_t i) const { return f[i] != 0 ? 1 : 0; }
-};
-struct StoreCompact {
-  const idx_t* f;
-  idx_t* out;
-  __device__ void operator()(int64_t i, idx_t pos) const {
-    if (f[i] != 0) out[pos] = (idx_t)i;
-  }
-};
 
 void compact_flags(const idx_t* flag, int32_t n, idx_t* out, idx_t* count_dev, Arena& arena, cudaStream_t st) {
   exclusive_scan<idx_t>(LoadNonZero{flag}, StoreCompact{flag, out}, n, count_dev, arena, st);

@@ -17,6 +17,7 @@ enum ProfId {
   kProfContract,      // k_contract_thread
   kProfCut,           // k_cut
   kProfGrow,          // k_grow
+  kProfLevel,         // k_refine_level: all passes of a small level in one launch
   kProfCount
 };
 

@@ -47,12 +47,12 @@ __device__ inline bool cand_better(int32_t ga, int32_t pa, int32_t gb, int32_t p
 //   kTable:  mover = boundary (used by the gain-table entry point)
 // ---------------------------------------------------------------------------
 template <bool HAS_W, int MODE>
-__global__ void k_gain(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
-                       const idx_t* __restrict__ adjwgt, int32_t n, int32_t ncon, const idx_t* __restrict__ part,
-                       int32_t k, const long long* __restrict__ pw0, const long long* __restrict__ over_thr,
-                       idx_t* __restrict__ mover, idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom,
-                       idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g) {
-  RMB_GRID_STRIDE(v, n) {
+__device__ void gain_body(Lanes L, const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                          const idx_t* __restrict__ adjwgt, int32_t n, int32_t ncon, const idx_t* __restrict__ part,
+                          int32_t k, const long long* __restrict__ pw0, const long long* __restrict__ over_thr,
+                          idx_t* __restrict__ mover, idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom,
+                          idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g) {
+  RMB_FOR(v, n, L) {
     const int32_t s = xadj[v], e = xadj[v + 1];
     if (e - s > kHeavyDegree) continue;  // warp path
     const int32_t pv = part[v];
@@ -116,6 +116,16 @@ __global__ void k_gain(const idx_t* __restrict__ xadj, const idx_t* __restrict__
   }
 }
 
+template <bool HAS_W, int MODE>
+__global__ void k_gain(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                       const idx_t* __restrict__ adjwgt, int32_t n, int32_t ncon, const idx_t* __restrict__ part,
+                       int32_t k, const long long* __restrict__ pw0, const long long* __restrict__ over_thr,
+                       idx_t* __restrict__ mover, idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom,
+                       idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g) {
+  gain_body<HAS_W, MODE>(grid_lanes(), xadj, adj, adjwgt, n, ncon, part, k, pw0, over_thr, mover, ncand, wfrom,
+                         cand_p, cand_g);
+}
+
 constexpr int kGainHist = 2048;  // dense per-warp part histogram in shared memory
 
 // Warp-per-vertex gain table for vertices of degree > kHeavyDegree. The part
@@ -123,19 +133,18 @@ constexpr int kGainHist = 2048;  // dense per-warp part histogram in shared memo
 // global scratch `ghist` of k entries per warp). Each explicit candidate is
 // written straight to its sorted position, its rank being the number of
 // better candidates.
+// Warps gw, gw + nw, ... take the heavy vertices; hist: k entries of this
+// warp's own.
 template <bool HAS_W, int MODE>
-__global__ void k_gain_heavy(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
-                             const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ heavy, int32_t nheavy,
-                             int32_t ncon, const idx_t* __restrict__ part, int32_t k,
-                             const long long* __restrict__ pw0, const long long* __restrict__ over_thr,
-                             idx_t* __restrict__ mover, idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom,
-                             idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g, int32_t* __restrict__ ghist) {
-  __shared__ int32_t sh_all[4][kGainHist];
+__device__ void gain_heavy_body(int32_t gw, int32_t nw, int32_t* hist, const idx_t* __restrict__ xadj,
+                                const idx_t* __restrict__ adj, const idx_t* __restrict__ adjwgt,
+                                const idx_t* __restrict__ heavy, int32_t nheavy, int32_t ncon,
+                                const idx_t* __restrict__ part, int32_t k, const long long* __restrict__ pw0,
+                                const long long* __restrict__ over_thr, idx_t* __restrict__ mover,
+                                idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom, idx_t* __restrict__ cand_p,
+                                idx_t* __restrict__ cand_g) {
   const unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int32_t gw = blockIdx.x * (blockDim.x >> 5) + wib;
-  const int32_t nw = gridDim.x * (blockDim.x >> 5);
-  int32_t* hist = (k <= kGainHist) ? sh_all[wib] : ghist + (int64_t)gw * k;
+  const int lane = threadIdx.x & 31;
   for (int32_t hi = gw; hi < nheavy; hi += nw) {
     const int32_t v = heavy[hi];
     const int32_t s = xadj[v], e = xadj[v + 1];
@@ -196,6 +205,22 @@ __global__ void k_gain_heavy(const idx_t* __restrict__ xadj, const idx_t* __rest
   }
 }
 
+template <bool HAS_W, int MODE>
+__global__ void k_gain_heavy(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                             const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ heavy, int32_t nheavy,
+                             int32_t ncon, const idx_t* __restrict__ part, int32_t k,
+                             const long long* __restrict__ pw0, const long long* __restrict__ over_thr,
+                             idx_t* __restrict__ mover, idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom,
+                             idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g, int32_t* __restrict__ ghist) {
+  __shared__ int32_t sh_all[4][kGainHist];
+  const int wib = threadIdx.x >> 5;
+  const int32_t gw = blockIdx.x * (blockDim.x >> 5) + wib;
+  const int32_t nw = gridDim.x * (blockDim.x >> 5);
+  int32_t* hist = (k <= kGainHist) ? sh_all[wib] : ghist + (int64_t)gw * k;
+  gain_heavy_body<HAS_W, MODE>(gw, nw, hist, xadj, adj, adjwgt, heavy, nheavy, ncon, part, k, pw0, over_thr, mover,
+                               ncand, wfrom, cand_p, cand_g);
+}
+
 
 // ---------------------------------------------------------------------------
 // Mover records and the walk
@@ -234,14 +259,14 @@ struct MoverRecs {  // structure of arrays, nm entries each
 // One thread per mover: copy its data into a record and add its weight to
 // the bounds: in_max[p] over every part it may move to, out_max[pv].
 template <int MODE>
-__global__ void k_walk_prep(const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
-                            const idx_t* __restrict__ part, const idx_t* __restrict__ vwgt, int32_t ncon,
-                            const idx_t* __restrict__ xadj, const idx_t* __restrict__ ncand,
-                            const idx_t* __restrict__ wfrom, const idx_t* __restrict__ cand_p,
-                            const idx_t* __restrict__ cand_g, MoverRecs r, long long* __restrict__ in_max,
-                            long long* __restrict__ out_max, int32_t* __restrict__ long_flag) {
+__device__ void prep_body(Lanes L, const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
+                          const idx_t* __restrict__ part, const idx_t* __restrict__ vwgt, int32_t ncon,
+                          const idx_t* __restrict__ xadj, const idx_t* __restrict__ ncand,
+                          const idx_t* __restrict__ wfrom, const idx_t* __restrict__ cand_p,
+                          const idx_t* __restrict__ cand_g, const MoverRecs& r, long long* __restrict__ in_max,
+                          long long* __restrict__ out_max, int32_t* __restrict__ long_flag) {
   const int32_t nm = *nm_dev;
-  RMB_GRID_STRIDE(j, nm) {
+  RMB_FOR(j, nm, L) {
     const int32_t v = movers[j];
     const int32_t pv = part[v];
     const int32_t s = xadj[v];
@@ -274,15 +299,27 @@ __global__ void k_walk_prep(const int32_t* __restrict__ nm_dev, const idx_t* __r
   }
 }
 
+template <int MODE>
+__global__ void k_walk_prep(const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
+                            const idx_t* __restrict__ part, const idx_t* __restrict__ vwgt, int32_t ncon,
+                            const idx_t* __restrict__ xadj, const idx_t* __restrict__ ncand,
+                            const idx_t* __restrict__ wfrom, const idx_t* __restrict__ cand_p,
+                            const idx_t* __restrict__ cand_g, MoverRecs r, long long* __restrict__ in_max,
+                            long long* __restrict__ out_max, int32_t* __restrict__ long_flag) {
+  prep_body<MODE>(grid_lanes(), nm_dev, movers, part, vwgt, ncon, xadj, ncand, wfrom, cand_p, cand_g, r, in_max,
+                  out_max, long_flag);
+}
+
 // Cut passes: fix the decision of every mover whose walk through its
 // candidates meets only parts that are infeasible whatever happens before it,
 // and then a part that is feasible whatever happens before it (or runs out).
-__global__ void k_walk_classify(const int32_t* __restrict__ nm_dev, int32_t ncon, const idx_t* __restrict__ cand_p,
-                                const idx_t* __restrict__ cand_g, MoverRecs r, const long long* __restrict__ pw0,
-                                const long long* __restrict__ feas, const long long* __restrict__ in_max,
-                                const long long* __restrict__ out_max, int32_t* __restrict__ long_flag) {
+__device__ void classify_body(Lanes L, const int32_t* __restrict__ nm_dev, int32_t ncon,
+                              const idx_t* __restrict__ cand_p, const idx_t* __restrict__ cand_g, const MoverRecs& r,
+                              const long long* __restrict__ pw0, const long long* __restrict__ feas,
+                              const long long* __restrict__ in_max, const long long* __restrict__ out_max,
+                              int32_t* __restrict__ long_flag) {
   const int32_t nm = *nm_dev;
-  RMB_GRID_STRIDE(j, nm) {
+  RMB_FOR(j, nm, L) {
     const int32_t ne = r.ne[j];
     const int32_t ig = (int32_t)(0u - (uint32_t)r.wf[j]);
     int32_t known = -1;
@@ -322,6 +359,13 @@ __global__ void k_walk_classify(const int32_t* __restrict__ nm_dev, int32_t ncon
     if (lm && (threadIdx.x & 31) == __ffs(lm) - 1) atomicAdd(long_flag, __popc(lm));
     r.known[j] = known;
   }
+}
+
+__global__ void k_walk_classify(const int32_t* __restrict__ nm_dev, int32_t ncon, const idx_t* __restrict__ cand_p,
+                                const idx_t* __restrict__ cand_g, MoverRecs r, const long long* __restrict__ pw0,
+                                const long long* __restrict__ feas, const long long* __restrict__ in_max,
+                                const long long* __restrict__ out_max, int32_t* __restrict__ long_flag) {
+  classify_body(grid_lanes(), nm_dev, ncon, cand_p, cand_g, r, pw0, feas, in_max, out_max, long_flag);
 }
 
 struct WalkBuf {
@@ -871,19 +915,26 @@ __device__ __forceinline__ void walk_chunks(int32_t nm, const MoverRecs& r, int3
 // positive-gain candidates take a branch-free path (both tests and votes at
 // once, then a select) and their record is fetched one mover ahead. The other
 // warps stream mover records.
+// Shared memory of the register walk.
+template <typename S, int R, int NC>
+struct WalkShared {
+  WalkBuf buf[2];
+  int32_t dbuf[kWalkChunk];
+  unsigned ebits[R];
+  S sslack[32 * R * NC];  // copy of the feasibility slacks for the long-list scans
+};
+
 template <int MODE, typename S, int R, int NC>
-__global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __restrict__ nm_dev, MoverRecs r,
-                                                           int32_t k, const idx_t* __restrict__ cand_p,
-                                                           const idx_t* __restrict__ cand_g,
-                                                           long long* __restrict__ pw,
-                                                           const long long* __restrict__ feas_g,
-                                                           const long long* __restrict__ over_g,
-                                                           WalkOut wo, int32_t* __restrict__ nmoves,
-                                                           int32_t* __restrict__ long_flag) {
-  __shared__ WalkBuf buf[2];
-  __shared__ int32_t dbuf[kWalkChunk];
-  __shared__ unsigned ebits[R];
-  __shared__ S sslack[32 * R * NC];  // copy of the feasibility slacks for the long-list scans
+__device__ __forceinline__ void walk_reg_body(WalkShared<S, R, NC>& sh, const int32_t* __restrict__ nm_dev,
+                                              const MoverRecs& r, int32_t k, const idx_t* __restrict__ cand_p,
+                                              const idx_t* __restrict__ cand_g, long long* __restrict__ pw,
+                                              const long long* __restrict__ feas_g,
+                                              const long long* __restrict__ over_g, const WalkOut& wo,
+                                              int32_t* __restrict__ nmoves, int32_t* __restrict__ long_flag) {
+  WalkBuf* buf = sh.buf;
+  int32_t* dbuf = sh.dbuf;
+  unsigned* ebits = sh.ebits;
+  S* sslack = sh.sslack;
   const int32_t nm = *nm_dev;
   // The long-list version of the loop pays off when long lists are common
   // (count from k_walk_prep / k_walk_classify); both versions decide alike.
@@ -933,6 +984,19 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
     *nmoves = moves;
     *long_flag = 0;  // every thread read it before the first barrier
   }
+}
+
+template <int MODE, typename S, int R, int NC>
+__global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __restrict__ nm_dev, MoverRecs r,
+                                                           int32_t k, const idx_t* __restrict__ cand_p,
+                                                           const idx_t* __restrict__ cand_g,
+                                                           long long* __restrict__ pw,
+                                                           const long long* __restrict__ feas_g,
+                                                           const long long* __restrict__ over_g,
+                                                           WalkOut wo, int32_t* __restrict__ nmoves,
+                                                           int32_t* __restrict__ long_flag) {
+  __shared__ WalkShared<S, R, NC> sh;
+  walk_reg_body<MODE, S, R, NC>(sh, nm_dev, r, k, cand_p, cand_g, pw, feas_g, over_g, wo, nmoves, long_flag);
 }
 
 
@@ -1039,6 +1103,111 @@ static int launch_walk(int32_t nmax, const int32_t* nm_dev, const idx_t* movers,
   return ph;
 }
 
+// ---------------------------------------------------------------------------
+// One level's refinement in one launch (small levels): a single block runs the
+// start-of-level part weights and then, for every pass, the gain table, the
+// mover compaction, the records, the classification and the walk, with block
+// barriers between the steps instead of kernel boundaries. The bodies are the
+// ones of the multi-kernel path, so every pass decides exactly as there.
+// ---------------------------------------------------------------------------
+constexpr int kFusedThreads = 512;
+
+struct LevelRefine {
+  const idx_t* xadj;
+  const idx_t* adj;
+  const idx_t* adjwgt;
+  const idx_t* vwgt;
+  int32_t n;
+  int32_t k;
+  int32_t niter;
+  idx_t* part;
+  long long* pw;
+  long long* in_max;
+  long long* out_max;
+  const long long* feas;
+  const long long* over;
+  idx_t* mover;
+  idx_t* ncand;
+  idx_t* wfrom;
+  idx_t* cand_p;
+  idx_t* cand_g;
+  idx_t* movers;
+  MoverRecs r;
+  const idx_t* heavy;
+  int32_t nheavy;
+  int32_t* ghist;     // [kFusedThreads / 32][k]
+  int32_t* counters;  // [2 * (niter + 1)]: movers, moves per pass
+  int32_t* long_flag;
+};
+
+template <bool HAS_W, int MODE, typename S, int R, int NC>
+__device__ __forceinline__ void fused_pass(const LevelRefine& P, WalkShared<S, R, NC>& sh, int32_t* sw, int pass) {
+  const Lanes L = block_lanes();
+  const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  int32_t* nm_dev = P.counters + 2 * pass;
+  gain_body<HAS_W, MODE>(L, P.xadj, P.adj, P.adjwgt, P.n, NC, P.part, P.k, P.pw, P.over, P.mover, P.ncand, P.wfrom,
+                         P.cand_p, P.cand_g);
+  if (P.nheavy > 0)
+    gain_heavy_body<HAS_W, MODE>(warp, nwarps, P.ghist + (int64_t)warp * P.k, P.xadj, P.adj, P.adjwgt, P.heavy,
+                                 P.nheavy, NC, P.part, P.k, P.pw, P.over, P.mover, P.ncand, P.wfrom, P.cand_p,
+                                 P.cand_g);
+  __syncthreads();
+  block_scan_n<int32_t>(LoadNonZero{P.mover}, StoreCompact{P.mover, P.movers}, P.n, nm_dev, sw);
+  __syncthreads();
+  prep_body<MODE>(L, nm_dev, P.movers, P.part, P.vwgt, NC, P.xadj, P.ncand, P.wfrom, P.cand_p, P.cand_g, P.r,
+                  P.in_max, P.out_max, P.long_flag);
+  __syncthreads();
+  if (MODE == kCut) {
+    classify_body(L, nm_dev, NC, P.cand_p, P.cand_g, P.r, P.pw, P.feas, P.in_max, P.out_max, P.long_flag);
+    __syncthreads();
+  }
+  const WalkOut wo{P.movers, P.part, P.in_max, P.out_max, P.k * NC};
+  walk_reg_body<MODE, S, R, NC>(sh, nm_dev, P.r, P.k, P.cand_p, P.cand_g, P.pw, P.feas, P.over, wo, nm_dev + 1,
+                                P.long_flag);
+  __syncthreads();
+}
+
+template <bool HAS_W, typename S, int R, int NC>
+__global__ void __launch_bounds__(kFusedThreads) k_refine_level(LevelRefine P) {
+  __shared__ WalkShared<S, R, NC> sh;
+  __shared__ int32_t sw[32];
+  const int32_t K = P.k * NC;
+  for (int32_t x = threadIdx.x; x < K; x += blockDim.x) {
+    P.pw[x] = 0;
+    P.in_max[x] = 0;
+    P.out_max[x] = 0;
+  }
+  if (threadIdx.x == 0) *P.long_flag = 0;
+  __syncthreads();
+  // Part weights of the start partition (src/graph/mod.rs:140-149).
+  RMB_FOR(v, P.n, block_lanes()) {
+    const int32_t p = P.part[v];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) atomic_add_i64(&P.pw[p * NC + c], P.vwgt ? P.vwgt[v * NC + c] : 1);
+  }
+  __syncthreads();
+  fused_pass<HAS_W, kRepair, S, R, NC>(P, sh, sw, 0);
+  for (int pass = 1; pass <= P.niter; ++pass) fused_pass<HAS_W, kCut, S, R, NC>(P, sh, sw, pass);
+}
+
+template <bool HAS_W, typename S, int NC>
+static void launch_fused_r(const LevelRefine& P, cudaStream_t st) {
+  const int k = P.k;
+  if (k <= 32) k_refine_level<HAS_W, S, 1, NC><<<1, kFusedThreads, 0, st>>>(P);
+  else if (k <= 64) k_refine_level<HAS_W, S, 2, NC><<<1, kFusedThreads, 0, st>>>(P);
+  else if (k <= 128) k_refine_level<HAS_W, S, 4, NC><<<1, kFusedThreads, 0, st>>>(P);
+  else k_refine_level<HAS_W, S, 8, NC><<<1, kFusedThreads, 0, st>>>(P);
+}
+
+template <bool HAS_W>
+static void launch_fused(const LevelRefine& P, int ncon, bool small_weights, cudaStream_t st) {
+  if (small_weights) {
+    if (ncon == 1) launch_fused_r<HAS_W, int32_t, 1>(P, st); else launch_fused_r<HAS_W, int32_t, 2>(P, st);
+  } else {
+    if (ncon == 1) launch_fused_r<HAS_W, long long, 1>(P, st); else launch_fused_r<HAS_W, long long, 2>(P, st);
+  }
+}
+
 RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, const idx_t* heavy, int32_t nheavy,
                           Arena& arena, cudaStream_t st, int32_t* h_scratch) {
   if (g.ncon > kMaxCon) throw Error(-2, "ncon above the supported maximum of 8");
@@ -1072,7 +1241,44 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
   r.cp = arena.alloc<int32_t>((size_t)g.n * kInline);
   r.cg = arena.alloc<int32_t>((size_t)g.n * kInline);
   r.vw = arena.alloc<int32_t>((size_t)g.n * g.ncon);
-  int32_t* ghist = (nheavy > 0 && k > kGainHist) ? arena.alloc<int32_t>((size_t)k * 256 * 4) : nullptr;
+  const bool fused = rp.fused_max_n > 0 && g.n <= rp.fused_max_n && k <= 256 && g.ncon <= 2;
+  int32_t* ghist = nullptr;
+  if (nheavy > 0 && (fused || k > kGainHist))
+    ghist = arena.alloc<int32_t>((size_t)k * (fused ? kFusedThreads / 32 : 256 * 4));
+  std::vector<int> walk_handles;
+  if (fused) {
+    LevelRefine P;
+    P.xadj = g.xadj;
+    P.adj = g.adjncy;
+    P.adjwgt = g.adjwgt;
+    P.vwgt = g.vwgt;
+    P.n = g.n;
+    P.k = k;
+    P.niter = rp.niter;
+    P.part = part;
+    P.pw = pw;
+    P.in_max = in_max;
+    P.out_max = out_max;
+    P.feas = rp.feas_max;
+    P.over = rp.over_thr;
+    P.mover = mover;
+    P.ncand = ncand;
+    P.wfrom = wfrom;
+    P.cand_p = cand_p;
+    P.cand_g = cand_g;
+    P.movers = movers;
+    P.r = r;
+    P.heavy = heavy;
+    P.nheavy = nheavy;
+    P.ghist = ghist;
+    P.counters = counters;
+    P.long_flag = long_flag;
+    const int ph = profiler().begin(kProfLevel, st);
+    if (g.adjwgt) launch_fused<true>(P, g.ncon, rp.small_weights, st);
+    else launch_fused<false>(P, g.ncon, rp.small_weights, st);
+    RMB_LAUNCH_CHECK();
+    profiler().end(ph, st, (rp.niter + 1) * (12.0 * g.n + (g.adjwgt ? 12.0 : 8.0) * (double)g.m));
+  } else {
   partition_weights_only(g, part, k, pw, st);
 
   // The reference stops the cut passes at the first pass without a move
@@ -1080,7 +1286,6 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
   // later pass would again find the same movers and make no move: running all
   // niter passes gives the same result, and the whole level is queued without
   // waiting for the host.
-  std::vector<int> walk_handles;
   for (int pass = 0; pass <= rp.niter; ++pass) {
     const int mode = pass == 0 ? kRepair : kCut;
     int32_t* nm_dev = counters + 2 * pass;
@@ -1098,8 +1303,9 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
                                                rp.feas_max, rp.over_thr, in_max, out_max, nm_dev + 1,
                                                rp.small_weights, long_flag, st));
   }
+  }
   static const bool trace = std::getenv("RMETIS_B200_TRACE") != nullptr;
-  if (profiler().on) {
+  if (profiler().on && !fused) {
     // The walk reads one record per mover (pv, ne, w_from, offset, known,
     // 4 inline candidates and gains, ncon weights) and writes its decision.
     RMB_CUDA(cudaMemcpyAsync(h_scratch, counters, sizeof(int32_t) * 2 * ((size_t)rp.niter + 1),

@@ -163,11 +163,44 @@ __global__ void __launch_bounds__(kScanSmallThreads) k_scan_small(Load load, Sto
   if (threadIdx.x == 0 && total_out) *total_out = carry;
 }
 
+// Exclusive scan of load(0..n-1) by one block (inside a fused kernel): each
+// thread takes a contiguous run of ceil(n / blockDim.x) items. Every thread of
+// the block must call it; sw holds 32 values of shared memory.
+template <typename T, typename Load, typename Store>
+__device__ void block_scan_n(Load load, Store store, int64_t n, T* total_out, T* sw) {
+  const int64_t per = (n + blockDim.x - 1) / blockDim.x;
+  const int64_t b = (int64_t)threadIdx.x * per;
+  const int64_t e = b + per < n ? b + per : n;
+  T s = 0;
+  for (int64_t i = b; i < e; ++i) s += load(i);
+  T tot;
+  T ex = block_exclusive_scan<T>(s, sw, &tot);
+  for (int64_t i = b; i < e; ++i) {
+    const T v = load(i);
+    store(i, ex);
+    ex += v;
+  }
+  if (threadIdx.x == 0 && total_out) *total_out = tot;
+}
+
 template <typename T>
 struct LoadArr {
   const T* p;
   __device__ T operator()(int64_t i) const { return p[i]; }
 };
+struct LoadNonZero {
+  const int32_t* f;
+  __device__ int32_t operator()(int64_t i) const { return f[i] != 0 ? 1 : 0; }
+};
+// Compaction store: the index of every nonzero flag goes to its rank.
+struct StoreCompact {
+  const int32_t* f;
+  int32_t* out;
+  __device__ void operator()(int64_t i, int32_t pos) const {
+    if (f[i] != 0) out[pos] = (int32_t)i;
+  }
+};
+
 template <typename T>
 struct StoreArr {
   T* p;
