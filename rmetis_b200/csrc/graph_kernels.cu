@@ -124,6 +124,35 @@ __global__ void k_cut(const idx_t* __restrict__ xadj, const idx_t* __restrict__ 
   if ((threadIdx.x & 31) == 0 && acc) atomicAdd(cut_acc, acc);
 }
 
+// Edge cut (both directions, signed weights) of ntrials partitions of one
+// graph at once: blockIdx.y is the trial, parts[trial][n], cuts[trial].
+template <bool HAS_W>
+__global__ void k_cut_trials(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                             const idx_t* __restrict__ adjwgt, int32_t n, const idx_t* __restrict__ parts,
+                             long long* __restrict__ cuts) {
+  __shared__ int32_t xs_all[8][33];
+  int32_t* xs = xs_all[threadIdx.x >> 5];
+  const idx_t* part = parts + (int64_t)blockIdx.y * n;
+  unsigned long long acc = 0;
+  const int32_t nwarps_total = gridDim.x * (blockDim.x >> 5);
+  for (int32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); (int64_t)w * 32 < n;
+       w += nwarps_total) {
+    warp_edge_tile(xadj, n, w * 32, xs, [&](int32_t v, int32_t p) {
+      if (part[v] != part[adj[p]]) acc += (unsigned long long)(long long)(HAS_W ? adjwgt[p] : 1);
+    });
+  }
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0 && acc) atomicAdd(reinterpret_cast<unsigned long long*>(&cuts[blockIdx.y]), acc);
+}
+
+void trial_cuts(const DGraph& g, const idx_t* parts, int ntrials, long long* cuts, cudaStream_t st) {
+  RMB_CUDA(cudaMemsetAsync(cuts, 0, sizeof(long long) * (size_t)ntrials, st));
+  const dim3 grid((unsigned)grid_for(ceil_div(g.n, 32), 8, 148 * 8), (unsigned)ntrials);
+  if (g.adjwgt) k_cut_trials<true><<<grid, 256, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, g.n, parts, cuts);
+  else k_cut_trials<false><<<grid, 256, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, g.n, parts, cuts);
+  RMB_LAUNCH_CHECK();
+}
+
 template <bool HAS_VW>
 __global__ void k_pw(const idx_t* __restrict__ vwgt, int32_t n, int32_t ncon, const idx_t* __restrict__ part,
                      int32_t K, long long* pw) {

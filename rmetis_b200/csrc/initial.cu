@@ -29,7 +29,7 @@ __global__ void __launch_bounds__(32) k_grow(const idx_t* __restrict__ xadj, con
                                              int32_t n, int32_t ncon, int32_t k, const idx_t* __restrict__ seeds,
                                              const long long* __restrict__ grow_tgt, idx_t* __restrict__ parts,
                                              unsigned char* __restrict__ gscratch, size_t scratch_bytes,
-                                             int use_smem, long long* __restrict__ cuts) {
+                                             int use_smem) {
   extern __shared__ __align__(16) unsigned char smem[];
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -57,6 +57,12 @@ __global__ void __launch_bounds__(32) k_grow(const idx_t* __restrict__ xadj, con
   }
   __syncwarp();
 
+  // A part whose queue has run empty can never grow again (its queue only
+  // receives vertices it claims by popping), so it is dropped from the rounds:
+  // lane w keeps the bits of parts 32w..32w+31 still holding a queue (k <=
+  // 1024; above that every part stays in).
+  const bool track = nwords <= 32;
+  unsigned alive = ~0u;
   bool any_active = true;
   while (any_active) {
     // Parts below target on some constraint (grow.rs:54-58), as a bitmap.
@@ -68,7 +74,8 @@ __global__ void __launch_bounds__(32) k_grow(const idx_t* __restrict__ xadj, con
           if (!(pw[(int64_t)p * ncon + c] >= grow_tgt[(int64_t)p * ncon + c])) { needs = true; break; }
       }
       const unsigned m = __ballot_sync(FULL, needs);
-      if (lane == 0) needy[w0] = m;
+      const unsigned al = track ? __shfl_sync(FULL, alive, w0) : ~0u;
+      if (lane == 0) needy[w0] = m & al;
     }
     __syncwarp();
     int32_t active = 0;
@@ -83,40 +90,56 @@ __global__ void __launch_bounds__(32) k_grow(const idx_t* __restrict__ xadj, con
           const int32_t v = qh;
           qh = next[v];
           const int32_t e = __ldg(&xadj[v + 1]);
-          for (int32_t b = __ldg(&xadj[v]); b < e; b += 32) {
-            const int32_t j = b + lane;
-            int32_t u = -1;
-            bool cand = false;
-            if (j < e) {
-              u = __ldg(&adj[j]);
-              cand = part[u] == -1;
+          // The row is read 4 chunks of 32 at a time: neighbours and their
+          // part labels are loaded together, then the chunks are claimed in
+          // order. A claim earlier in the group may have taken a neighbour that
+          // is listed again later in the row, so after one the later
+          // candidates' labels are read again.
+          for (int32_t b0 = __ldg(&xadj[v]); b0 < e; b0 += 4 * 32) {
+            int32_t uu[4];
+            bool cc[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int32_t j = b0 + q * 32 + lane;
+              uu[q] = j < e ? __ldg(&adj[j]) : -1;
             }
-            const unsigned peers = __match_any_sync(FULL, cand ? u : -(lane + 2));
-            const bool first = cand && (__ffs(peers) - 1) == lane;
-            const unsigned fm = __ballot_sync(FULL, first);
-            if (fm) {
-              grew = true;
-              if (first) part[u] = p;
-              for (int c = 0; c < ncon; ++c) {
-                long long w = first ? (long long)(HAS_VW ? __ldg(&vwgt[(int64_t)u * ncon + c]) : 1) : 0;
-                w = warp_sum(w);
-                if (lane == 0) pw[(int64_t)p * ncon + c] += w;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) cc[q] = uu[q] >= 0 && part[uu[q]] == -1;
+            bool claimed = false;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              if (b0 + q * 32 >= e) break;
+              const int32_t u = uu[q];
+              bool cand = cc[q];
+              if (claimed && cand) cand = part[u] == -1;
+              const unsigned peers = __match_any_sync(FULL, cand ? u : -(lane + 2));
+              const bool first = cand && (__ffs(peers) - 1) == lane;
+              const unsigned fm = __ballot_sync(FULL, first);
+              if (fm) {
+                grew = true;
+                claimed = true;
+                if (first) part[u] = p;
+                for (int c = 0; c < ncon; ++c) {
+                  long long w = first ? (long long)(HAS_VW ? __ldg(&vwgt[(int64_t)u * ncon + c]) : 1) : 0;
+                  w = warp_sum(w);
+                  if (lane == 0) pw[(int64_t)p * ncon + c] += w;
+                }
+                // Link the claimed vertices in lane order and append them.
+                const unsigned above = fm & ~((2u << lane) - 1u);
+                const int nl = above ? (__ffs(above) - 1) : lane;
+                const int32_t unext = __shfl_sync(FULL, u, nl);
+                if (first) next[u] = above ? unext : -1;
+                const int32_t ufirst = __shfl_sync(FULL, u, __ffs(fm) - 1);
+                const int32_t ulast = __shfl_sync(FULL, u, 31 - __clz(fm));
+                if (qh == -1) {
+                  qh = ufirst;
+                } else if (lane == 0) {
+                  next[qt] = ufirst;
+                }
+                qt = ulast;
               }
-              // Link the claimed vertices in lane order and append them.
-              const unsigned above = fm & ~((2u << lane) - 1u);
-              const int nl = above ? (__ffs(above) - 1) : lane;
-              const int32_t unext = __shfl_sync(FULL, u, nl);
-              if (first) next[u] = above ? unext : -1;
-              const int32_t ufirst = __shfl_sync(FULL, u, __ffs(fm) - 1);
-              const int32_t ulast = __shfl_sync(FULL, u, 31 - __clz(fm));
-              if (qh == -1) {
-                qh = ufirst;
-              } else if (lane == 0) {
-                next[qt] = ufirst;
-              }
-              qt = ulast;
+              __syncwarp();
             }
-            __syncwarp();
           }
           if (grew) break;
         }
@@ -124,6 +147,7 @@ __global__ void __launch_bounds__(32) k_grow(const idx_t* __restrict__ xadj, con
           head[p] = qh;
           tail[p] = qt;
         }
+        if (track && qh == -1 && lane == (p >> 5)) alive &= ~(1u << (p & 31));
         __syncwarp();
         if (grew) ++active;
       }
@@ -215,16 +239,9 @@ __global__ void __launch_bounds__(32) k_grow(const idx_t* __restrict__ xadj, con
   }
   __syncwarp();
 
-  // Write the partition out and compute its edge cut (both directions).
-  long long acc = 0;
-  for (int32_t v = lane; v < n; v += 32) {
-    const int32_t pv = part[v];
-    out[v] = pv;
-    for (int32_t j = __ldg(&xadj[v]); j < __ldg(&xadj[v + 1]); ++j)
-      if (part[__ldg(&adj[j])] != pv) acc += adjwgt ? __ldg(&adjwgt[j]) : 1;
-  }
-  acc = warp_sum(acc);
-  if (lane == 0) cuts[trial] = acc;
+  // Write the partition out; the trial cuts are computed edge-parallel for
+  // all trials at once afterwards (trial_cuts).
+  for (int32_t v = lane; v < n; v += 32) out[v] = part[v];
 }
 
 void grow_trials(const DGraph& g, int k, int ntrials, const idx_t* seeds, const long long* grow_tgt, idx_t* parts,
@@ -241,8 +258,9 @@ void grow_trials(const DGraph& g, int k, int ntrials, const idx_t* seeds, const 
   RMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimit));
   const int ph = profiler().begin(kProfGrow, st);
   kern<<<ntrials, 32, dyn, st>>>(g.xadj, g.adjncy, g.adjwgt, g.vwgt, g.n, g.ncon, k, seeds, grow_tgt, parts, scratch,
-                                 bytes_al, use_smem, cuts);
+                                 bytes_al, use_smem);
   RMB_LAUNCH_CHECK();
+  trial_cuts(g, parts, ntrials, cuts, st);
   profiler().end(ph, st, (double)ntrials * (16.0 * g.n + 8.0 * (double)g.m));
   arena.reset_to(mk);
 }

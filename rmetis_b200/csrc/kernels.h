@@ -41,6 +41,8 @@ int validate_device(const DGraph& g, Arena& arena, cudaStream_t st, int32_t* h_s
 void cut_and_weights(const DGraph& g, const idx_t* part, int k, unsigned long long* cut_acc,
                      long long* pw, cudaStream_t st);
 void partition_weights_only(const DGraph& g, const idx_t* part, int k, long long* pw, cudaStream_t st);
+// Edge cuts (both directions) of ntrials partitions parts[trial][g.n].
+void trial_cuts(const DGraph& g, const idx_t* parts, int ntrials, long long* cuts, cudaStream_t st);
 
 // total_weight (src/graph/mod.rs:152-160): i64 sums per constraint (zeroed here).
 void total_weight(const DGraph& g, long long* tot, cudaStream_t st);

@@ -20,6 +20,8 @@
 #include <chrono>
 #include <vector>
 #include <climits>
+#include <mutex>
+#include <set>
 #include <cstdio>
 #include <cstdlib>
 
@@ -254,7 +256,18 @@ struct MoverRecs {  // structure of arrays, nm entries each
   int32_t* cp;     // [nm][kInline] candidate parts
   int32_t* cg;     // [nm][kInline] candidate gains
   int32_t* vw;     // [nm][ncon]
+  int32_t* np;     // kLong movers with -w_from <= 0: number of positive-gain candidates, else -1
 };
+
+// Positive-gain candidates of kLong movers, gathered into shared memory by the
+// loader warps (dynamic shared memory after the walk's static buffers): per
+// buffer, 32 slots per mover and the count (-1: not gathered).
+constexpr int kPoolSlots = 32;
+constexpr size_t kPoolBytes = sizeof(int32_t) * 2 * ((size_t)kWalkChunk * kPoolSlots + kWalkChunk);
+__device__ __forceinline__ int32_t* pool_cand(int32_t* dyn, int buf) { return dyn + buf * kWalkChunk * kPoolSlots; }
+__device__ __forceinline__ int32_t* pool_np(int32_t* dyn, int buf) {
+  return dyn + 2 * kWalkChunk * kPoolSlots + buf * kWalkChunk;
+}
 
 // One thread per mover: copy its data into a record and add its weight to
 // the bounds: in_max[p] over every part it may move to, out_max[pv].
@@ -354,6 +367,15 @@ __device__ void classify_body(Lanes L, const int32_t* __restrict__ nm_dev, int32
       }
     }
     if (known == kContended && ne > kInline) known = kLong;
+    int32_t npos = -1;
+    if (known == kLong && ig <= 0) {
+      // The decision of such a mover is the first feasible part among its
+      // positive-gain candidates (the scan ends at the first gain <= 0).
+      const int32_t s0 = r.coff[j];
+      npos = 0;
+      while (npos < ne && (npos < kInline ? r.cg[j * kInline + npos] : cand_g[s0 + npos]) > 0) ++npos;
+    }
+    r.np[j] = npos;
     // Count the kLong movers (one atomic per warp).
     const unsigned lm = __ballot_sync(__activemask(), known == kLong);
     if (lm && (threadIdx.x & 31) == __ffs(lm) - 1) atomicAdd(long_flag, __popc(lm));
@@ -401,6 +423,21 @@ __device__ inline void walk_load(WalkBuf& b, const MoverRecs& r, int32_t j0, int
   for (int i = tid; i < kWalkChunk * ncon; i += nthreads) {
     const int64_t j = (int64_t)j0 * ncon + i;
     if (j < (int64_t)nm * ncon) b.vw[(i / ncon) * kMaxCon + (i % ncon)] = r.vw[j];
+  }
+}
+
+// Loader warps: the positive-gain candidates of the chunk's kLong movers
+// (one warp per mover, one lane per candidate, at most kPoolSlots).
+__device__ inline void walk_pool_load(int32_t* pc, int32_t* pn, const MoverRecs& r, const idx_t* __restrict__ cand_p,
+                                      int32_t j0, int32_t nm, int tid, int nthreads) {
+  const int lw = tid >> 5, nlw = nthreads >> 5, lane = tid & 31;
+  for (int i = lw; i < kWalkChunk; i += nlw) {
+    const int32_t j = j0 + i;
+    if (j >= nm) break;
+    const int32_t npv = r.known[j] == kLong ? r.np[j] : -1;
+    if (lane == 0) pn[i] = npv;
+    const int32_t cnt = npv < kPoolSlots ? npv : kPoolSlots;
+    if (lane < cnt) pc[i * kPoolSlots + lane] = cand_p[r.coff[j] + lane];
   }
 }
 
@@ -831,14 +868,17 @@ __device__ __forceinline__ void walk_chunks(int32_t nm, const MoverRecs& r, int3
                                             const idx_t* __restrict__ cand_p, const idx_t* __restrict__ cand_g,
                                             const WalkOut& wo, WalkBuf* buf, int32_t* dbuf, unsigned* ebits,
                                             S* sslack, PartRegs<S, R, NC>& s, int32_t& moves, int tid, int lane,
-                                            int warp) {
+                                            int warp, int32_t* dyn) {
   bool dirty = false;  // a move since sslack was last written
+  constexpr bool POOL = LONG && MODE == kCut;  // kLong candidates gathered by the loaders
   const int32_t nchunks = (int32_t)ceil_div(nm, kWalkChunk);
   for (int32_t ch = 0; ch < nchunks; ++ch) {
     const int32_t j0 = ch * kWalkChunk;
     const int32_t cnt = min(kWalkChunk, nm - j0);
     if (warp == 0) {
       const WalkBuf& b = buf[ch & 1];
+      const int32_t* pc = POOL ? pool_cand(dyn, ch & 1) : nullptr;
+      const int32_t* pn = POOL ? pool_np(dyn, ch & 1) : nullptr;
       auto c_of = [&](int i, int q) { return b.cg[i * kInline + q] > 0 ? b.cp[i * kInline + q] : -1; };
       // kContended and kLong movers take the general decision (in the repair
       // pass every mover is kContended, and most leave at the overweight
@@ -849,7 +889,7 @@ __device__ __forceinline__ void walk_chunks(int32_t nm, const MoverRecs& r, int3
 #pragma unroll
       for (int c = 0; c < NC; ++c) nw[c] = b.vw[c];
       CandChunk npre{0, -1};
-      if (LONG && MODE == kCut && nk == kLong) npre = first_chunk(b, 0, lane, cand_p, cand_g);
+      if (POOL && nk == kLong && pn[0] < 0) npre = first_chunk(b, 0, lane, cand_p, cand_g);
       for (int32_t i = 0; i < cnt; ++i) {
         const int32_t kn = nk, pv = npv, c1 = nc1, c2 = nc2;
         int32_t w[NC];
@@ -863,7 +903,7 @@ __device__ __forceinline__ void walk_chunks(int32_t nm, const MoverRecs& r, int3
           nc2 = c_of(i + 1, 1);
 #pragma unroll
           for (int c = 0; c < NC; ++c) nw[c] = b.vw[(i + 1) * kMaxCon + c];
-          if (LONG && MODE == kCut && nk == kLong) npre = first_chunk(b, i + 1, lane, cand_p, cand_g);
+          if (POOL && nk == kLong && pn[i + 1] < 0) npre = first_chunk(b, i + 1, lane, cand_p, cand_g);
         }
         int32_t d = kn;
         if (MODE == kCut && kn == kFast) {
@@ -872,7 +912,35 @@ __device__ __forceinline__ void walk_chunks(int32_t nm, const MoverRecs& r, int3
           d = f1 ? c1 : (f2 ? c2 : -1);
         } else if (kn <= kContended && kn != kFast) {  // kContended or kLong (this form keeps the
                                                         // common kFast path short)
-          if (LONG)
+          if (POOL && kn == kLong && pn[i] >= 0) {
+            // Gathered positive-gain candidates: the first feasible one, in
+            // order, against the shared slack copy.
+            if (dirty) {
+#pragma unroll
+              for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+                for (int c = 0; c < NC; ++c) sslack[(rr * 32 + lane) * NC + c] = s.sl[rr][c];
+              __syncwarp();
+              dirty = false;
+            }
+            const int32_t npos = pn[i];
+            const int32_t cp = npos < kPoolSlots ? npos : kPoolSlots;
+            const int32_t p = lane < cp ? pc[i * kPoolSlots + lane] : -1;
+            bool fits = p >= 0;
+#pragma unroll
+            for (int c = 0; c < NC; ++c) fits = fits && (S)w[c] <= sslack[(p >= 0 ? p : 0) * NC + c];
+            const unsigned m = __ballot_sync(0xffffffffu, fits);
+            if (m) {
+              d = __shfl_sync(0xffffffffu, p, __ffs(m) - 1);
+            } else if (npos > kPoolSlots) {
+              const int32_t ig = (int32_t)(0u - (uint32_t)b.wf[i]);
+              const int32_t rs = coop_scan<S, NC>(sslack, lane, b, i, kPoolSlots, b.ne[i], ig, 0, cand_p, cand_g, w,
+                                                  CandChunk{0, -1});
+              d = rs >= -1 ? rs : -1;
+            } else {
+              d = -1;
+            }
+          } else if (LONG)
             d = reg_decide<MODE, S, R, NC>(s, lane, b, i, k, cand_p, cand_g, w, ebits,
                                            MODE == kCut && kn == kLong ? &pre : nullptr, sslack, dirty);
           else
@@ -899,6 +967,9 @@ __device__ __forceinline__ void walk_chunks(int32_t nm, const MoverRecs& r, int3
         if (dbuf[i] >= 0) wo.part[wo.movers[j0 + i]] = dbuf[i];
     } else if (ch + 1 < nchunks) {
       walk_load(buf[(ch + 1) & 1], r, (ch + 1) * kWalkChunk, nm, NC, tid - 32, blockDim.x - 32);
+      if (POOL)
+        walk_pool_load(pool_cand(dyn, (ch + 1) & 1), pool_np(dyn, (ch + 1) & 1), r, cand_p, (ch + 1) * kWalkChunk,
+                       nm, tid - 32, blockDim.x - 32);
     }
     __syncthreads();
   }
@@ -930,7 +1001,8 @@ __device__ __forceinline__ void walk_reg_body(WalkShared<S, R, NC>& sh, const in
                                               const idx_t* __restrict__ cand_g, long long* __restrict__ pw,
                                               const long long* __restrict__ feas_g,
                                               const long long* __restrict__ over_g, const WalkOut& wo,
-                                              int32_t* __restrict__ nmoves, int32_t* __restrict__ long_flag) {
+                                              int32_t* __restrict__ nmoves, int32_t* __restrict__ long_flag,
+                                              int32_t* dyn) {
   WalkBuf* buf = sh.buf;
   int32_t* dbuf = sh.dbuf;
   unsigned* ebits = sh.ebits;
@@ -957,15 +1029,18 @@ __device__ __forceinline__ void walk_reg_body(WalkShared<S, R, NC>& sh, const in
       }
     }
   }
-  if (nm > 0) walk_load(buf[0], r, 0, nm, NC, tid, blockDim.x);
+  if (nm > 0) {
+    walk_load(buf[0], r, 0, nm, NC, tid, blockDim.x);
+    if (MODE == kCut && any_long) walk_pool_load(pool_cand(dyn, 0), pool_np(dyn, 0), r, cand_p, 0, nm, tid, blockDim.x);
+  }
   __syncthreads();
   int32_t moves = 0;
   if (any_long)
     walk_chunks<MODE, S, R, NC, true>(nm, r, k, cand_p, cand_g, wo, buf, dbuf, ebits, sslack, s, moves, tid, lane,
-                                      warp);
+                                      warp, dyn);
   else
     walk_chunks<MODE, S, R, NC, false>(nm, r, k, cand_p, cand_g, wo, buf, dbuf, ebits, sslack, s, moves, tid,
-                                       lane, warp);
+                                       lane, warp, dyn);
   if (warp == 0) {
 #pragma unroll
     for (int rr = 0; rr < R; ++rr) {
@@ -996,7 +1071,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
                                                            WalkOut wo, int32_t* __restrict__ nmoves,
                                                            int32_t* __restrict__ long_flag) {
   __shared__ WalkShared<S, R, NC> sh;
-  walk_reg_body<MODE, S, R, NC>(sh, nm_dev, r, k, cand_p, cand_g, pw, feas_g, over_g, wo, nmoves, long_flag);
+  extern __shared__ __align__(16) int32_t wdyn[];  // kPoolBytes
+  walk_reg_body<MODE, S, R, NC>(sh, nm_dev, r, k, cand_p, cand_g, pw, feas_g, over_g, wo, nmoves, long_flag, wdyn);
 }
 
 
@@ -1042,6 +1118,18 @@ void gain_table(const DGraph& g, const idx_t* part, int k, idx_t* boundary, idx_
   if (ghist) RMB_CUDA(cudaFreeAsync(ghist, st));
 }
 
+// Opts a kernel in to `bytes` of dynamic shared memory on the current device
+// (once per kernel and device).
+static void allow_dyn_smem(const void* kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  RMB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.insert({kernel, dev}).second)
+    RMB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
 template <int MODE>
 static int launch_walk(int32_t nmax, const int32_t* nm_dev, const idx_t* movers, const DGraph& g, const idx_t* part,
                         int k, const idx_t* ncand, const idx_t* wfrom, const idx_t* cand_p, const idx_t* cand_g,
@@ -1062,9 +1150,12 @@ static int launch_walk(int32_t nmax, const int32_t* nm_dev, const idx_t* movers,
   }
   const int ph = profiler().begin(kProfDecide, st);
   const int ncon = g.ncon;
-#define RMB_WALK_REG(ST, RR, NCC)                                                                     \
-  k_walk_reg<MODE, ST, RR, NCC><<<1, kWalkThreads, 0, st>>>(nm_dev, r, k, cand_p, cand_g, pw, feas, over, wo, \
-                                                            nmoves, long_flag)
+#define RMB_WALK_REG(ST, RR, NCC)                                                                         \
+  do {                                                                                                    \
+    allow_dyn_smem((const void*)k_walk_reg<MODE, ST, RR, NCC>, kPoolBytes);                               \
+    k_walk_reg<MODE, ST, RR, NCC><<<1, kWalkThreads, kPoolBytes, st>>>(nm_dev, r, k, cand_p, cand_g, pw, feas, \
+                                                                       over, wo, nmoves, long_flag);       \
+  } while (0)
 #define RMB_WALK_REG_R(ST, NCC)                       \
   do {                                                \
     if (rr == 1) RMB_WALK_REG(ST, 1, NCC);            \
@@ -1162,8 +1253,9 @@ __device__ __forceinline__ void fused_pass(const LevelRefine& P, WalkShared<S, R
     __syncthreads();
   }
   const WalkOut wo{P.movers, P.part, P.in_max, P.out_max, P.k * NC};
+  extern __shared__ __align__(16) int32_t wdyn[];  // kPoolBytes
   walk_reg_body<MODE, S, R, NC>(sh, nm_dev, P.r, P.k, P.cand_p, P.cand_g, P.pw, P.feas, P.over, wo, nm_dev + 1,
-                                P.long_flag);
+                                P.long_flag, wdyn);
   __syncthreads();
 }
 
@@ -1193,10 +1285,11 @@ __global__ void __launch_bounds__(kFusedThreads) k_refine_level(LevelRefine P) {
 template <bool HAS_W, typename S, int NC>
 static void launch_fused_r(const LevelRefine& P, cudaStream_t st) {
   const int k = P.k;
-  if (k <= 32) k_refine_level<HAS_W, S, 1, NC><<<1, kFusedThreads, 0, st>>>(P);
-  else if (k <= 64) k_refine_level<HAS_W, S, 2, NC><<<1, kFusedThreads, 0, st>>>(P);
-  else if (k <= 128) k_refine_level<HAS_W, S, 4, NC><<<1, kFusedThreads, 0, st>>>(P);
-  else k_refine_level<HAS_W, S, 8, NC><<<1, kFusedThreads, 0, st>>>(P);
+  auto kern = k <= 32 ? k_refine_level<HAS_W, S, 1, NC>
+              : k <= 64 ? k_refine_level<HAS_W, S, 2, NC>
+              : k <= 128 ? k_refine_level<HAS_W, S, 4, NC> : k_refine_level<HAS_W, S, 8, NC>;
+  allow_dyn_smem((const void*)kern, kPoolBytes);
+  kern<<<1, kFusedThreads, kPoolBytes, st>>>(P);
 }
 
 template <bool HAS_W>
@@ -1241,6 +1334,7 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
   r.cp = arena.alloc<int32_t>((size_t)g.n * kInline);
   r.cg = arena.alloc<int32_t>((size_t)g.n * kInline);
   r.vw = arena.alloc<int32_t>((size_t)g.n * g.ncon);
+  r.np = arena.alloc<int32_t>((size_t)g.n);
   const bool fused = rp.fused_max_n > 0 && g.n <= rp.fused_max_n && k <= 256 && g.ncon <= 2;
   int32_t* ghist = nullptr;
   if (nheavy > 0 && (fused || k > kGainHist))

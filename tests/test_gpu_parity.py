@@ -392,3 +392,33 @@ def test_grow_leftovers_skewed_levels(rmb, oracle):
     parts, _ = F.grow_partition(rmb.Graph(n, 1, x, a), k, t, seeds)
     ref, _ = oracle.grow_partition(x, a, k, t, seeds=seeds[0])
     assert (parts[0] == ref).all()
+
+
+@pytest.mark.parametrize("L,shift", [(100, 100), (60, 33), (300, 150)])
+def test_grow_duplicate_neighbours(rmb, oracle, L, shift):
+    """A hub's row lists every leaf twice (the reference does not reject
+    duplicate entries, src/graph/validate.rs:88-108): the second occurrence,
+    in a later chunk or group of the row scan, must not be claimed again
+    (src/initial/grow.rs:60-80)."""
+    from rmetis_b200 import functions as F
+    n = L + 1 + 40
+    rows = [[] for _ in range(n)]
+    leaves = list(range(1, L + 1))
+    order = leaves[shift % L:] + leaves[:shift % L]
+    rows[0] = leaves + order                  # each leaf twice, far apart
+    for u in leaves:
+        rows[u] = [0, 0]
+    for i in range(L + 1, n - 1):             # a path elsewhere
+        rows[i].append(i + 1)
+        rows[i + 1].append(i)
+    x = np.zeros(n + 1, np.int32)
+    x[1:] = np.cumsum([len(r) for r in rows])
+    a = np.array([u for r in rows for u in r], np.int32)
+    assert oracle.validate_csr(n, 1, x, a) == 0
+    k = 3
+    t = oracle.compute_target_weights(n, 1, None, k)
+    seeds = np.array([[0, L + 1, n - 1], [3, L + 5, 0]], np.int32)
+    parts, _ = F.grow_partition(rmb.Graph(n, 1, x, a), k, t, seeds)
+    for i in range(2):
+        ref, _ = oracle.grow_partition(x, a, k, t, seeds=seeds[i])
+        assert (parts[i] == ref).all()
