@@ -427,17 +427,46 @@ __device__ inline void walk_load(WalkBuf& b, const MoverRecs& r, int32_t j0, int
 }
 
 // Loader warps: the positive-gain candidates of the chunk's kLong movers
-// (one warp per mover, one lane per candidate, at most kPoolSlots).
+// (at most kPoolSlots each). A warp takes 32 movers at a time: one coalesced
+// read of their kind, count and offset, then their candidate rows, eight
+// movers per step so that eight loads are in flight before any store.
 __device__ inline void walk_pool_load(int32_t* pc, int32_t* pn, const MoverRecs& r, const idx_t* __restrict__ cand_p,
                                       int32_t j0, int32_t nm, int tid, int nthreads) {
+  const unsigned FULL = 0xffffffffu;
   const int lw = tid >> 5, nlw = nthreads >> 5, lane = tid & 31;
-  for (int i = lw; i < kWalkChunk; i += nlw) {
-    const int32_t j = j0 + i;
-    if (j >= nm) break;
-    const int32_t npv = r.known[j] == kLong ? r.np[j] : -1;
-    if (lane == 0) pn[i] = npv;
-    const int32_t cnt = npv < kPoolSlots ? npv : kPoolSlots;
-    if (lane < cnt) pc[i * kPoolSlots + lane] = cand_p[r.coff[j] + lane];
+  for (int g0 = lw * 32; g0 < kWalkChunk; g0 += nlw * 32) {
+    const int32_t j = j0 + g0 + lane;
+    int32_t npv = -1, coff = 0;
+    if (j < nm && r.known[j] == kLong) {
+      npv = r.np[j];
+      coff = r.coff[j];
+    }
+    pn[g0 + lane] = npv;
+    unsigned todo = __ballot_sync(FULL, npv > 0);
+    while (todo) {
+      constexpr int kB = 8;
+      int li[kB], cnt[kB], co[kB];
+#pragma unroll
+      for (int q = 0; q < kB; ++q) {
+        li[q] = -1;
+        cnt[q] = 0;
+        co[q] = 0;
+        if (todo) {  // uniform
+          const int l = __ffs(todo) - 1;
+          todo &= todo - 1;
+          const int32_t c = __shfl_sync(FULL, npv, l);
+          li[q] = l;
+          cnt[q] = c < kPoolSlots ? c : kPoolSlots;
+          co[q] = __shfl_sync(FULL, coff, l);
+        }
+      }
+      int32_t val[kB];
+#pragma unroll
+      for (int q = 0; q < kB; ++q) val[q] = lane < cnt[q] ? __ldg(&cand_p[co[q] + lane]) : 0;
+#pragma unroll
+      for (int q = 0; q < kB; ++q)
+        if (lane < cnt[q]) pc[(g0 + li[q]) * kPoolSlots + lane] = val[q];
+    }
   }
 }
 
