@@ -422,3 +422,50 @@ def test_grow_duplicate_neighbours(rmb, oracle, L, shift):
     for i in range(2):
         ref, _ = oracle.grow_partition(x, a, k, t, seeds=seeds[i])
         assert (parts[i] == ref).all()
+
+
+@pytest.mark.parametrize("k", [300, 700])
+def test_greedy_refine_general_walk(rmb, oracle, k):
+    """More than 256 parts: the windowed walk against shared-memory weights
+    (k * ncon <= 4096), on long candidate lists."""
+    x, a = G.rmat(12, seed=17)
+    n = len(x) - 1
+    part = np.random.default_rng(k).integers(0, k, n).astype(np.int32)
+    stats = _refine_case(rmb, oracle, x, a, None, None, part, k, [1.03])
+    assert stats[1] > 0
+
+
+def test_greedy_refine_general_walk_global_weights(rmb, oracle):
+    """k * ncon above 4096: part weights and thresholds stay in global memory;
+    heavy rows with k above the shared histogram of the warp gain path."""
+    x, a, v, w = load("star_1500")
+    n = len(x) - 1
+    k = 2100
+    v2 = np.random.default_rng(3).integers(1, 5, 2 * n).astype(np.int32)
+    part = np.random.default_rng(4).integers(0, k, n).astype(np.int32)
+    _refine_case(rmb, oracle, x, a, v2, w, part, k, [1.2, 1.3], ncon=2)
+
+
+@pytest.mark.parametrize("ncon", [3, 5])
+def test_greedy_refine_many_constraints(rmb, oracle, ncon):
+    x, a, _, w = G.random_graph(3000, 8.0, seed=41 + ncon)
+    n = len(x) - 1
+    v = np.random.default_rng(ncon).integers(1, 9, ncon * n).astype(np.int32)
+    k = 20
+    part = np.random.default_rng(5).integers(0, k, n).astype(np.int32)
+    _refine_case(rmb, oracle, x, a, v, w, part, k, [1.05 + 0.02 * c for c in range(ncon)], ncon=ncon)
+
+
+@pytest.mark.parametrize("k,ncon", [(300, 1), (24, 3)])
+def test_pipeline_replay_general_walk(rmb, oracle, k, ncon):
+    from tests.conftest import greedy_options
+    x, a, _, w = G.random_graph(9000, 10.0, seed=61)
+    n = len(x) - 1
+    v = np.random.default_rng(62).integers(1, 6, ncon * n).astype(np.int32)
+    g = rmb.Graph(n, ncon, x, a, vwgt=v, adjwgt=w)
+    res, mats, seeds, _ = rmb.part_graph_kway_trace(g, k, options=rmb.Options(rtype=rmb.RType.Greedy, seed=8))
+    rc, part, obj = oracle.part_graph_kway(x, a, k, vwgt=v, adjwgt=w, ncon=ncon, options=greedy_options(seed=8),
+                                           script=(mats, seeds))
+    assert rc == 1
+    assert obj == res.objval
+    assert (part == res.part).all()
