@@ -919,22 +919,72 @@ __device__ __forceinline__ void walk_chunks(int32_t nm, const MoverRecs& r, int3
       for (int c = 0; c < NC; ++c) nw[c] = b.vw[c];
       CandChunk npre{0, -1};
       if (POOL && nk == kLong && pn[0] < 0) npre = first_chunk(b, 0, lane, cand_p, cand_g);
+      // Moves a vertex of weight wv from part `from` to part `to` in the
+      // register slacks.
+      auto apply = [&](int32_t from, int32_t to, const int32_t* wv) {
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            const S dw = (S)wv[c];
+            const int32_t p = rr * 32 + lane;
+            const S delta = (from == p ? dw : (S)0) - (to == p ? dw : (S)0);
+            s.sl[rr][c] += delta;
+            s.ov[rr][c] += delta;
+          }
+      };
+      auto load_next = [&](int32_t j) {
+        nk = b.known[j];
+        npv = b.pv[j];
+        nc1 = c_of(j, 0);
+        nc2 = c_of(j, 1);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) nw[c] = b.vw[j * kMaxCon + c];
+        if (POOL && nk == kLong && pn[j] < 0) npre = first_chunk(b, j, lane, cand_p, cand_g);
+      };
       for (int32_t i = 0; i < cnt; ++i) {
         const int32_t kn = nk, pv = npv, c1 = nc1, c2 = nc2;
         int32_t w[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) w[c] = nw[c];
         CandChunk pre = npre;
-        if (i + 1 < cnt) {
-          nk = b.known[i + 1];
-          npv = b.pv[i + 1];
-          nc1 = c_of(i + 1, 0);
-          nc2 = c_of(i + 1, 1);
-#pragma unroll
-          for (int c = 0; c < NC; ++c) nw[c] = b.vw[(i + 1) * kMaxCon + c];
-          if (POOL && nk == kLong && pn[i + 1] < 0) npre = first_chunk(b, i + 1, lane, cand_p, cand_g);
-        }
+        if (i + 1 < cnt) load_next(i + 1);
         int32_t d = kn;
+        if (MODE == kCut && kn == kFast && nk == kFast && i + 1 < cnt) {
+          // Two two-candidate movers in a row, decided together against the
+          // same slacks. The second one's decision depends only on the slacks
+          // of its own two candidates, which the first one's move changes
+          // only if one of them is that move's source or target; then it is
+          // decided again after the move.
+          const bool f1 = __any_sync(0xffffffffu, lane_fits(s, lane, c1, w));
+          const bool f2 = __any_sync(0xffffffffu, lane_fits(s, lane, c2, w));
+          const bool g1 = __any_sync(0xffffffffu, lane_fits(s, lane, nc1, nw));
+          const bool g2 = __any_sync(0xffffffffu, lane_fits(s, lane, nc2, nw));
+          d = f1 ? c1 : (f2 ? c2 : -1);
+          int32_t d2 = g1 ? nc1 : (g2 ? nc2 : -1);
+          if (d >= 0) {
+            apply(pv, d, w);
+            dirty = true;
+            ++moves;
+            if (nc1 == pv || nc1 == d || nc2 == pv || nc2 == d) {
+              const bool h1 = __any_sync(0xffffffffu, lane_fits(s, lane, nc1, nw));
+              const bool h2 = __any_sync(0xffffffffu, lane_fits(s, lane, nc2, nw));
+              d2 = h1 ? nc1 : (h2 ? nc2 : -1);
+            }
+          }
+          if (lane == 0) {
+            dbuf[i] = d;
+            dbuf[i + 1] = d2;
+          }
+          if (d2 >= 0) {
+            apply(npv, d2, nw);
+            dirty = true;
+            ++moves;
+          }
+          ++i;
+          if (i + 1 < cnt) load_next(i + 1);
+          continue;
+        }
         if (MODE == kCut && kn == kFast) {
           const bool f1 = __any_sync(0xffffffffu, lane_fits(s, lane, c1, w));
           const bool f2 = __any_sync(0xffffffffu, lane_fits(s, lane, c2, w));
@@ -977,16 +1027,7 @@ __device__ __forceinline__ void walk_chunks(int32_t nm, const MoverRecs& r, int3
         }
         if (lane == 0) dbuf[i] = d;
         if (d >= 0) {
-#pragma unroll
-          for (int rr = 0; rr < R; ++rr)
-#pragma unroll
-            for (int c = 0; c < NC; ++c) {
-              const S dw = (S)w[c];
-              const int32_t p = rr * 32 + lane;
-              const S delta = (pv == p ? dw : (S)0) - (d == p ? dw : (S)0);
-              s.sl[rr][c] += delta;
-              s.ov[rr][c] += delta;
-            }
+          apply(pv, d, w);
           dirty = true;
           ++moves;
         }
