@@ -115,7 +115,10 @@ size_t footprint_bytes(int64_t n, int64_t m, int k, int ncon);
 // submission order when their footprint fits in the budget next to the jobs
 // running (a job larger than the whole budget runs alone). A job's return
 // value (or the code of the rmb::Error it throws) completes its future; the
-// worker's workspace is rewound after every job.
+// worker's workspace is rewound after every job. The footprint is an
+// estimate: a job that runs out of device memory next to others is retried
+// once alone, after every worker has freed the workspace it keeps between
+// jobs (so jobs must be safe to run again).
 class WorkerPool {
  public:
   WorkerPool(int device, int nworkers, size_t budget_bytes);
@@ -130,6 +133,7 @@ class WorkerPool {
     size_t footprint;
     std::function<int(Engine&)> fn;
     std::promise<int> prom;
+    bool alone = false;  // retry after running out of memory: nothing else runs
   };
   void worker_main(int idx);
   int device_;
@@ -141,6 +145,7 @@ class WorkerPool {
   size_t in_use_ = 0;
   int running_ = 0;
   bool stop_ = false;
+  unsigned trim_epoch_ = 0;  // bumped when a job ran out of memory: workers free their workspace
 };
 
 // The pool of a device, created on first use: RMETIS_B200_WORKERS threads

@@ -63,23 +63,41 @@ void WorkerPool::worker_main(int idx) {
   } catch (...) {
     engine.reset();  // every job this thread takes then fails with METIS_ERROR
   }
+  auto free_workspace = [&] {
+    if (!engine) return;
+    cudaStreamSynchronize(engine->stream());
+    engine->arena().release();
+  };
+  unsigned my_epoch = 0;
   for (;;) {
     std::unique_ptr<Job> job;
+    bool trim = false;
     {
       std::unique_lock<std::mutex> lk(mu_);
       // Admission in submission order: the head starts when its footprint
-      // fits next to the running jobs, or when nothing runs.
+      // fits next to the running jobs, or when nothing runs (a retried job
+      // only then).
       cv_.wait(lk, [&] {
-        if (stop_) return true;
+        if (stop_ || my_epoch != trim_epoch_) return true;
         if (queue_.empty()) return false;
-        const size_t fp = queue_.front()->footprint;
-        return running_ == 0 || in_use_ + fp <= budget_;
+        const Job& h = *queue_.front();
+        if (h.alone) return running_ == 0;
+        return running_ == 0 || in_use_ + h.footprint <= budget_;
       });
       if (stop_) return;
-      job = std::move(queue_.front());
-      queue_.pop_front();
-      in_use_ += job->footprint;
-      ++running_;
+      if (my_epoch != trim_epoch_) {
+        my_epoch = trim_epoch_;
+        trim = true;
+      } else {
+        job = std::move(queue_.front());
+        queue_.pop_front();
+        in_use_ += job->footprint;
+        ++running_;
+      }
+    }
+    if (trim) {
+      free_workspace();
+      continue;
     }
     int rc = -4;
     if (engine) {
@@ -95,13 +113,27 @@ void WorkerPool::worker_main(int idx) {
       // A failed job must not leave its workspace half used.
       engine->arena().rewind();
     }
+    bool retry = false;
     {
       std::lock_guard<std::mutex> lk(mu_);
       in_use_ -= job->footprint;
       --running_;
+      if (rc == -3 && !job->alone && engine) {
+        // Out of device memory next to other jobs: every worker frees its
+        // workspace, and this job runs again with nothing beside it.
+        retry = true;
+        ++trim_epoch_;
+        my_epoch = trim_epoch_;
+      }
+    }
+    if (retry) {
+      free_workspace();
+      std::lock_guard<std::mutex> lk(mu_);
+      job->alone = true;
+      queue_.push_front(std::move(job));
     }
     cv_.notify_all();
-    job->prom.set_value(rc);
+    if (!retry) job->prom.set_value(rc);
   }
 }
 

@@ -123,7 +123,13 @@ __global__ void k_gain(const idx_t* __restrict__ xadj, const idx_t* __restrict__
                        const idx_t* __restrict__ adjwgt, int32_t n, int32_t ncon, const idx_t* __restrict__ part,
                        int32_t k, const long long* __restrict__ pw0, const long long* __restrict__ over_thr,
                        idx_t* __restrict__ mover, idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom,
-                       idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g) {
+                       idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g, const int32_t* __restrict__ stop) {
+  // stop: moves of the previous cut pass. None means this pass would find the
+  // same movers and make no move either (the reference stops there): no movers.
+  if (stop && *stop == 0) {
+    RMB_GRID_STRIDE(v, n) mover[v] = 0;
+    return;
+  }
   gain_body<HAS_W, MODE>(grid_lanes(), xadj, adj, adjwgt, n, ncon, part, k, pw0, over_thr, mover, ncand, wfrom,
                          cand_p, cand_g);
 }
@@ -213,7 +219,9 @@ __global__ void k_gain_heavy(const idx_t* __restrict__ xadj, const idx_t* __rest
                              int32_t ncon, const idx_t* __restrict__ part, int32_t k,
                              const long long* __restrict__ pw0, const long long* __restrict__ over_thr,
                              idx_t* __restrict__ mover, idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom,
-                             idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g, int32_t* __restrict__ ghist) {
+                             idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g, int32_t* __restrict__ ghist,
+                             const int32_t* __restrict__ stop) {
+  if (stop && *stop == 0) return;  // k_gain has cleared every mover flag
   __shared__ int32_t sh_all[4][kGainHist];
   const int wib = threadIdx.x >> 5;
   const int32_t gw = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -1150,9 +1158,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
 // Host side
 // ---------------------------------------------------------------------------
 template <int MODE>
-static void launch_gain(const DGraph& g, const idx_t* part, int k, const long long* pw0, const long long* over_thr,
-                        idx_t* mover, idx_t* ncand, idx_t* wfrom, idx_t* cand_p, idx_t* cand_g, const idx_t* heavy,
-                        int32_t nheavy, int32_t* ghist, cudaStream_t st) {
+static int launch_gain(const DGraph& g, const idx_t* part, int k, const long long* pw0, const long long* over_thr,
+                       idx_t* mover, idx_t* ncand, idx_t* wfrom, idx_t* cand_p, idx_t* cand_g, const idx_t* heavy,
+                       int32_t nheavy, int32_t* ghist, cudaStream_t st, const int32_t* stop = nullptr) {
   const int blocks = grid_for(g.n, 256);
   // Algorithmic bytes of a full pass: xadj, part (own + neighbour gathers),
   // adjncy, adjwgt, mover flag.
@@ -1160,22 +1168,23 @@ static void launch_gain(const DGraph& g, const idx_t* part, int k, const long lo
   const int ph = MODE == kCut ? profiler().begin(kProfGain, st) : -1;
   if (g.adjwgt)
     k_gain<true, MODE><<<blocks, 256, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, g.n, g.ncon, part, k, pw0, over_thr,
-                                                mover, ncand, wfrom, cand_p, cand_g);
+                                                mover, ncand, wfrom, cand_p, cand_g, stop);
   else
     k_gain<false, MODE><<<blocks, 256, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, g.n, g.ncon, part, k, pw0, over_thr,
-                                                 mover, ncand, wfrom, cand_p, cand_g);
+                                                 mover, ncand, wfrom, cand_p, cand_g, stop);
   RMB_LAUNCH_CHECK();
   profiler().end(ph, st, bytes);
   if (nheavy > 0) {
     const int hb = grid_for(nheavy, 4, 256);
     if (g.adjwgt)
       k_gain_heavy<true, MODE><<<hb, 128, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, heavy, nheavy, g.ncon, part, k, pw0,
-                                                    over_thr, mover, ncand, wfrom, cand_p, cand_g, ghist);
+                                                    over_thr, mover, ncand, wfrom, cand_p, cand_g, ghist, stop);
     else
       k_gain_heavy<false, MODE><<<hb, 128, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, heavy, nheavy, g.ncon, part, k, pw0,
-                                                     over_thr, mover, ncand, wfrom, cand_p, cand_g, ghist);
+                                                     over_thr, mover, ncand, wfrom, cand_p, cand_g, ghist, stop);
     RMB_LAUNCH_CHECK();
   }
+  return ph;
 }
 
 void gain_table(const DGraph& g, const idx_t* part, int k, idx_t* boundary, idx_t* ncand, idx_t* wfrom,
@@ -1349,7 +1358,12 @@ __global__ void __launch_bounds__(kFusedThreads) k_refine_level(LevelRefine P) {
   }
   __syncthreads();
   fused_pass<HAS_W, kRepair, S, R, NC>(P, sh, sw, 0);
-  for (int pass = 1; pass <= P.niter; ++pass) fused_pass<HAS_W, kCut, S, R, NC>(P, sh, sw, pass);
+  for (int pass = 1; pass <= P.niter; ++pass) {
+    // A cut pass without a move ends the level (greedy.rs:184-186); the
+    // count is read by every thread after the pass's last barrier.
+    if (pass >= 2 && P.counters[2 * (pass - 1) + 1] == 0) break;
+    fused_pass<HAS_W, kCut, S, R, NC>(P, sh, sw, pass);
+  }
 }
 
 template <bool HAS_W, typename S, int NC>
@@ -1409,7 +1423,7 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
   int32_t* ghist = nullptr;
   if (nheavy > 0 && (fused || k > kGainHist))
     ghist = arena.alloc<int32_t>((size_t)k * (fused ? kFusedThreads / 32 : 256 * 4));
-  std::vector<int> walk_handles;
+  std::vector<int> walk_handles, gain_handles;
   if (fused) {
     LevelRefine P;
     P.xadj = g.xadj;
@@ -1453,10 +1467,14 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
   for (int pass = 0; pass <= rp.niter; ++pass) {
     const int mode = pass == 0 ? kRepair : kCut;
     int32_t* nm_dev = counters + 2 * pass;
+    // From the second cut pass on, a previous cut pass without a move makes
+    // this one empty on the device (same result as the reference's break).
+    const int32_t* stop = pass >= 2 ? counters + 2 * (pass - 1) + 1 : nullptr;
     if (mode == kRepair)
       launch_gain<kRepair>(g, part, k, pw, rp.over_thr, mover, ncand, wfrom, cand_p, cand_g, heavy, nheavy, ghist, st);
     else
-      launch_gain<kCut>(g, part, k, pw, rp.over_thr, mover, ncand, wfrom, cand_p, cand_g, heavy, nheavy, ghist, st);
+      gain_handles.push_back(launch_gain<kCut>(g, part, k, pw, rp.over_thr, mover, ncand, wfrom, cand_p, cand_g,
+                                               heavy, nheavy, ghist, st, stop));
     compact_flags(mover, g.n, movers, nm_dev, arena, st);
     if (mode == kRepair)
       walk_handles.push_back(launch_walk<kRepair>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r,
@@ -1478,6 +1496,12 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
     const double rec_bytes = 4.0 * (5 + 2 * kInline + g.ncon) + 4.0;
     for (int pass = 0; pass <= rp.niter; ++pass)
       profiler().set_bytes(walk_handles[pass], rec_bytes * h_scratch[2 * pass]);
+    // A cut pass emptied by the one before it only clears the mover flags.
+    for (int pass = 2; pass <= rp.niter; ++pass)
+      if (h_scratch[2 * (pass - 1) + 1] == 0) {
+        profiler().set_bytes(gain_handles[pass - 1], 4.0 * g.n);
+        for (int q = pass; q <= rp.niter; ++q) h_scratch[2 * q + 1] = 0;
+      }
   }
   if (trace || rp.collect_stats) {
     RMB_CUDA(cudaMemcpyAsync(h_scratch, counters, sizeof(int32_t) * 2 * ((size_t)rp.niter + 1),
