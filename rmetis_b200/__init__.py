@@ -462,3 +462,6 @@ def submit_kway(graph: Graph, nparts: int, tpwgts=None, ubvec=None, options: Opt
     if t <= 0:
         _raise_for(int(t), "submit_kway")
     return KwayRequest(t, (graph, opts, nv, nc, npr, tp, ub), part, obj)
+
+
+from .graphio import format_metis_graph, parse_metis_graph, read_metis_graph, write_metis_graph  # noqa: E402
