@@ -908,6 +908,11 @@ __device__ __forceinline__ void walk_chunks(int32_t nm, const MoverRecs& r, int3
                                             int warp, int32_t* dyn) {
   bool dirty = false;  // a move since sslack was last written
   constexpr bool POOL = LONG && MODE == kCut;  // kLong candidates gathered by the loaders
+  // With 4+ part slots per lane the register test of a candidate costs a
+  // compare per slot plus a vote; two-candidate movers then read the shared
+  // slack copy instead (k > 128; moves are rare there, so the copy is rarely
+  // rewritten). With fewer slots they stay on registers and go in pairs.
+  constexpr bool kSharedFast = R >= 4;
   const int32_t nchunks = (int32_t)ceil_div(nm, kWalkChunk);
   for (int32_t ch = 0; ch < nchunks; ++ch) {
     const int32_t j0 = ch * kWalkChunk;
@@ -958,7 +963,7 @@ __device__ __forceinline__ void walk_chunks(int32_t nm, const MoverRecs& r, int3
         CandChunk pre = npre;
         if (i + 1 < cnt) load_next(i + 1);
         int32_t d = kn;
-        if (MODE == kCut && kn == kFast && nk == kFast && i + 1 < cnt) {
+        if (!kSharedFast && MODE == kCut && kn == kFast && nk == kFast && i + 1 < cnt) {
           // Two two-candidate movers in a row, decided together against the
           // same slacks. The second one's decision depends only on the slacks
           // of its own two candidates, which the first one's move changes
@@ -993,7 +998,26 @@ __device__ __forceinline__ void walk_chunks(int32_t nm, const MoverRecs& r, int3
           if (i + 1 < cnt) load_next(i + 1);
           continue;
         }
-        if (MODE == kCut && kn == kFast) {
+        if (MODE == kCut && kn == kFast && kSharedFast) {
+          // Many part slots per lane: test the two candidates against the
+          // shared slack copy (one broadcast read each), rewritten only after
+          // a move.
+          if (dirty) {
+#pragma unroll
+            for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+              for (int c = 0; c < NC; ++c) sslack[(rr * 32 + lane) * NC + c] = s.sl[rr][c];
+            __syncwarp();
+            dirty = false;
+          }
+          bool f1 = c1 >= 0, f2 = c2 >= 0;
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            f1 = f1 && (S)w[c] <= sslack[(c1 >= 0 ? c1 : 0) * NC + c];
+            f2 = f2 && (S)w[c] <= sslack[(c2 >= 0 ? c2 : 0) * NC + c];
+          }
+          d = f1 ? c1 : (f2 ? c2 : -1);
+        } else if (MODE == kCut && kn == kFast) {
           const bool f1 = __any_sync(0xffffffffu, lane_fits(s, lane, c1, w));
           const bool f2 = __any_sync(0xffffffffu, lane_fits(s, lane, c2, w));
           d = f1 ? c1 : (f2 ? c2 : -1);
