@@ -64,9 +64,21 @@ __device__ void gain_body(Lanes L, const idx_t* __restrict__ xadj, const idx_t* 
         if (pw0[(int64_t)pv * ncon + c] > over_thr[(int64_t)pv * ncon + c]) over = true;
       if (!over) { mover[v] = 0; continue; }
     }
+    // Connection weight per neighbouring part, in first-appearance order:
+    // up to kRegParts parts accumulate in registers (compile-time slots, so
+    // no local memory) and are written out once; a vertex next to more parts
+    // runs the accumulation again in its global candidate slots.
+    constexpr int kRegParts = 8;
     uint32_t wf = 0;
     int cnt = 0;
-    bool boundary = false;
+    bool boundary = false, spill = false;
+    int32_t rp[kRegParts];
+    uint32_t rw[kRegParts];
+#pragma unroll
+    for (int i = 0; i < kRegParts; ++i) {
+      rp[i] = -1;
+      rw[i] = 0;
+    }
     for (int32_t j = s; j < e; ++j) {
       const int32_t pu = part[adj[j]];
       const uint32_t w = (uint32_t)(HAS_W ? adjwgt[j] : 1);
@@ -74,6 +86,42 @@ __device__ void gain_body(Lanes L, const idx_t* __restrict__ xadj, const idx_t* 
         wf += w;
       } else {
         boundary = true;
+        bool found = false;
+#pragma unroll
+        for (int i = 0; i < kRegParts; ++i)
+          if (rp[i] == pu) {
+            rw[i] += w;
+            found = true;
+          }
+        if (!found) {
+          if (cnt < kRegParts) {
+#pragma unroll
+            for (int i = 0; i < kRegParts; ++i)
+              if (i == cnt) {
+                rp[i] = pu;
+                rw[i] = w;
+              }
+            ++cnt;
+          } else {
+            spill = true;
+          }
+        }
+      }
+    }
+    if (!boundary) { mover[v] = 0; continue; }
+    if (!spill) {
+#pragma unroll
+      for (int i = 0; i < kRegParts; ++i)
+        if (i < cnt) {
+          cand_p[s + i] = rp[i];
+          cand_g[s + i] = (int32_t)rw[i];
+        }
+    } else {
+      cnt = 0;
+      for (int32_t j = s; j < e; ++j) {
+        const int32_t pu = part[adj[j]];
+        if (pu == pv) continue;
+        const uint32_t w = (uint32_t)(HAS_W ? adjwgt[j] : 1);
         int i = 0;
         for (; i < cnt; ++i)
           if (cand_p[s + i] == pu) break;
@@ -86,7 +134,6 @@ __device__ void gain_body(Lanes L, const idx_t* __restrict__ xadj, const idx_t* 
         }
       }
     }
-    if (!boundary) { mover[v] = 0; continue; }
     int ne = 0;
     for (int i = 0; i < cnt; ++i) {
       const int32_t wt = cand_g[s + i];
