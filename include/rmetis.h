@@ -99,12 +99,13 @@ RMETIS_API int RMETIS_GPU_SetStream(void *stream);
  * (lowest cut kept), matching rounds per level, whether a graph without
  * vertex weights gets summed coarse weights (1) or the reference's unit coarse
  * weights (0, default), whether ncuts > 1 attempts run concurrently on the
- * device's worker pool (1, default) or one after another (0), and the largest
+ * device's worker pool (1, default) or one after another (0), the largest
  * level (vertices) whose refinement runs in one single-block launch (default
- * 2048, 0 = never); the last two never change a result. Values < 0 leave a
- * knob unchanged. */
+ * 2048, 0 = never), and the largest level (vertices) from which all remaining
+ * coarsening levels run in one single-block launch (default 4096, 0 = never);
+ * the last three never change a result. Values < 0 leave a knob unchanged. */
 RMETIS_API int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weights,
-                                    int parallel_attempts, int fused_max_n);
+                                    int parallel_attempts, int fused_max_n, int tail_max_n);
 
 /* Many graphs in one call (no counterpart in the reference, which partitions
  * one graph per call). Host arrays of the concatenated batch: graph g has
@@ -139,7 +140,8 @@ RMETIS_API int RMETIS_GPU_WaitKway(int64_t ticket);
 
 /* Per-launch CUDA-event timing of the hot kernels (off by default).
  * RMETIS_GPU_GetProfile fills, per kernel id (0 gain, 1 decide, 2 propose,
- * 3 contract, 4 cut, 5 grow), launches[i], ms[i] (summed device time) and
+ * 3 contract, 4 cut, 5 grow, 6 single-block level refinement, 7 single-block
+ * coarse tail), launches[i], ms[i] (summed device time) and
  * bytes[i] (summed algorithmic bytes); returns the number of ids. With
  * max_ids above that number, launches[ids] receives the count of all kernel
  * launches made by this library in the process so far. */

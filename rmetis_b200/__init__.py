@@ -362,10 +362,10 @@ def part_graph_kway_trace(graph: Graph, nparts: int, tpwgts=None, ubvec=None, op
 
 
 def set_tuning(grow_trials: int = -1, match_rounds: int = -1, summed_unit_weights: int = -1,
-               parallel_attempts: int = -1, fused_max_n: int = -1):
+               parallel_attempts: int = -1, fused_max_n: int = -1, tail_max_n: int = -1):
     """Engine knobs without an options slot (-1 leaves a knob unchanged)."""
     _raise_for(_lib.load().RMETIS_GPU_SetTuning(grow_trials, match_rounds, summed_unit_weights, parallel_attempts,
-                                                fused_max_n), "set_tuning")
+                                                fused_max_n, tail_max_n), "set_tuning")
 
 
 def part_graph_kway_batch(graphs, nparts, ubvec=None, options: Options | None = None):

@@ -40,6 +40,7 @@ struct Tuning {
   int summed_unit_weights = 0;
   int parallel_attempts = 1;
   int fused_max_n = 2048;
+  int tail_max_n = 4096;
 };
 Tuning& tuning() {
   static Tuning t;
@@ -52,6 +53,7 @@ void apply_tuning(KwayOptions& o) {
   o.summed_unit_weights = tuning().summed_unit_weights;
   o.parallel_attempts = tuning().parallel_attempts;
   o.fused_max_n = tuning().fused_max_n;
+  o.tail_max_n = tuning().tail_max_n;
 }
 
 template <typename F>
@@ -253,12 +255,13 @@ int RMETIS_GPU_SetStream(void* stream) {
 }
 
 int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weights, int parallel_attempts,
-                         int fused_max_n) {
+                         int fused_max_n, int tail_max_n) {
   if (grow_trials >= 0) tuning().grow_trials = grow_trials > 0 ? grow_trials : 1;
   if (match_rounds >= 0) tuning().match_rounds = match_rounds > 0 ? match_rounds : 1;
   if (summed_unit_weights >= 0) tuning().summed_unit_weights = summed_unit_weights ? 1 : 0;
   if (parallel_attempts >= 0) tuning().parallel_attempts = parallel_attempts ? 1 : 0;
   if (fused_max_n >= 0) tuning().fused_max_n = fused_max_n;
+  if (tail_max_n >= 0) tuning().tail_max_n = tail_max_n;
   return METIS_OK;
 }
 

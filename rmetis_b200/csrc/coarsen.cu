@@ -40,11 +40,14 @@ struct EdgeKey {
   }
 };
 
+// The bodies below run over a lane set (common.cuh): every thread of a grid
+// kernel, or the threads of the one block of the fused coarse-tail kernel.
+// They take no __restrict__ because the fused kernel reads, within one launch,
+// arrays that it wrote in an earlier phase.
 template <bool HAS_W, int MODE>
-__global__ void k_match_propose(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
-                                const idx_t* __restrict__ adjwgt, int32_t n, const idx_t* __restrict__ match,
-                                idx_t* __restrict__ prop, uint64_t seed) {
-  RMB_GRID_STRIDE(v, n) {
+__device__ __forceinline__ void propose_body(const idx_t* xadj, const idx_t* adj, const idx_t* adjwgt, int32_t n,
+                                             const idx_t* match, idx_t* prop, uint64_t seed, Lanes L) {
+  RMB_FOR(v, n, L) {
     if (match[v] >= 0) continue;
     const int32_t s = xadj[v], e = xadj[v + 1];
     if (e - s > kHeavyDegree) continue;
@@ -60,14 +63,13 @@ __global__ void k_match_propose(const idx_t* __restrict__ xadj, const idx_t* __r
   }
 }
 
+// Rows of degree > kHeavyDegree, one warp each (W runs over warps).
 template <bool HAS_W, int MODE>
-__global__ void k_match_propose_heavy(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
-                                      const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ heavy,
-                                      int32_t nheavy, const idx_t* __restrict__ match, idx_t* __restrict__ prop,
-                                      uint64_t seed) {
+__device__ __forceinline__ void propose_heavy_body(const idx_t* xadj, const idx_t* adj, const idx_t* adjwgt,
+                                                   const idx_t* heavy, int32_t nheavy, const idx_t* match,
+                                                   idx_t* prop, uint64_t seed, Lanes W) {
   const int lane = threadIdx.x & 31;
-  const int32_t nw = gridDim.x * (blockDim.x >> 5);
-  for (int32_t i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < nheavy; i += nw) {
+  RMB_FOR(i, nheavy, W) {
     const int32_t v = heavy[i];
     if (match[v] >= 0) continue;  // warp-uniform
     EdgeKey best{INT32_MIN, 0u, -1};
@@ -91,14 +93,10 @@ __global__ void k_match_propose_heavy(const idx_t* __restrict__ xadj, const idx_
   }
 }
 
-__global__ void k_match_init(int32_t n, idx_t* match) {
-  RMB_GRID_STRIDE(v, n) { match[v] = -1; }
-}
-
 // Marks every vertex that received a proposal this round (stamp = round + 1).
-__global__ void k_match_stamp(int32_t n, const idx_t* __restrict__ match, const idx_t* __restrict__ prop,
-                              int32_t* __restrict__ stamp, int32_t round) {
-  RMB_GRID_STRIDE(v, n) {
+__device__ __forceinline__ void stamp_body(int32_t n, const idx_t* match, const idx_t* prop, int32_t* stamp,
+                                           int32_t round, Lanes L) {
+  RMB_FOR(v, n, L) {
     if (match[v] < 0) {
       const int32_t t = prop[v];
       if (t >= 0) stamp[t] = round + 1;
@@ -107,10 +105,10 @@ __global__ void k_match_stamp(int32_t n, const idx_t* __restrict__ match, const 
 }
 
 // Pure proposers compete for their target with their visit-order key.
-__global__ void k_match_compete(const idx_t* __restrict__ xadj, int32_t n, const idx_t* __restrict__ match,
-                                const idx_t* __restrict__ prop, const int32_t* __restrict__ stamp, int32_t round,
-                                unsigned long long* __restrict__ best, uint64_t vseed, int use_degree) {
-  RMB_GRID_STRIDE(v, n) {
+__device__ __forceinline__ void compete_body(const idx_t* xadj, int32_t n, const idx_t* match, const idx_t* prop,
+                                             const int32_t* stamp, int32_t round, unsigned long long* best,
+                                             uint64_t vseed, int use_degree, Lanes L) {
+  RMB_FOR(v, n, L) {
     if (match[v] >= 0) continue;
     const int32_t t = prop[v];
     if (t < 0 || stamp[v] == round + 1 || prop[t] == (int32_t)v) continue;
@@ -123,12 +121,13 @@ __global__ void k_match_compete(const idx_t* __restrict__ xadj, int32_t n, const
 }
 
 // Mutual pairs match; a target that is not in a mutual pair takes its winning
-// competitor. Only the target writes the pair, the winner (a pure proposer)
-// writes nothing this round.
-__global__ void k_match_resolve(int32_t n, const idx_t* __restrict__ prop, idx_t* __restrict__ match,
-                                unsigned long long* __restrict__ best, int32_t* __restrict__ newly) {
+// competitor. Only the target writes the pair, the winner (a pure proposer,
+// which nobody proposed to and so has no competitor) writes nothing this
+// round. Every thread of each warp must call it (warp sum of the count).
+__device__ __forceinline__ void resolve_body(int32_t n, const idx_t* prop, idx_t* match, unsigned long long* best,
+                                             int32_t* newly, Lanes L) {
   int32_t cnt = 0;
-  RMB_GRID_STRIDE(u, n) {
+  RMB_FOR(u, n, L) {
     if (match[u] >= 0) continue;
     const int32_t t = prop[u];
     const unsigned long long b = best[u];
@@ -147,10 +146,10 @@ __global__ void k_match_resolve(int32_t n, const idx_t* __restrict__ prop, idx_t
   if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(newly, cnt);
 }
 
-__global__ void k_match_accept(int32_t n, const idx_t* __restrict__ prop, idx_t* __restrict__ match,
-                               int32_t* __restrict__ newly) {
+// Finishing rounds: mutual proposals only.
+__device__ __forceinline__ void accept_body(int32_t n, const idx_t* prop, idx_t* match, int32_t* newly, Lanes L) {
   int32_t cnt = 0;
-  RMB_GRID_STRIDE(v, n) {
+  RMB_FOR(v, n, L) {
     if (match[v] < 0) {
       const int32_t u = prop[v];
       if (u >= 0 && prop[u] == (int32_t)v) {
@@ -161,6 +160,46 @@ __global__ void k_match_accept(int32_t n, const idx_t* __restrict__ prop, idx_t*
   }
   cnt = warp_sum(cnt);
   if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(newly, cnt);
+}
+
+template <bool HAS_W, int MODE>
+__global__ void k_match_propose(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                                const idx_t* __restrict__ adjwgt, int32_t n, const idx_t* __restrict__ match,
+                                idx_t* __restrict__ prop, uint64_t seed) {
+  propose_body<HAS_W, MODE>(xadj, adj, adjwgt, n, match, prop, seed, grid_lanes());
+}
+
+template <bool HAS_W, int MODE>
+__global__ void k_match_propose_heavy(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                                      const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ heavy,
+                                      int32_t nheavy, const idx_t* __restrict__ match, idx_t* __restrict__ prop,
+                                      uint64_t seed) {
+  propose_heavy_body<HAS_W, MODE>(xadj, adj, adjwgt, heavy, nheavy, match, prop, seed, grid_warps());
+}
+
+__global__ void k_match_init(int32_t n, idx_t* match) {
+  RMB_GRID_STRIDE(v, n) { match[v] = -1; }
+}
+
+__global__ void k_match_stamp(int32_t n, const idx_t* __restrict__ match, const idx_t* __restrict__ prop,
+                              int32_t* __restrict__ stamp, int32_t round) {
+  stamp_body(n, match, prop, stamp, round, grid_lanes());
+}
+
+__global__ void k_match_compete(const idx_t* __restrict__ xadj, int32_t n, const idx_t* __restrict__ match,
+                                const idx_t* __restrict__ prop, const int32_t* __restrict__ stamp, int32_t round,
+                                unsigned long long* __restrict__ best, uint64_t vseed, int use_degree) {
+  compete_body(xadj, n, match, prop, stamp, round, best, vseed, use_degree, grid_lanes());
+}
+
+__global__ void k_match_resolve(int32_t n, const idx_t* __restrict__ prop, idx_t* __restrict__ match,
+                                unsigned long long* __restrict__ best, int32_t* __restrict__ newly) {
+  resolve_body(n, prop, match, best, newly, grid_lanes());
+}
+
+__global__ void k_match_accept(int32_t n, const idx_t* __restrict__ prop, idx_t* __restrict__ match,
+                               int32_t* __restrict__ newly) {
+  accept_body(n, prop, match, newly, grid_lanes());
 }
 
 __global__ void k_match_finalize(int32_t n, idx_t* match) {
@@ -240,10 +279,9 @@ struct LoadLeader {
 
 // cmap numbering identical to the reference's ascending scan (mod.rs:286-297):
 // the coarse id of a pair is the number of leaders (min endpoint) before it.
-__global__ void k_build_cmap(const idx_t* __restrict__ xadj, int32_t n, const idx_t* __restrict__ match,
-                             const idx_t* __restrict__ cidx, idx_t* __restrict__ cmap, idx_t* __restrict__ mem0,
-                             idx_t* __restrict__ mem1, idx_t* __restrict__ ub) {
-  RMB_GRID_STRIDE(v, n) {
+__device__ __forceinline__ void build_cmap_body(const idx_t* xadj, int32_t n, const idx_t* match, const idx_t* cidx,
+                                                idx_t* cmap, idx_t* mem0, idx_t* mem1, idx_t* ub, Lanes L) {
+  RMB_FOR(v, n, L) {
     const int32_t m = match[v];
     if (m >= (int32_t)v) {
       const int32_t c = cidx[v];
@@ -258,10 +296,9 @@ __global__ void k_build_cmap(const idx_t* __restrict__ xadj, int32_t n, const id
   }
 }
 
-__global__ void k_coarse_vwgt(int32_t cn, int32_t ncon, const idx_t* __restrict__ mem0,
-                              const idx_t* __restrict__ mem1, const idx_t* __restrict__ vwgt,
-                              idx_t* __restrict__ cvwgt) {
-  RMB_GRID_STRIDE(i, (int64_t)cn * ncon) {
+__device__ __forceinline__ void coarse_vwgt_body(int32_t cn, int32_t ncon, const idx_t* mem0, const idx_t* mem1,
+                                                 const idx_t* vwgt, idx_t* cvwgt, Lanes L) {
+  RMB_FOR(i, (int64_t)cn * ncon, L) {
     const int64_t c = i / ncon;
     const int cc = (int)(i - c * ncon);
     const int32_t a = mem0[c], b = mem1[c];
@@ -274,15 +311,15 @@ __global__ void k_coarse_vwgt(int32_t cn, int32_t ncon, const idx_t* __restrict_
 // Merge of one coarse row in registers (bound <= kContractThreadMax). The
 // row of the first member is scanned before the second, each in CSR order,
 // and a neighbour is appended at its first appearance (mod.rs:323-341).
+// Longer rows are listed in hlist for the warp merge.
 template <bool HAS_W>
-__global__ void k_contract_thread(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
-                                  const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ cmap, int32_t cn,
-                                  const idx_t* __restrict__ mem0, const idx_t* __restrict__ mem1,
-                                  const idx_t* __restrict__ ub, const idx_t* __restrict__ ub_off,
-                                  idx_t* __restrict__ tmp_adj, idx_t* __restrict__ tmp_w, idx_t* __restrict__ cdeg,
-                                  idx_t* __restrict__ hlist, int32_t* __restrict__ hcount) {
+__device__ __forceinline__ void contract_thread_body(const idx_t* xadj, const idx_t* adj, const idx_t* adjwgt,
+                                                     const idx_t* cmap, int32_t cn, const idx_t* mem0,
+                                                     const idx_t* mem1, const idx_t* ub, const idx_t* ub_off,
+                                                     idx_t* tmp_adj, idx_t* tmp_w, idx_t* cdeg, idx_t* hlist,
+                                                     int32_t* hcount, Lanes L) {
   constexpr int T = kContractThreadMax;
-  RMB_GRID_STRIDE(c, cn) {
+  RMB_FOR(c, cn, L) {
     if (ub[c] > T) {
       hlist[atomicAdd(hcount, 1)] = (idx_t)c;
       continue;
@@ -327,36 +364,29 @@ __global__ void k_contract_thread(const idx_t* __restrict__ xadj, const idx_t* _
 constexpr int kWarpTable = 1024;  // shared hash slots per warp
 
 // Merge of a long coarse row by one warp, 32 entries at a time, with an
-// open-addressing table (shared memory, or global scratch for long rows).
-// New keys of a chunk get slots in lane order, which keeps first-appearance
-// order; each key's weights are summed by the lowest lane holding it.
+// open-addressing table (this warp's shared table when it is given and the
+// row fits, else global scratch at twice the row's scratch offset). New keys
+// of a chunk get slots in lane order, which keeps first-appearance order; each
+// key's weights are summed by the lowest lane holding it. lanew: 32 shared
+// ints of this warp. W runs over warps.
 template <bool HAS_W>
-__global__ void k_contract_warp(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
-                                const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ cmap,
-                                const idx_t* __restrict__ mem0, const idx_t* __restrict__ mem1,
-                                const idx_t* __restrict__ ub, const idx_t* __restrict__ ub_off,
-                                const idx_t* __restrict__ hlist, const int32_t* __restrict__ hcount,
-                                idx_t* __restrict__ tmp_adj, idx_t* __restrict__ tmp_w, idx_t* __restrict__ cdeg,
-                                int32_t* __restrict__ gkey, int32_t* __restrict__ gslot) {
-  __shared__ int32_t skey_all[4][kWarpTable];
-  __shared__ int32_t sslot_all[4][kWarpTable];
-  __shared__ int32_t lanew_all[4][32];
-  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int32_t* lanew = lanew_all[wib];
-  const int32_t nh = *hcount;
-  const int32_t nw = gridDim.x * (blockDim.x >> 5);
-  for (int32_t hi = blockIdx.x * (blockDim.x >> 5) + wib; hi < nh; hi += nw) {
+__device__ __forceinline__ void contract_warp_body(const idx_t* xadj, const idx_t* adj, const idx_t* adjwgt,
+                                                   const idx_t* cmap, const idx_t* mem0, const idx_t* mem1,
+                                                   const idx_t* ub, const idx_t* ub_off, const idx_t* hlist,
+                                                   int32_t nh, idx_t* tmp_adj, idx_t* tmp_w, idx_t* cdeg,
+                                                   int32_t* gkey, int32_t* gslot, int32_t* skey, int32_t* sslot,
+                                                   int32_t* lanew, Lanes W) {
+  const int lane = threadIdx.x & 31;
+  RMB_FOR(hi, nh, W) {
     const int32_t c = hlist[hi];
     const int32_t ubc = ub[c];
     const int32_t off = ub_off[c];
-    int32_t tsize;
+    const int32_t tsize = 2 * ubc;
     int32_t *tkey, *tslot;
-    if (2 * ubc <= kWarpTable) {
-      tsize = 2 * ubc;
-      tkey = skey_all[wib];
-      tslot = sslot_all[wib];
+    if (skey && tsize <= kWarpTable) {
+      tkey = skey;
+      tslot = sslot;
     } else {
-      tsize = 2 * ubc;
       tkey = gkey + 2 * (int64_t)off;
       tslot = gslot + 2 * (int64_t)off;
     }
@@ -418,18 +448,15 @@ __global__ void k_contract_warp(const idx_t* __restrict__ xadj, const idx_t* __r
   }
 }
 
-// Gather the merged rows into the final coarse CSR (one warp per 32 coarse
-// vertices, striding over their contiguous scratch range).
-__global__ void k_contract_compact(int32_t cn, const idx_t* __restrict__ ub_off, const idx_t* __restrict__ cdeg,
-                                   const idx_t* __restrict__ cxadj, const idx_t* __restrict__ tmp_adj,
-                                   const idx_t* __restrict__ tmp_w, idx_t* __restrict__ cadj,
-                                   idx_t* __restrict__ cw) {
-  __shared__ int32_t xs_all[8][33];
-  int32_t* xs = xs_all[threadIdx.x >> 5];
+// Gather the merged rows into the final coarse CSR: a warp takes 32 coarse
+// vertices and strides over their contiguous scratch range. xs: 33 shared
+// ints of this warp. W runs over warps.
+__device__ __forceinline__ void compact_body(int32_t cn, const idx_t* ub_off, const idx_t* cdeg, const idx_t* cxadj,
+                                             const idx_t* tmp_adj, const idx_t* tmp_w, idx_t* cadj, idx_t* cw,
+                                             int32_t* xs, Lanes W) {
   const int lane = threadIdx.x & 31;
-  const int32_t nw = gridDim.x * (blockDim.x >> 5);
-  for (int32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); (int64_t)w * 32 < cn; w += nw) {
-    const int32_t v0 = w * 32;
+  RMB_FOR(w, ceil_div(cn, 32), W) {
+    const int32_t v0 = (int32_t)w * 32;
     const int32_t vend = min(v0 + 32, cn);
     const int cnt = vend - v0;
     if (lane < cnt) xs[lane] = ub_off[v0 + lane];
@@ -452,6 +479,53 @@ __global__ void k_contract_compact(int32_t cn, const idx_t* __restrict__ ub_off,
     }
     __syncwarp();
   }
+}
+
+__global__ void k_build_cmap(const idx_t* __restrict__ xadj, int32_t n, const idx_t* __restrict__ match,
+                             const idx_t* __restrict__ cidx, idx_t* __restrict__ cmap, idx_t* __restrict__ mem0,
+                             idx_t* __restrict__ mem1, idx_t* __restrict__ ub) {
+  build_cmap_body(xadj, n, match, cidx, cmap, mem0, mem1, ub, grid_lanes());
+}
+
+__global__ void k_coarse_vwgt(int32_t cn, int32_t ncon, const idx_t* __restrict__ mem0,
+                              const idx_t* __restrict__ mem1, const idx_t* __restrict__ vwgt,
+                              idx_t* __restrict__ cvwgt) {
+  coarse_vwgt_body(cn, ncon, mem0, mem1, vwgt, cvwgt, grid_lanes());
+}
+
+template <bool HAS_W>
+__global__ void k_contract_thread(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                                  const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ cmap, int32_t cn,
+                                  const idx_t* __restrict__ mem0, const idx_t* __restrict__ mem1,
+                                  const idx_t* __restrict__ ub, const idx_t* __restrict__ ub_off,
+                                  idx_t* __restrict__ tmp_adj, idx_t* __restrict__ tmp_w, idx_t* __restrict__ cdeg,
+                                  idx_t* __restrict__ hlist, int32_t* __restrict__ hcount) {
+  contract_thread_body<HAS_W>(xadj, adj, adjwgt, cmap, cn, mem0, mem1, ub, ub_off, tmp_adj, tmp_w, cdeg, hlist,
+                              hcount, grid_lanes());
+}
+
+template <bool HAS_W>
+__global__ void k_contract_warp(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                                const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ cmap,
+                                const idx_t* __restrict__ mem0, const idx_t* __restrict__ mem1,
+                                const idx_t* __restrict__ ub, const idx_t* __restrict__ ub_off,
+                                const idx_t* __restrict__ hlist, const int32_t* __restrict__ hcount,
+                                idx_t* __restrict__ tmp_adj, idx_t* __restrict__ tmp_w, idx_t* __restrict__ cdeg,
+                                int32_t* __restrict__ gkey, int32_t* __restrict__ gslot) {
+  __shared__ int32_t skey_all[4][kWarpTable];
+  __shared__ int32_t sslot_all[4][kWarpTable];
+  __shared__ int32_t lanew_all[4][32];
+  const int wib = threadIdx.x >> 5;
+  contract_warp_body<HAS_W>(xadj, adj, adjwgt, cmap, mem0, mem1, ub, ub_off, hlist, *hcount, tmp_adj, tmp_w, cdeg,
+                            gkey, gslot, skey_all[wib], sslot_all[wib], lanew_all[wib], grid_warps());
+}
+
+__global__ void k_contract_compact(int32_t cn, const idx_t* __restrict__ ub_off, const idx_t* __restrict__ cdeg,
+                                   const idx_t* __restrict__ cxadj, const idx_t* __restrict__ tmp_adj,
+                                   const idx_t* __restrict__ tmp_w, idx_t* __restrict__ cadj,
+                                   idx_t* __restrict__ cw) {
+  __shared__ int32_t xs_all[8][33];
+  compact_body(cn, ub_off, cdeg, cxadj, tmp_adj, tmp_w, cadj, cw, xs_all[threadIdx.x >> 5], grid_warps());
 }
 
 struct LoadHeavy {
@@ -558,6 +632,295 @@ CoarseResult contract(const DGraph& g, const idx_t* match, int coarse_vwgt, Aren
   r.g.adjwgt = cw;
   r.g.vwgt = cvwgt;
   return r;
+}
+
+// ---------------------------------------------------------------------------
+// Coarse tail: every remaining coarsening level of a small graph in one
+// single-block launch. The level loop of the host (heavy list, matching
+// rounds with their progress checks, contraction, the stop rule of
+// coarsen/mod.rs:43-66) runs inside the block with the same bodies as the
+// grid kernels above, so it yields exactly the levels the host loop would;
+// the host reads the level table back once instead of about six scalars per
+// level. Small levels stay in the SM's L1, and the block needs no launch or
+// host round trip between phases.
+// ---------------------------------------------------------------------------
+constexpr int kTailThreads = 1024;
+
+struct TailArgs {
+  DGraph g;
+  int has_vw, summed_unit, mode, lvl0, k, rounds;
+  uint64_t seed64;
+  long long limit;
+  char* ws;
+  long long ws_bytes;
+};
+
+__device__ __forceinline__ long long tail_round(long long b) { return (b + 255) & ~255LL; }
+
+__global__ void __launch_bounds__(kTailThreads, 1) k_coarsen_tail(TailArgs a) {
+  __shared__ idx_t sw[32];
+  __shared__ int32_t lanew_all[kTailThreads / 32][32];
+  __shared__ int32_t xs_all[kTailThreads / 32][33];
+  const Lanes L = block_lanes(), W = block_warps();
+  const int wib = threadIdx.x >> 5;
+  TailOut* out = reinterpret_cast<TailOut*>(a.ws);
+  if ((a.ws_bytes & 255) != 0) {  // offsets from the top would lose their alignment: leave it to the host loop
+    if (threadIdx.x == 0) {
+      out->levels = 0;
+      out->ncoarse = 0;
+      out->finished = 0;
+    }
+    return;
+  }
+  // Level data is taken from the bottom of the workspace and kept; the
+  // scratch of one level is taken from the top and dropped after it. Every
+  // thread computes the same offsets from block-uniform sizes.
+  long long lo = tail_round(sizeof(TailOut));
+  DGraph cur = a.g;
+  int has_vw = a.has_vw;
+  int nh_lv = 0, nc = 0, finished = 0;
+  for (int lvl = a.lvl0; nh_lv < kTailMaxLevels - 1; ++lvl) {
+    const int32_t n = cur.n;
+    const bool w = cur.adjwgt != nullptr;
+    const long long lvl_lo = lo;
+    long long hi = a.ws_bytes;
+    auto take_lo = [&](long long b) {
+      const long long o = lo;
+      lo += tail_round(b);
+      return a.ws + o;
+    };
+    auto take_hi = [&](long long b) {
+      hi -= tail_round(b);
+      return a.ws + hi;
+    };
+    idx_t* hl = (idx_t*)take_lo(4LL * n);
+    idx_t* match = (idx_t*)take_lo(4LL * n);
+    idx_t* prop = (idx_t*)take_hi(4LL * n);
+    int32_t* stamp = (int32_t*)take_hi(4LL * n);
+    unsigned long long* best = (unsigned long long*)take_hi(8LL * n);
+    idx_t* cidx = (idx_t*)take_hi(4LL * n);
+    int32_t* newly = (int32_t*)take_hi(4LL * (a.rounds + 1));
+    idx_t* cnt = (idx_t*)take_hi(64);  // [0] heavy rows, [1] cn, [2] long coarse rows
+    if (lo > hi) {
+      lo = lvl_lo;
+      break;
+    }
+    // ---- heavy list and matching (match_parallel) ----
+    block_scan_n<idx_t>(LoadHeavy{cur.xadj}, StoreHeavy{cur.xadj, hl}, n, cnt, sw);
+    RMB_FOR(v, n, L) {
+      match[v] = -1;
+      stamp[v] = 0;
+      best[v] = 0;
+    }
+    RMB_FOR(i, a.rounds + 1, L) newly[i] = 0;
+    if (threadIdx.x == 0) cnt[2] = 0;
+    __syncthreads();
+    const int32_t nheavy = cnt[0];
+    const uint64_t lseed = mix64(a.seed64 * 0x100000001b3ULL + (uint64_t)lvl + 1);
+    const uint64_t vseed = mix64(lseed ^ 0x7669736974ULL);
+    bool handshake = true;
+    int phase_start = 0;
+    for (int r = 0; r < a.rounds; ++r) {
+      if (handshake && a.mode == 1) {
+        if (w) {
+          propose_body<true, 1>(cur.xadj, cur.adjncy, cur.adjwgt, n, match, prop, lseed, L);
+          propose_heavy_body<true, 1>(cur.xadj, cur.adjncy, cur.adjwgt, hl, nheavy, match, prop, lseed, W);
+        } else {
+          propose_body<false, 1>(cur.xadj, cur.adjncy, cur.adjwgt, n, match, prop, lseed, L);
+          propose_heavy_body<false, 1>(cur.xadj, cur.adjncy, cur.adjwgt, hl, nheavy, match, prop, lseed, W);
+        }
+      } else {
+        propose_body<false, 0>(cur.xadj, cur.adjncy, cur.adjwgt, n, match, prop, lseed, L);
+        propose_heavy_body<false, 0>(cur.xadj, cur.adjncy, cur.adjwgt, hl, nheavy, match, prop, lseed, W);
+      }
+      __syncthreads();
+      if (handshake) {
+        stamp_body(n, match, prop, stamp, r, L);
+        __syncthreads();
+        compete_body(cur.xadj, n, match, prop, stamp, r, best, vseed, a.mode == 1 ? 1 : 0, L);
+        __syncthreads();
+        resolve_body(n, prop, match, best, newly + r, L);
+      } else {
+        accept_body(n, prop, match, newly + r, L);
+      }
+      __syncthreads();
+      if (r - phase_start >= 1 && ((r - phase_start) & 1) == 1) {
+        const int64_t last2 = (int64_t)newly[r - 1] + newly[r];
+        if (last2 * 1000 < (int64_t)n) {
+          if (!handshake) break;
+          handshake = false;
+          phase_start = r + 1;
+        }
+      }
+    }
+    RMB_FOR(v, n, L) {
+      if (match[v] < 0) match[v] = (idx_t)v;
+    }
+    __syncthreads();
+    // ---- contraction (contract) ----
+    block_scan_n<idx_t>(LoadLeader{match}, StoreArr<idx_t>{cidx}, n, cnt + 1, sw);
+    __syncthreads();
+    const int32_t cn = cnt[1];
+    const int coarse_vw = (has_vw || a.summed_unit) ? 1 : 0;
+    const long long coarse_lo = lo;
+    idx_t* cmap = (idx_t*)take_lo(4LL * n);
+    idx_t* cxadj = (idx_t*)take_lo(4LL * (cn + 1));
+    idx_t* cvwgt = coarse_vw ? (idx_t*)take_lo(4LL * cn * cur.ncon) : nullptr;
+    idx_t* mem0 = (idx_t*)take_hi(4LL * cn);
+    idx_t* mem1 = (idx_t*)take_hi(4LL * cn);
+    idx_t* ub = (idx_t*)take_hi(4LL * cn);
+    idx_t* ub_off = (idx_t*)take_hi(4LL * (cn + 1));
+    idx_t* cdeg = (idx_t*)take_hi(4LL * cn);
+    idx_t* hlist = (idx_t*)take_hi(4LL * cn);
+    if (lo > hi) {
+      lo = lvl_lo;
+      break;
+    }
+    build_cmap_body(cur.xadj, n, match, cidx, cmap, mem0, mem1, ub, L);
+    __syncthreads();
+    block_scan_n<idx_t>(LoadArr<idx_t>{ub}, StoreArr<idx_t>{ub_off}, cn, ub_off + cn, sw);
+    __syncthreads();
+    const int32_t mb = ub_off[cn];
+    idx_t* tmp_adj = (idx_t*)take_hi(4LL * mb + 4);
+    idx_t* tmp_w = (idx_t*)take_hi(4LL * mb + 4);
+    int32_t* gkey = (int32_t*)take_hi(8LL * mb + 8);
+    int32_t* gslot = (int32_t*)take_hi(8LL * mb + 8);
+    if (lo > hi) {
+      lo = lvl_lo;
+      break;
+    }
+    if (w)
+      contract_thread_body<true>(cur.xadj, cur.adjncy, cur.adjwgt, cmap, cn, mem0, mem1, ub, ub_off, tmp_adj, tmp_w,
+                                 cdeg, hlist, cnt + 2, L);
+    else
+      contract_thread_body<false>(cur.xadj, cur.adjncy, cur.adjwgt, cmap, cn, mem0, mem1, ub, ub_off, tmp_adj,
+                                  tmp_w, cdeg, hlist, cnt + 2, L);
+    __syncthreads();
+    const int32_t nlong = cnt[2];
+    if (w)
+      contract_warp_body<true>(cur.xadj, cur.adjncy, cur.adjwgt, cmap, mem0, mem1, ub, ub_off, hlist, nlong, tmp_adj,
+                               tmp_w, cdeg, gkey, gslot, nullptr, nullptr, lanew_all[wib], W);
+    else
+      contract_warp_body<false>(cur.xadj, cur.adjncy, cur.adjwgt, cmap, mem0, mem1, ub, ub_off, hlist, nlong, tmp_adj,
+                                tmp_w, cdeg, gkey, gslot, nullptr, nullptr, lanew_all[wib], W);
+    __syncthreads();
+    block_scan_n<idx_t>(LoadArr<idx_t>{cdeg}, StoreArr<idx_t>{cxadj}, cn, cxadj + cn, sw);
+    __syncthreads();
+    const int32_t cm = cxadj[cn];
+    idx_t* cadj = (idx_t*)take_lo(4LL * cm);
+    idx_t* cw = (idx_t*)take_lo(4LL * cm);
+    if (lo > hi) {
+      lo = lvl_lo;
+      break;
+    }
+    compact_body(cn, ub_off, cdeg, cxadj, tmp_adj, tmp_w, cadj, cw, xs_all[wib], W);
+    if (coarse_vw) coarse_vwgt_body(cn, cur.ncon, mem0, mem1, cur.vwgt, cvwgt, L);
+    __syncthreads();
+    // ---- the level is complete: record it and apply the stop rule ----
+    if (threadIdx.x == 0) {
+      out->heavy[nh_lv] = (long long)hl;
+      out->nheavy[nh_lv] = nheavy;
+      out->match[nh_lv] = (long long)match;
+    }
+    ++nh_lv;
+    if (cn < a.k) {  // too few vertices to seed k parts: keep the finer level
+      lo = coarse_lo;
+      finished = 1;
+      break;
+    }
+    if (threadIdx.x == 0) {
+      out->cmap[nc] = (long long)cmap;
+      out->xadj[nc] = (long long)cxadj;
+      out->adj[nc] = (long long)cadj;
+      out->adjw[nc] = (long long)cw;
+      out->vwgt[nc] = (long long)cvwgt;
+      out->cn[nc] = cn;
+      out->cm[nc] = cm;
+      out->coarse_vw[nc] = coarse_vw;
+    }
+    ++nc;
+    const float ratio = (float)cn / (float)n;
+    cur.n = cn;
+    cur.m = cm;
+    cur.xadj = cxadj;
+    cur.adjncy = cadj;
+    cur.adjwgt = cw;
+    cur.vwgt = cvwgt;
+    has_vw = coarse_vw;
+    if ((long long)cn <= a.limit || ratio > 0.95f) {
+      finished = 1;
+      // heavy list of the coarsest level (its refinement reads it)
+      idx_t* hl2 = (idx_t*)take_lo(4LL * cn);
+      idx_t* c2 = (idx_t*)(a.ws + a.ws_bytes - 256);
+      if (lo <= a.ws_bytes - 256) {
+        block_scan_n<idx_t>(LoadHeavy{cur.xadj}, StoreHeavy{cur.xadj, hl2}, cn, c2, sw);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          out->heavy[nh_lv] = (long long)hl2;
+          out->nheavy[nh_lv] = c2[0];
+          out->match[nh_lv] = 0;
+        }
+        ++nh_lv;
+      }
+      break;
+    }
+    __syncthreads();  // the next level reuses this level's scratch
+  }
+  if (threadIdx.x == 0) {
+    out->levels = nh_lv;
+    out->ncoarse = nc;
+    out->finished = finished;
+  }
+}
+
+int64_t tail_workspace_bytes(const DGraph& g, int rounds) {
+  const int64_t n = g.n, m = g.m, ncon = g.ncon;
+  // kept data of all levels (geometric shrinking, with margin) + one
+  // level's scratch + allocation rounding
+  const int64_t b = (int64_t)sizeof(TailOut) + 3 * (20 * n + 4 * n * ncon + 8 * m) + (44 * n + 24 * m) +
+                    4 * (rounds + 1) + (int64_t)kTailMaxLevels * 16 * 256 + 4096;
+  return (b + 255) & ~(int64_t)255;  // scratch is taken from the top: keep every offset 256-aligned
+}
+
+void coarsen_tail(const DGraph& g, int has_vw, int summed_unit, int mode, uint64_t seed64, int lvl0, int k,
+                  int64_t limit, int rounds, Arena& arena, cudaStream_t st, TailOut* h_out) {
+  const int64_t bytes = tail_workspace_bytes(g, rounds);
+  char* ws = arena.alloc<char>((size_t)bytes);
+  TailArgs a;
+  a.g = g;
+  a.has_vw = has_vw;
+  a.summed_unit = summed_unit;
+  a.mode = mode;
+  a.lvl0 = lvl0;
+  a.k = k;
+  a.rounds = rounds;
+  a.seed64 = seed64;
+  a.limit = (long long)limit;
+  a.ws = ws;
+  a.ws_bytes = (long long)bytes;
+  const int ph = profiler().begin(kProfTail, st);
+  k_coarsen_tail<<<1, kTailThreads, 0, st>>>(a);
+  RMB_LAUNCH_CHECK();
+  profiler().end(ph, st, 0.0);
+  RMB_CUDA(cudaMemcpyAsync(h_out, ws, sizeof(TailOut), cudaMemcpyDeviceToHost, st));
+  RMB_CUDA(cudaStreamSynchronize(st));
+  if (ph >= 0) {
+    // algorithmic bytes as the grid kernels count them: matching round 0 and
+    // the contraction of every matched level
+    double bytes = 0.0;
+    int64_t n = g.n, m = g.m;
+    bool w = g.adjwgt != nullptr;
+    for (int j = 0; j < h_out->levels && h_out->match[j]; ++j) {
+      const int64_t cn = j < h_out->ncoarse ? h_out->cn[j] : n;
+      bytes += 12.0 * n + (w && mode == 1 ? 12.0 : 8.0) * m + 20.0 * cn + 8.0 * n + (w ? 20.0 : 16.0) * m;
+      if (j < h_out->ncoarse) {
+        n = h_out->cn[j];
+        m = h_out->cm[j];
+        w = true;
+      }
+    }
+    profiler().set_bytes(ph, bytes);
+  }
 }
 
 }  // namespace rmb

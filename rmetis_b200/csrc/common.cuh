@@ -59,6 +59,11 @@ __device__ inline Lanes grid_lanes() {
   return {(int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x};
 }
 __device__ inline Lanes block_lanes() { return {(int64_t)threadIdx.x, (int64_t)blockDim.x}; }
+// The same over warps (a body that gives each item to one warp).
+__device__ inline Lanes grid_warps() {
+  return {(int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), (int64_t)gridDim.x * (blockDim.x >> 5)};
+}
+__device__ inline Lanes block_warps() { return {(int64_t)(threadIdx.x >> 5), (int64_t)(blockDim.x >> 5)}; }
 #define RMB_FOR(i, n, L) for (int64_t i = (L).first; i < (int64_t)(n); i += (L).stride)
 
 #define RMB_GRID_STRIDE(i, n) \

@@ -105,6 +105,7 @@ Engine::Engine(bool is_worker) : is_worker_(is_worker) {
   RMB_CUDA(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
   stream_ = own_stream_;
   RMB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_scratch_), 4096));
+  RMB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_tail_), sizeof(TailOut)));
 }
 
 Engine::~Engine() {
@@ -112,6 +113,7 @@ Engine::~Engine() {
   arena_.release();
   if (h_thr_) cudaFreeHost(h_thr_);
   if (h_scratch_) cudaFreeHost(h_scratch_);
+  if (h_tail_) cudaFreeHost(h_tail_);
   if (own_stream_) cudaStreamDestroy(own_stream_);
 }
 
@@ -251,7 +253,47 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
     std::vector<idx_t*> heavy_lists;
     std::vector<int32_t> heavy_counts;
     std::vector<bool> has_vw{g0.vwgt != nullptr};
+    bool tail_open = o.tail_max_n > 0;
     for (int lvl = 0;; ++lvl) {
+      if (tail_open && levels.back().n <= o.tail_max_n && levels.back().m <= 64LL * o.tail_max_n) {
+        // The remaining levels in one launch; a tail that ran out of room
+        // hands back to this loop at the level after the last one it kept.
+        tail_open = false;
+        const DGraph from = levels.back();
+        const size_t base = levels.size() - 1;
+        coarsen_tail(from, has_vw.back() ? 1 : 0, o.summed_unit_weights, o.ctype == 0 ? 0 : 1, seed64, lvl, k,
+                     (int64_t)limit, o.match_rounds, arena_, st, h_tail_);
+        const TailOut& t = *h_tail_;
+        for (int j = 0; j < t.ncoarse; ++j) {
+          DGraph c;
+          c.n = t.cn[j];
+          c.m = t.cm[j];
+          c.ncon = from.ncon;
+          c.xadj = reinterpret_cast<const idx_t*>(t.xadj[j]);
+          c.adjncy = reinterpret_cast<const idx_t*>(t.adj[j]);
+          c.adjwgt = reinterpret_cast<const idx_t*>(t.adjw[j]);
+          c.vwgt = t.coarse_vw[j] ? reinterpret_cast<const idx_t*>(t.vwgt[j]) : nullptr;
+          levels.push_back(c);
+          cmaps.push_back(reinterpret_cast<idx_t*>(t.cmap[j]));
+          has_vw.push_back(t.coarse_vw[j] != 0);
+        }
+        for (int j = 0; j < t.levels; ++j) {
+          heavy_lists.push_back(reinterpret_cast<idx_t*>(t.heavy[j]));
+          heavy_counts.push_back(t.nheavy[j]);
+          if (trace && t.match[j]) {
+            std::vector<int32_t> hm(levels[base + j].n);
+            RMB_CUDA(cudaMemcpyAsync(hm.data(), reinterpret_cast<const void*>(t.match[j]), sizeof(int32_t) * hm.size(),
+                                     cudaMemcpyDeviceToHost, st));
+            RMB_CUDA(cudaStreamSynchronize(st));
+            local.matchings.push_back(std::move(hm));
+          }
+        }
+        if (t.finished) break;
+        if (t.ncoarse > 0) {
+          lvl += t.ncoarse - 1;
+          continue;
+        }
+      }
       const DGraph& cur = levels.back();
       idx_t* hl = arena_.alloc<idx_t>((size_t)cur.n);
       const int32_t nh = heavy_list(cur, hl, arena_, st, h_scratch_);

@@ -33,6 +33,7 @@ struct KwayOptions {
   int summed_unit_weights = 0;  // 1: a graph without vwgt gets summed coarse weights
   int parallel_attempts = 1;    // 1: ncuts > 1 attempts run concurrently on the worker pool
   int fused_max_n = 2048;       // levels up to this size refine in one single-block launch
+  int tail_max_n = 4096;        // from a level of at most this size, coarsening runs in one launch
 };
 
 // Per-kernel-family device time, measured with CUDA events on the engine's
@@ -96,6 +97,7 @@ class Engine {
   cudaStream_t own_stream_ = nullptr;
   cudaStream_t stream_ = nullptr;
   int32_t* h_scratch_ = nullptr;   // pinned
+  TailOut* h_tail_ = nullptr;      // pinned level table of the coarse-tail kernel
   long long* h_thr_ = nullptr;     // pinned staging for thresholds
   size_t h_thr_cap_ = 0;
   bool profiling_ = false;

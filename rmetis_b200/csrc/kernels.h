@@ -88,6 +88,35 @@ CoarseResult contract(const DGraph& g, const idx_t* match, int coarse_vwgt, Aren
 // Degree > kHeavyDegree vertex list of a level (ascending ids).
 int32_t heavy_list(const DGraph& g, idx_t* out, Arena& arena, cudaStream_t st, int32_t* h_scratch);
 
+// The level table written by the coarse-tail kernel: heavy lists (and the
+// matching, null for a level that was not matched) of the levels it started
+// from, in order, and the coarse levels it kept. finished = 1 when the stop
+// rule ended coarsening; 0 when the workspace or the table ran out and the
+// host loop goes on from the last kept level.
+constexpr int kTailMaxLevels = 32;
+struct TailOut {
+  int32_t levels, ncoarse, finished, pad;
+  long long heavy[kTailMaxLevels];
+  int32_t nheavy[kTailMaxLevels];
+  long long match[kTailMaxLevels];
+  long long cmap[kTailMaxLevels], xadj[kTailMaxLevels], adj[kTailMaxLevels], adjw[kTailMaxLevels],
+      vwgt[kTailMaxLevels];
+  int32_t cn[kTailMaxLevels];
+  long long cm[kTailMaxLevels];
+  int32_t coarse_vw[kTailMaxLevels];
+};
+
+// The coarsening loop of coarsen/mod.rs:36-71 from level lvl0 (graph g) on,
+// in one single-block launch: per level the heavy list, match_parallel (same
+// seeds, rounds and progress checks) and contract, then the stop rule (cn < k
+// keeps the finer level; cn <= limit or cn/n > 0.95 stops). The levels are
+// the ones the host loop would produce. has_vw: g carries vertex weights;
+// summed_unit: coarse levels of a unit-weight graph get summed weights. The
+// level data lives in a workspace taken from the arena; the table is copied
+// to h_out (pinned) before return.
+void coarsen_tail(const DGraph& g, int has_vw, int summed_unit, int mode, uint64_t seed64, int lvl0, int k,
+                  int64_t limit, int rounds, Arena& arena, cudaStream_t st, TailOut* h_out);
+
 // ---- initial.cu ----------------------------------------------------------
 // grow_partition (src/initial/grow.rs:12-103), exact given the seed vertices:
 // one warp per trial. seeds: [ntrials][k]; grow_tgt: [k][ncon] integer form of

@@ -18,6 +18,7 @@ enum ProfId {
   kProfCut,           // k_cut
   kProfGrow,          // k_grow
   kProfLevel,         // k_refine_level: all passes of a small level in one launch
+  kProfTail,          // k_coarsen_tail: the remaining coarsening levels of a small graph
   kProfCount
 };
 
