@@ -100,10 +100,12 @@ RMETIS_API int RMETIS_GPU_SetStream(void *stream);
  * vertex weights gets summed coarse weights (1) or the reference's unit coarse
  * weights (0, default), whether ncuts > 1 attempts run concurrently on the
  * device's worker pool (1, default) or one after another (0), the largest
- * level (vertices) whose refinement runs in one single-block launch (default
- * 2048, 0 = never), and the largest level (vertices) from which all remaining
- * coarsening levels run in one single-block launch (default 4096, 0 = never);
- * the last three never change a result. Values < 0 leave a knob unchanged. */
+ * level (vertices; its adjacency entries at most 4 times that) whose
+ * refinement runs in one single-block launch (default 4096, 0 = never), and
+ * the largest level (vertices; its adjacency entries at most 64 times that)
+ * from which all remaining coarsening levels run in one single-block launch
+ * (default 4096, 0 = never); the last three never change a result. Values
+ * < 0 leave a knob unchanged. */
 RMETIS_API int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weights,
                                     int parallel_attempts, int fused_max_n, int tail_max_n);
 

@@ -39,7 +39,7 @@ struct Tuning {
   int match_rounds = 24;
   int summed_unit_weights = 0;
   int parallel_attempts = 1;
-  int fused_max_n = 2048;
+  int fused_max_n = 4096;
   int tail_max_n = 4096;
 };
 Tuning& tuning() {

@@ -32,7 +32,7 @@ struct KwayOptions {
   int match_rounds = 24;     // proposal rounds per coarsening level (upper bound)
   int summed_unit_weights = 0;  // 1: a graph without vwgt gets summed coarse weights
   int parallel_attempts = 1;    // 1: ncuts > 1 attempts run concurrently on the worker pool
-  int fused_max_n = 2048;       // levels up to this size refine in one single-block launch
+  int fused_max_n = 4096;       // levels up to this size (and 4x its edges) refine in one launch
   int tail_max_n = 4096;        // from a level of at most this size, coarsening runs in one launch
 };
 

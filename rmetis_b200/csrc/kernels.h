@@ -135,8 +135,9 @@ struct RefineParams {
   // Set when every part weight (|pw| <= total < 2^28) and every threshold
   // (|feas|, |over| < 2^29) is small: the walk may then keep 32-bit slacks.
   bool small_weights = false;
-  // Levels with at most this many vertices (and k <= 256, ncon <= 2) run all
-  // their passes in one single-block launch (k_refine_level); 0 = never.
+  // Levels with at most this many vertices and 4 times as many adjacency
+  // entries (and k <= 256, ncon <= 2) run all their passes in one
+  // single-block launch (k_refine_level); 0 = never.
   int32_t fused_max_n = 0;
 };
 

@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 def refine_path(rmb, request):
     rmb.set_tuning(fused_max_n=(1 << 30) if request.param == "fused" else 0)
     yield request.param
-    rmb.set_tuning(fused_max_n=2048)
+    rmb.set_tuning(fused_max_n=4096)
 
 
 @pytest.mark.parametrize("name", list(GRAPHS))
@@ -77,6 +77,6 @@ def test_full_partitions_identical_across_paths(rmb):
             rmb.set_tuning(fused_max_n=1 << 30)
             fused = rmb.part_graph_kway(g, k, options=o)
         finally:
-            rmb.set_tuning(fused_max_n=2048)
+            rmb.set_tuning(fused_max_n=4096)
         assert multi.objval == fused.objval
         np.testing.assert_array_equal(multi.part, fused.part)
