@@ -213,6 +213,17 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # Batched seeds, batched graphs and the serving stream
 # ---------------------------------------------------------------------------
+TUNING = {}
+
+
+def _apply_tuning():
+    """Set the launch-shape knobs the autotuner recorded for this device in
+    rmetis_b200/tuning.json (none recorded: the engine defaults stay)."""
+    from rmetis_b200 import autotune
+    dev = autotune.device_name(int(os.environ.get("LOCAL_RANK", "0")))
+    TUNING.update(autotune.apply(device=dev) or {"engine defaults": dict(autotune.DEFAULTS)})
+
+
 def _setup_device():
     import torch
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -302,7 +313,7 @@ def run_rmat_seeds(args):
         "config": {"workload": f"R-MAT scale {args.scale} (a,b,c=.57,.19,.19, edge factor 16, torch seed 22, "
                                "symmetrised, deduplicated), unit weights, nparts=256, ncuts=16 (seed 1+attempt), "
                                "Shem+Greedy, ufactor=30", "name": "rmat_seeds", "n": n, "m": m,
-                   "generation_s": round(gen_s, 1), "l2": "inputs larger than L2"},
+                   "generation_s": round(gen_s, 1), "tuning": TUNING, "l2": "inputs larger than L2"},
         "objval": int(obj16.value), "objval_first_attempt": int(obj1.value),
         "attempts_per_s": ncuts / (ms / 1e3),
         "plain_gpu": {"ms": plain[0], "attempts_per_s": ncuts / (plain[0] / 1e3), "same_result": same},
@@ -434,7 +445,7 @@ def run_rgg_batch(args):
         "config": {"workload": f"{args.graphs} 2D RGGs, n log-uniform [1e3, 2e5], mean degree 10, "
                                "edge w = 1+floor(10(1-d/r)), ncon=2 vwgt U{1..8}, k from {2,..,64}, ufactor=50, "
                                "Shem+Greedy, seed 1", "name": "rgg_batch", "n_total": n_tot, "m_total": m_tot,
-                   "generation_s": round(gen_s, 1),
+                   "generation_s": round(gen_s, 1), "tuning": TUNING,
                    "timing": "host wall clock around the whole batched call (one upload, all graphs, results "
                              "back on the host)"},
         "edges_per_s": m_tot / b,
@@ -562,7 +573,7 @@ def run_serving(args):
         "config": {"workload": f"{R} requests per rate, Poisson arrivals at {args.rates} req/s, 24 graph "
                                "templates (2D grid / 3D grid / RGG 1:1:1, n log-uniform [1e4, 2e6], unit or "
                                "U{1..10} edge weights), k U{2..128}, ncuts=1, Shem+Greedy",
-                   "name": "serving", "generation_s": round(gen_s, 1),
+                   "name": "serving", "generation_s": round(gen_s, 1), "tuning": TUNING,
                    "pool": {"workers": int(os.environ.get("RMETIS_B200_WORKERS", "8")),
                             "budget_bytes": int(os.environ.get("RMETIS_B200_POOL_BYTES", str(150 << 30)))}},
         "rates": results,
@@ -594,6 +605,7 @@ def main():
     if args.impl == "reference":
         run_reference(args)
         return
+    _apply_tuning()
     if args.workload in EXTRA_WORKLOADS:
         {"rmat_seeds": run_rmat_seeds, "rgg_batch": run_rgg_batch, "serving": run_serving}[args.workload](args)
         return
@@ -736,7 +748,7 @@ def main():
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "config": {"workload": desc, "name": args.workload, "n": n, "m": m, "nparts": k,
                        "l2": "flushed before every timed step (256 MiB write)",
-                       "parallelism": "replicas" if world > 1 else "single"},
+                       "parallelism": "replicas" if world > 1 else "single", "tuning": TUNING},
             "objval": cut_val,
             "gpu_launches": gpu_launches,
             "gpu_launches_per_step": gpu_launches / args.steps,

@@ -109,6 +109,15 @@ RMETIS_API int RMETIS_GPU_SetStream(void *stream);
 RMETIS_API int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weights,
                                     int parallel_attempts, int fused_max_n, int tail_max_n);
 
+/* The last two knobs of RMETIS_GPU_SetTuning for jobs that share the device
+ * with other jobs: the graphs of RMETIS_GPU_PartGraphKwayBatch and requests of
+ * RMETIS_GPU_SubmitKway (no counterpart in the reference). A single-block
+ * launch leaves most SMs idle in a lone call but not beside other jobs, so
+ * the best sizes differ; rmetis_b200/autotune.py measures both. -1 = use the
+ * RMETIS_GPU_SetTuning value (default); values < -1 leave a knob unchanged.
+ * Neither knob changes a result. */
+RMETIS_API int RMETIS_GPU_SetPoolTuning(int fused_max_n, int tail_max_n);
+
 /* Many graphs in one call (no counterpart in the reference, which partitions
  * one graph per call). Host arrays of the concatenated batch: graph g has
  * n_g = vtx_off[g+1]-vtx_off[g] vertices and m_g = edge_off[g+1]-edge_off[g]

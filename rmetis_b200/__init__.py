@@ -368,6 +368,13 @@ def set_tuning(grow_trials: int = -1, match_rounds: int = -1, summed_unit_weight
                                                 fused_max_n, tail_max_n), "set_tuning")
 
 
+def set_pool_tuning(fused_max_n: int = -2, tail_max_n: int = -2):
+    """Launch-shape knobs for batch graphs and submitted requests, which share
+    the device with other jobs (-1 = the set_tuning value, -2 leaves a knob
+    unchanged). Neither changes a result; rmetis_b200.autotune measures them."""
+    _raise_for(_lib.load().RMETIS_GPU_SetPoolTuning(fused_max_n, tail_max_n), "set_pool_tuning")
+
+
 def part_graph_kway_batch(graphs, nparts, ubvec=None, options: Options | None = None):
     """Partition many graphs in one call: the batch is uploaded once and the
     graphs run concurrently on the device's worker pool. Returns one

@@ -56,6 +56,26 @@ void apply_tuning(KwayOptions& o) {
   o.tail_max_n = tuning().tail_max_n;
 }
 
+// Launch-shape knobs of jobs that share the device with other jobs (batch
+// graphs and submitted requests); -1 = the single-call value. A single-block
+// launch occupies one SM, which costs a lone call the idle rest of the device
+// but not a job running beside others, so the best sizes differ.
+struct PoolTuning {
+  int fused_max_n = -1;
+  int tail_max_n = -1;
+};
+PoolTuning& pool_tuning() {
+  static PoolTuning t;
+  return t;
+}
+
+void apply_pool_tuning(KwayOptions& o) {
+  apply_tuning(o);
+  if (pool_tuning().fused_max_n >= 0) o.fused_max_n = pool_tuning().fused_max_n;
+  if (pool_tuning().tail_max_n >= 0) o.tail_max_n = pool_tuning().tail_max_n;
+  o.parallel_attempts = 0;  // the jobs already run concurrently
+}
+
 template <typename F>
 int guarded(F f) {
   try {
@@ -265,6 +285,12 @@ int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weig
   return METIS_OK;
 }
 
+int RMETIS_GPU_SetPoolTuning(int fused_max_n, int tail_max_n) {
+  if (fused_max_n >= -1) pool_tuning().fused_max_n = fused_max_n;
+  if (tail_max_n >= -1) pool_tuning().tail_max_n = tail_max_n;
+  return METIS_OK;
+}
+
 int RMETIS_GPU_SetProfiling(int on) {
   return guarded([&] {
     profiler().on = on != 0;
@@ -305,8 +331,7 @@ int RMETIS_GPU_PartGraphKwayBatch(idx_t ngraphs, idx_t ncon, const int64_t* vtx_
     }
     KwayOptions o = parse_options(options);
     if (o.rtype != 1) return METIS_ERROR_INPUT;
-    apply_tuning(o);
-    o.parallel_attempts = 0;  // the graphs already run concurrently
+    apply_pool_tuning(o);
     const int64_t ntot = vtx_off[ngraphs], mtot = edge_off[ngraphs];
     Engine& E = engine_for_current_device();
     std::lock_guard<std::mutex> lk(E.mu);
@@ -383,8 +408,7 @@ int64_t RMETIS_GPU_SubmitKway(const idx_t* nvtxs, const idx_t* ncon, const idx_t
     const int64_t ne = xadj[n];
     KwayOptions o = parse_options(options);
     if (o.rtype != 1) return METIS_ERROR_INPUT;
-    apply_tuning(o);
-    o.parallel_attempts = 0;
+    apply_pool_tuning(o);
     // tpwgts and ubvec are copied now; the CSR arrays, part and objval are
     // read and written by the worker until the request completes.
     std::vector<real_t> tp, ub;
