@@ -207,6 +207,7 @@ def run_reference(args):
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{desc}: {threads} independent partitions per step in {threads} threads"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line["repro"] = _repro()
     print(json.dumps(line))
 
 
@@ -214,6 +215,33 @@ def run_reference(args):
 # Batched seeds, batched graphs and the serving stream
 # ---------------------------------------------------------------------------
 TUNING = {}
+
+
+def _repro():
+    """What a rerun needs to know: device, driver, CUDA runtime, host cores,
+    source revision (when the tree has its git metadata)."""
+    out = {"host_cores": len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()}
+    try:
+        import torch
+        out["cuda_runtime"] = torch.version.cuda
+        if torch.cuda.is_available():
+            out["gpu"] = torch.cuda.get_device_name()
+    except Exception:
+        pass
+    try:
+        q = subprocess.run(["nvidia-smi", "--query-gpu=driver_version", "--format=csv,noheader"],
+                           capture_output=True, text=True, timeout=20)
+        if q.returncode == 0 and q.stdout.strip():
+            out["driver"] = q.stdout.strip().splitlines()[0]
+    except Exception:
+        pass
+    try:
+        q = subprocess.run(["git", "rev-parse", "--short", "HEAD"], cwd=os.path.dirname(os.path.abspath(__file__)),
+                           capture_output=True, text=True, timeout=20)
+        out["git"] = q.stdout.strip() if q.returncode == 0 else "not a git checkout"
+    except Exception:
+        out["git"] = "not a git checkout"
+    return out
 
 
 def _apply_tuning():
@@ -336,6 +364,7 @@ def run_rmat_seeds(args):
         line["cpu_baseline"] = {"value": len(as_) / dt, "unit": "edges/s (attempt-edges)", "cores": 1,
                                 "kind": "port", "sample": f"R-MAT scale 16 (n={len(xs) - 1}, m={len(as_)}), "
                                 f"k=256, 1 attempt, {dt:.2f} s, cut {cobj}"}
+    line["repro"] = _repro()
     print(json.dumps(line))
 
 
@@ -466,6 +495,7 @@ def run_rgg_batch(args):
         dt = time.perf_counter() - t0
         line["cpu_baseline"] = {"value": len(sample) / dt, "unit": "graphs/s", "cores": 1, "kind": "port",
                                 "sample": f"the first {len(sample)} graphs of the batch, 1 thread, {dt:.2f} s"}
+    line["repro"] = _repro()
     print(json.dumps(line))
 
 
@@ -582,6 +612,7 @@ def run_serving(args):
                 "d2h_bytes_per_step": None},
         "clocks": sampler.summary(tw0, tw1),
     }
+    line["repro"] = _repro()
     print(json.dumps(line))
 
 
@@ -764,7 +795,8 @@ def main():
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.workload, graph=(x, a, v, w))
-        print(json.dumps(line))
+        line["repro"] = _repro()
+    print(json.dumps(line))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -39,6 +39,7 @@ def lib():
         _lib.orc_boundary_vertices.restype = ctypes.c_int64
         _lib.orc_build_coarse_graph.restype = ctypes.c_int64
         _lib.orc_greedy_refine.restype = ctypes.c_int32
+        _lib.orc_fm_kway_refine.restype = ctypes.c_int32
         _lib.orc_rng_gen_range.restype = ctypes.c_uint64
         for name in ("orc_validate_csr", "orc_SetDefaultOptions", "orc_PartGraphKway",
                      "orc_PartGraphKway_script"):
@@ -201,6 +202,21 @@ def greedy_refine(xadj, adjncy, part, nparts, tpwgts, ubvec, niter, vwgt=None, a
                                   ctypes.c_int64(nparts), _p(tp, F64P), _p(ub, F64P), ctypes.c_int64(niter),
                                   _p(moves, I64P), ctypes.byref(npasses))
     return part, int(cut), moves[:npasses.value].copy()
+
+
+def fm_kway_refine(xadj, adjncy, part, nparts, tpwgts, ubvec, niter, vwgt=None, adjwgt=None, ncon=1):
+    """Restated fm_kway_refine (src/refine/fm_kway.rs:12-31). Returns
+    (part, cut, passes, moves)."""
+    xadj = _i32(xadj); adjncy = _i32(adjncy); vwgt = _i32(vwgt); adjwgt = _i32(adjwgt)
+    part = np.array(part, dtype=np.int32)
+    tp = np.ascontiguousarray(tpwgts, dtype=np.float64)
+    ub = np.ascontiguousarray(ubvec, dtype=np.float64)
+    st = np.zeros(2, dtype=np.int64)
+    cut = lib().orc_fm_kway_refine(ctypes.c_int64(len(xadj) - 1), ctypes.c_int64(ncon), _p(xadj, I32P),
+                                   _p(adjncy, I32P), _p(vwgt, I32P), _p(adjwgt, I32P), _p(part, I32P),
+                                   ctypes.c_int64(nparts), _p(tp, F64P), _p(ub, F64P), ctypes.c_int64(niter),
+                                   _p(st, I64P))
+    return part, int(cut), int(st[0]), int(st[1])
 
 
 def set_default_options():

@@ -24,6 +24,7 @@
 #include <deque>
 #include <limits>
 #include <random>
+#include <set>
 #include <vector>
 
 namespace {
@@ -507,6 +508,150 @@ Idx greedy_refine(const Graph& g, std::vector<Idx>& part, size_t nparts, const d
   return g.edge_cut(part.data());
 }
 
+// fm_kway_refine (src/refine/fm_kway.rs:12-31) and fm_kway_pass (:34-158).
+// The reference keeps its boundary vertices in a priority_queue 1.4.0
+// PriorityQueue keyed by gain (Cargo.lock; not vendored). Among equal gains
+// this restatement pops the lowest vertex id first; the crate's heap order
+// among equal priorities is not restated (parity unpinned for that order).
+// i32 sums wrap like the reference's release build.
+struct FmStats {
+  int64_t passes = 0;
+  int64_t moves = 0;
+};
+
+// compute_best_move (fm_kway.rs:47-71): the adjacent part p != pv with the
+// largest gain edge_to[p] - edge_to[pv] > 0 (strict >, so the lowest p on
+// ties); false when there is none.
+bool fm_best_move(const Graph& g, size_t v, const Idx* part, size_t nparts, std::vector<Idx>& edge_to,
+                  size_t* best_p_out, Idx* best_g_out) {
+  size_t pv = (size_t)part[v];
+  std::fill(edge_to.begin(), edge_to.end(), 0);
+  for (Idx j = g.xadj[v]; j < g.xadj[v + 1]; ++j) {
+    size_t pu = (size_t)part[g.adjncy[j]];
+    edge_to[pu] = (Idx)((uint32_t)edge_to[pu] + (uint32_t)g.edge_weight_at(j));
+  }
+  size_t best_p = std::numeric_limits<size_t>::max();
+  Idx best_g = 0;
+  for (size_t p = 0; p < nparts; ++p) {
+    if (p == pv) continue;
+    if (edge_to[p] == 0) continue;
+    Idx gain = (Idx)((uint32_t)edge_to[p] - (uint32_t)edge_to[pv]);
+    if (gain > best_g) { best_g = gain; best_p = p; }
+  }
+  if (best_p == std::numeric_limits<size_t>::max()) return false;
+  *best_p_out = best_p;
+  *best_g_out = best_g;
+  return true;
+}
+
+bool fm_kway_pass(const Graph& g, std::vector<Idx>& part, size_t nparts, std::vector<Idx>& pw,
+                  const double* tpwgts, const double* ubvec, FmStats* st) {
+  const size_t n = g.nvtxs, ncon = g.ncon;
+  std::vector<Idx> edge_to(nparts);
+  std::vector<size_t> bm_p(n);
+  std::vector<Idx> bm_g(n);
+  std::vector<char> has_bm(n, 0);
+  // The queue: (gain desc, vertex asc), plus each queued vertex's key.
+  auto cmp = [](const std::pair<Idx, size_t>& a, const std::pair<Idx, size_t>& b) {
+    if (a.first != b.first) return a.first > b.first;
+    return a.second < b.second;
+  };
+  std::set<std::pair<Idx, size_t>, decltype(cmp)> pq(cmp);
+  std::vector<Idx> key(n);
+  std::vector<char> queued(n, 0);
+  auto push = [&](size_t v, Idx gain) {   // push, or change_priority when queued
+    if (queued[v]) pq.erase({key[v], v});
+    key[v] = gain;
+    queued[v] = 1;
+    pq.insert({gain, v});
+  };
+  auto remove = [&](size_t v) {
+    if (queued[v]) { pq.erase({key[v], v}); queued[v] = 0; }
+  };
+  for (size_t v = 0; v < n; ++v) {                            // fm_kway.rs:74-85
+    Idx pv = part[v];
+    bool on_boundary = false;
+    for (Idx j = g.xadj[v]; j < g.xadj[v + 1]; ++j)
+      if (part[g.adjncy[j]] != pv) { on_boundary = true; break; }
+    if (!on_boundary) continue;
+    size_t tp;
+    Idx gain;
+    if (fm_best_move(g, v, part.data(), nparts, edge_to, &tp, &gain)) {
+      bm_p[v] = tp; bm_g[v] = gain; has_bm[v] = 1;
+      push(v, gain);
+    }
+  }
+  std::vector<char> locked(n, 0);
+  struct Move { size_t v; Idx from, to; };
+  std::vector<Move> moves;
+  Idx cut = g.edge_cut(part.data());
+  Idx best_cut = cut;
+  size_t best_len = 0;
+  std::vector<Idx> vw(ncon);
+  while (!pq.empty()) {                                       // fm_kway.rs:93-149
+    auto top = *pq.begin();
+    pq.erase(pq.begin());
+    size_t v = top.second;
+    Idx gain = top.first;
+    queued[v] = 0;
+    if (locked[v] || gain <= 0) break;
+    if (!has_bm[v]) continue;
+    size_t to = bm_p[v];
+    size_t from = (size_t)part[v];
+    for (size_t c = 0; c < ncon; ++c) vw[c] = g.vwgt_at(v, c);
+    bool feasible = true;
+    for (size_t c = 0; c < ncon; ++c) {
+      Idx new_w = (Idx)((uint32_t)pw[to * ncon + c] + (uint32_t)vw[c]);
+      if (!((double)new_w <= tpwgts[to * ncon + c] * ubvec[c])) { feasible = false; break; }
+    }
+    if (!feasible) continue;
+    part[v] = (Idx)to;
+    for (size_t c = 0; c < ncon; ++c) {
+      pw[from * ncon + c] = (Idx)((uint32_t)pw[from * ncon + c] - (uint32_t)vw[c]);
+      pw[to * ncon + c] = (Idx)((uint32_t)pw[to * ncon + c] + (uint32_t)vw[c]);
+    }
+    locked[v] = 1;
+    moves.push_back({v, (Idx)from, (Idx)to});
+    cut = (Idx)((uint32_t)cut - (uint32_t)gain);
+    if (cut < best_cut) { best_cut = cut; best_len = moves.size(); }
+    for (Idx j = g.xadj[v]; j < g.xadj[v + 1]; ++j) {         // fm_kway.rs:131-148
+      size_t u = (size_t)g.adjncy[j];
+      if (locked[u]) continue;
+      size_t tp;
+      Idx gu;
+      if (fm_best_move(g, u, part.data(), nparts, edge_to, &tp, &gu)) {
+        bm_p[u] = tp; bm_g[u] = gu; has_bm[u] = 1;
+        push(u, gu);
+      } else {
+        remove(u);
+        has_bm[u] = 0;
+      }
+    }
+  }
+  for (size_t i = moves.size(); i-- > best_len;) {            // fm_kway.rs:152-161 (rollback)
+    const Move& m = moves[i];
+    size_t cur = (size_t)part[m.v];
+    for (size_t c = 0; c < ncon; ++c) {
+      Idx w = g.vwgt_at(m.v, c);
+      pw[cur * ncon + c] = (Idx)((uint32_t)pw[cur * ncon + c] - (uint32_t)w);
+      pw[(size_t)m.from * ncon + c] = (Idx)((uint32_t)pw[(size_t)m.from * ncon + c] + (uint32_t)w);
+    }
+    part[m.v] = m.from;
+  }
+  if (st) st->moves += (int64_t)best_len;
+  return best_len > 0 && best_cut < (Idx)((uint32_t)g.edge_cut(part.data()) + 1u);
+}
+
+Idx fm_kway_refine(const Graph& g, std::vector<Idx>& part, size_t nparts, const double* tpwgts,
+                   const double* ubvec, size_t niter, FmStats* st) {
+  std::vector<Idx> pw = g.partition_weights(part.data(), nparts);
+  for (size_t it = 0; it < niter; ++it) {
+    if (st) st->passes += 1;
+    if (!fm_kway_pass(g, part, nparts, pw, tpwgts, ubvec, st)) break;
+  }
+  return g.edge_cut(part.data());
+}
+
 // Options (src/types.rs:52-95) with the C-ABI option codec (types.rs:190-245).
 struct Options {
   int ctype = 1;      // 0 = Rm, 1 = Shem
@@ -579,8 +724,15 @@ struct KwayStats {
   int64_t level_m[64];
 };
 
-// partition_kway (src/partition/kway.rs:20-141) with SingleComm, rtype
-// Greedy or (for completeness of dispatch) Greedy-only: FM is out of scope.
+// refine_level (src/partition/kway.rs:145-162): Greedy, or FM through
+// refine_kway (src/refine/mod.rs:26-38).
+void refine_level(const Graph& g, std::vector<Idx>& part, size_t nparts, const double* t, const double* ub,
+                  const Options& opt) {
+  if (opt.rtype == 1) greedy_refine(g, part, nparts, t, ub, (size_t)opt.niter, nullptr);
+  else fm_kway_refine(g, part, nparts, t, ub, (size_t)opt.niter, nullptr);
+}
+
+// partition_kway (src/partition/kway.rs:20-141) with SingleComm.
 // Returns 1 / -2 / -4 like the C ABI.
 int partition_kway(const Graph& graph, size_t nparts, const float* tpwgts, const float* ubvec,
                    const Options& opt, std::vector<Idx>& best_part, Idx& best_obj,
@@ -651,13 +803,13 @@ int partition_kway(const Graph& graph, size_t nparts, const float* tpwgts, const
       part = grow_partition(coarsest, nparts, coarse_t.data(), &rng,
                             script ? script->grow_seeds : nullptr, nullptr);
     }
-    greedy_refine(coarsest, part, nparts, coarse_t.data(), ub.data(), (size_t)opt.niter, nullptr);
+    refine_level(coarsest, part, nparts, coarse_t.data(), ub.data(), opt);  // kway.rs:72
     for (size_t i = levels.size(); i-- > 0;) {                // kway.rs:76-92
       const Graph& fine = (i == 0) ? graph : levels[i - 1];
       std::vector<Idx> fine_part(fine.nvtxs);
       for (size_t v = 0; v < fine.nvtxs; ++v) fine_part[v] = part[cmaps[i][v]];
       std::vector<double> t = fine.compute_target_weights(nparts, tpwgts);
-      greedy_refine(fine, fine_part, nparts, t.data(), ub.data(), (size_t)opt.niter, nullptr);
+      refine_level(fine, fine_part, nparts, t.data(), ub.data(), opt);
       part = std::move(fine_part);
     }
     Idx obj = graph.edge_cut(part.data());
@@ -835,6 +987,20 @@ Idx orc_greedy_refine(int64_t n, int64_t ncon, const Idx* xadj, const Idx* adjnc
   return cut;
 }
 
+// fm_kway_refine on a graph; part is updated in place; returns the edge cut.
+// stats (optional): [passes run, moves kept].
+Idx orc_fm_kway_refine(int64_t n, int64_t ncon, const Idx* xadj, const Idx* adjncy, const Idx* vwgt,
+                       const Idx* adjwgt, Idx* part, int64_t nparts, const double* tpwgts, const double* ubvec,
+                       int64_t niter, int64_t* stats) {
+  Graph g = make_graph(n, ncon, xadj, adjncy, vwgt, adjwgt, nullptr);
+  std::vector<Idx> p(part, part + n);
+  FmStats st;
+  Idx cut = fm_kway_refine(g, p, (size_t)nparts, tpwgts, ubvec, (size_t)niter, &st);
+  std::memcpy(part, p.data(), n * sizeof(Idx));
+  if (stats) { stats[0] = st.passes; stats[1] = st.moves; }
+  return cut;
+}
+
 // Restated RMETIS_SetDefaultOptions (src/ffi/c_api.rs:15-23).
 int orc_SetDefaultOptions(Idx* options) {
   if (!options) return -2;
@@ -844,8 +1010,7 @@ int orc_SetDefaultOptions(Idx* options) {
 }
 
 // Restated RMETIS_PartGraphKway (src/ffi/c_api.rs:56-81, 140-222) with an
-// optional script (matchings per level + grow seeds) for replay. rtype FM is
-// outside the restated path and is answered with -2 here.
+// optional script (matchings per level + grow seeds) for replay.
 int orc_PartGraphKway_script(const Idx* nvtxs, const Idx* ncon, const Idx* xadj, const Idx* adjncy,
                              const Idx* vwgt, const Idx* vsize, const Idx* adjwgt, const Idx* nparts,
                              const float* tpwgts, const float* ubvec, const Idx* options, Idx* objval,
@@ -858,7 +1023,6 @@ int orc_PartGraphKway_script(const Idx* nvtxs, const Idx* ncon, const Idx* xadj,
   if (ne < 0) return -2;
   Options o;
   if (options && options[0] != -1) o = from_raw(options);    // c_api.rs:211-222
-  if (o.rtype != 1) return -2;
   if (validate_csr((size_t)n, (size_t)nc, xadj, (size_t)n + 1, adjncy, (size_t)ne, vwgt,
                    vwgt ? (size_t)(n * nc) : 0, adjwgt, adjwgt ? (size_t)ne : 0) != 0)
     return -2;

@@ -44,3 +44,10 @@ def greedy_options(seed=1, ncuts=1, niter=10, ufactor=30, ctype=1, iptype=0):
     a[16] = ufactor
     a[17] = 0
     return a
+
+
+def fm_options(seed=1, ncuts=1, niter=10, ufactor=30, ctype=1, iptype=0):
+    """The option array of greedy_options with RTYPE = 0 (k-way FM)."""
+    a = greedy_options(seed, ncuts, niter, ufactor, ctype, iptype)
+    a[4] = 0
+    return a

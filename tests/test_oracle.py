@@ -274,3 +274,86 @@ def test_script_replay_reproduces_run(oracle):
     _, seeds = oracle.grow_partition(cur_x, cur_a, 4, t, rng=rng)
     rc2, part2, obj2 = oracle.part_graph_kway(xadj, adj, 4, options=o, script=(mats, seeds))
     assert rc2 == 1 and obj2 == obj and (part2 == part).all()
+
+
+# ---- fm_kway.rs (k-way FM, the reference's default rtype) -------------------
+
+from tests.conftest import fm_options  # noqa: E402
+from tests import fm_check  # noqa: E402
+
+
+def grid3x3():
+    return grid_graph(3, 3)
+
+
+def test_fm_kway_does_not_increase_cut(oracle):    # fm_kway.rs:207-219
+    xadj, adj = grid3x3()
+    part0 = [v // 3 for v in range(9)]
+    before = oracle.edge_cut(xadj, adj, None, part0)
+    part, cut, passes, moves = oracle.fm_kway_refine(xadj, adj, part0, 3, [3.0, 3.0, 3.0], [1.1], 5)
+    assert cut <= before
+    assert cut == oracle.edge_cut(xadj, adj, None, part)
+
+
+def _fm_case(seed):
+    from rmetis_b200 import generators as G
+    rng = np.random.default_rng(seed)
+    x, a, _, w = G.random_graph(int(rng.integers(60, 400)), 6.0, seed)
+    k = int(rng.choice([2, 3, 5, 8]))
+    n = len(x) - 1
+    ncon = int(rng.choice([1, 2]))
+    vw = rng.integers(1, 5, size=n * ncon).astype(np.int32)
+    part0 = rng.integers(0, k, size=n).astype(np.int32)
+    tot = vw.reshape(n, ncon).sum(axis=0)
+    t = np.repeat(tot[None, :] / k, k, axis=0).reshape(-1)
+    ub = np.full(ncon, 1.05)
+    return x, a, w, vw, ncon, k, part0, t, ub
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_fm_kway_properties(oracle, seed):
+    """Cut never rises and equals edge_cut; parts only receive while feasible;
+    after a pass without a move no vertex has a feasible positive-gain best
+    move; the same input gives the same output."""
+    x, a, w, vw, ncon, k, part0, t, ub = _fm_case(seed)
+    before = oracle.edge_cut(x, a, w, part0)
+    part, cut, passes, moves = oracle.fm_kway_refine(x, a, part0, k, t, ub, 50, vwgt=vw, adjwgt=w, ncon=ncon)
+    assert cut <= before and cut == oracle.edge_cut(x, a, w, part)
+    assert fm_check.balance_bound_holds(part0, part, k, vw, ncon, t, ub)
+    assert passes < 50
+    assert fm_check.fixed_point_violations(x, a, w, vw, part, k, ncon, t, ub) == []
+    again = oracle.fm_kway_refine(x, a, part0, k, t, ub, 50, vwgt=vw, adjwgt=w, ncon=ncon)
+    assert again[1] == cut and (again[0] == part).all()
+
+
+def test_kway_cycle4_k2_fm(oracle):               # correctness.rs:100-108
+    rc, part, obj = oracle.part_graph_kway(*CYCLE4, 2, options=fm_options(seed=1))
+    assert rc == 1 and ((part >= 0) & (part < 2)).all()
+    assert _balanced(oracle, *CYCLE4, part, 2, 30)
+    assert obj <= 4
+
+
+def test_kway_grid2x3_k2_fm(oracle):              # correctness.rs:110-117
+    xadj, adj = grid_graph(2, 3)
+    rc, part, obj = oracle.part_graph_kway(xadj, adj, 2, options=fm_options(seed=42))
+    assert rc == 1 and ((part >= 0) & (part < 2)).all()
+    assert _balanced(oracle, xadj, adj, part, 2, 30)
+
+
+def test_kway_deterministic_fm(oracle):           # correctness.rs:179-187
+    xadj, adj = grid4x4()
+    r1 = oracle.part_graph_kway(xadj, adj, 4, options=fm_options(seed=123))
+    r2 = oracle.part_graph_kway(xadj, adj, 4, options=fm_options(seed=123))
+    assert r1[0] == 1 and r1[2] == r2[2] and (r1[1] == r2[1]).all()
+
+
+def test_kway_weighted_fm(oracle):                # correctness.rs:221-235
+    rc, part, obj = oracle.part_graph_kway(*CYCLE4, 2, vwgt=[2, 1, 2, 1], adjwgt=[3, 1, 3, 1, 3, 1, 3, 1],
+                                           options=fm_options(seed=5))
+    assert rc == 1 and ((part >= 0) & (part < 2)).all()
+
+
+def test_kway_default_options_run_fm(oracle):     # c_api.rs:217-219: NULL options = defaults (rtype Fm)
+    xadj, adj = grid_graph(8, 8)
+    rc, part, obj = oracle.part_graph_kway(xadj, adj, 4, options=None)
+    assert rc == 1 and obj == oracle.edge_cut(xadj, adj, None, part)
