@@ -68,9 +68,12 @@ CPU_SAMPLE = {
 }
 
 
+RTYPE = {"code": 1, "name": "greedy"}  # --rtype: 1 = Greedy (default), 0 = Fm
+
+
 def kway_options(seed, ncuts=1, niter=10, ufactor=30):
     a = np.full(40, -1, dtype=np.int32)
-    a[0] = 0; a[1] = 0; a[2] = 1; a[3] = 0; a[4] = 1; a[5] = 0
+    a[0] = 0; a[1] = 0; a[2] = 1; a[3] = 0; a[4] = RTYPE["code"]; a[5] = 0
     a[6] = niter; a[7] = ncuts; a[8] = seed; a[9] = 0; a[10] = 0; a[11] = 0
     a[16] = ufactor; a[17] = 0
     return a
@@ -203,7 +206,9 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": {"workload": WORKLOADS[args.workload][3], "sample": desc, "n": len(x) - 1, "m": len(a)},
+            "config": {"workload": WORKLOADS[args.workload][3].replace("Greedy", "Fm" if RTYPE["code"] == 0
+                                                                        else "Greedy"),
+                       "sample": desc, "n": len(x) - 1, "m": len(a), "rtype": RTYPE["name"]},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{desc}: {threads} independent partitions per step in {threads} threads"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -627,11 +632,14 @@ def main():
     ap.add_argument("--graphs", type=int, default=512, help="rgg_batch: number of graphs")
     ap.add_argument("--requests", type=int, default=1000, help="serving: requests per arrival rate")
     ap.add_argument("--rates", default="50,100,200,500", help="serving: arrival rates, requests/s")
+    ap.add_argument("--rtype", default="greedy", choices=["greedy", "fm"],
+                    help="refinement: greedy (the measured path) or fm (the reference's default rtype)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    RTYPE.update(code=0 if args.rtype == "fm" else 1, name=args.rtype)
 
     if args.impl == "reference":
         run_reference(args)
@@ -654,6 +662,8 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
     build, k, seed, desc = WORKLOADS[args.workload]
+    if RTYPE["name"] == "fm":
+        desc = desc.replace("Greedy", "Fm")
     x, a, v, w = build()
     n, m = len(x) - 1, len(a)
     lib = rmb._lib.load()
@@ -779,7 +789,8 @@ def main():
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "config": {"workload": desc, "name": args.workload, "n": n, "m": m, "nparts": k,
                        "l2": "flushed before every timed step (256 MiB write)",
-                       "parallelism": "replicas" if world > 1 else "single", "tuning": TUNING},
+                       "parallelism": "replicas" if world > 1 else "single", "tuning": TUNING,
+                       "rtype": RTYPE["name"]},
             "objval": cut_val,
             "gpu_launches": gpu_launches,
             "gpu_launches_per_step": gpu_launches / args.steps,

@@ -9,11 +9,12 @@
  *                              parse_options :211-222)
  *
  * The k-way path computes on the GPU (CType Shem/Rm, IpType Grow/Random/MetisRb,
- * RType Greedy). RType Fm (the reference's default) is not on this path: such a
- * call returns METIS_ERROR_INPUT instead of silently running another
- * algorithm. Callers select Greedy with options[METIS_OPTION_PTYPE] != -1 and
- * options[METIS_OPTION_RTYPE] = 1, exactly as the reference's from_raw
- * (src/types.rs:190-224) decodes them.
+ * RType Greedy and Fm). Greedy is refined pass for pass as the reference does;
+ * Fm (the reference's default, src/refine/fm_kway.rs) runs the same move rule
+ * in parallel rounds, so its partitions match the reference's in quality
+ * rather than bit for bit (RMETIS_GPU_FmRefine). Callers select Greedy with
+ * options[METIS_OPTION_PTYPE] != -1 and options[METIS_OPTION_RTYPE] = 1,
+ * exactly as the reference's from_raw (src/types.rs:190-224) decodes them.
  *
  * Everything after the drop-in section is additive: a device-pointer variant,
  * stream/tuning/profiling controls, and one entry point per reference function
@@ -224,6 +225,19 @@ RMETIS_API int RMETIS_GPU_GrowPartition(idx_t n, idx_t ncon, const idx_t *xadj, 
 RMETIS_API int RMETIS_GPU_GreedyRefine(idx_t n, idx_t ncon, const idx_t *xadj, const idx_t *adjncy, const idx_t *vwgt,
                             const idx_t *adjwgt, idx_t *part, idx_t nparts, const double *targets,
                             const double *ubvec, idx_t niter, idx_t *cut, int64_t *stats);
+
+/* fm_kway_refine (src/refine/fm_kway.rs:12-158, selected through
+ * refine_kway src/refine/mod.rs:26-38): up to niter passes of positive-gain
+ * moves to each vertex's best adjacent part, every target feasible
+ * ((pw+vw) as f64 <= target*ub), moved vertices locked for the pass; stops
+ * after a pass without a move. Same arguments as RMETIS_GPU_GreedyRefine;
+ * stats (optional, 4 entries): passes, moves, rounds with movers, movers.
+ * The cut never rises and ends at a fixed point of the reference's move rule;
+ * the order of the moves differs from the reference's queue, so partitions
+ * match it in quality, not bit for bit. */
+RMETIS_API int RMETIS_GPU_FmRefine(idx_t n, idx_t ncon, const idx_t *xadj, const idx_t *adjncy, const idx_t *vwgt,
+                                   const idx_t *adjwgt, idx_t *part, idx_t nparts, const double *targets,
+                                   const double *ubvec, idx_t niter, idx_t *cut, int64_t *stats);
 
 /* Edge cut and partition weights of a device-resident graph without any
  * allocation, for callers that cannot allocate device memory at the point of

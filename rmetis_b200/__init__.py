@@ -314,8 +314,9 @@ def part_graph_kway(graph: Graph, nparts: int, tpwgts=None, ubvec=None, options:
                     ) -> PartitionResult:
     """Multilevel k-way partition (src/lib.rs:48-56) on the GPU.
 
-    Only RType::Greedy is on the GPU path; an Options with rtype Fm raises
-    InputError rather than running another algorithm."""
+    RType::Greedy refines pass for pass as the reference does; RType::Fm (the
+    default) runs the reference's FM move rule in parallel rounds, equal to
+    the reference's in quality rather than bit for bit."""
     options = options or Options()
     if nparts < 2:
         raise InputError(f"nparts must be >= 2, got {nparts}")

@@ -110,7 +110,6 @@ int kway_common(Engine& E, int32_t n, int32_t nc, int32_t np, const idx_t* d_xad
                 const idx_t* options, idx_t* objval, idx_t* d_part, KwayTrace* trace,
                 const KwayOptions* preset = nullptr) {
   KwayOptions o = preset ? *preset : parse_options(options);
-  if (o.rtype != 1) throw Error(METIS_ERROR_INPUT, "RType Fm is not on the GPU path; select Greedy");
   if (!preset) apply_tuning(o);
   DGraph g;
   g.n = n;
@@ -330,7 +329,6 @@ int RMETIS_GPU_PartGraphKwayBatch(idx_t ngraphs, idx_t ncon, const int64_t* vtx_
       if (x[0] != 0 || x[n] != m) return METIS_ERROR_INPUT;
     }
     KwayOptions o = parse_options(options);
-    if (o.rtype != 1) return METIS_ERROR_INPUT;
     apply_pool_tuning(o);
     const int64_t ntot = vtx_off[ngraphs], mtot = edge_off[ngraphs];
     Engine& E = engine_for_current_device();
@@ -407,7 +405,6 @@ int64_t RMETIS_GPU_SubmitKway(const idx_t* nvtxs, const idx_t* ncon, const idx_t
     if (xadj[0] != 0 || xadj[n] < 0) return METIS_ERROR_INPUT;
     const int64_t ne = xadj[n];
     KwayOptions o = parse_options(options);
-    if (o.rtype != 1) return METIS_ERROR_INPUT;
     apply_pool_tuning(o);
     // tpwgts and ubvec are copied now; the CSR arrays, part and objval are
     // read and written by the worker until the request completes.
@@ -659,9 +656,10 @@ int RMETIS_GPU_GrowPartition(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t
   });
 }
 
-int RMETIS_GPU_GreedyRefine(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
-                            const idx_t* adjwgt, idx_t* part, idx_t nparts, const double* targets,
-                            const double* ubvec, idx_t niter, idx_t* cut, int64_t* stats) {
+// The refinement of a host graph and partition by greedy_refine or fm_refine.
+static int refine_entry(bool fm, idx_t n, idx_t ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
+                        const idx_t* adjwgt, idx_t* part, idx_t nparts, const double* targets, const double* ubvec,
+                        idx_t niter, idx_t* cut, int64_t* stats) {
   return guarded([&] {
     if (n <= 0 || ncon <= 0 || nparts <= 0 || niter < 0 || !xadj || !adjncy || !part || !targets || !ubvec)
       return METIS_ERROR_INPUT;
@@ -693,7 +691,8 @@ int RMETIS_GPU_GreedyRefine(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t*
         for (int c = 0; c < ncon; ++c) tot[c] += vwgt ? vwgt[v * ncon + c] : 1;
       rp.small_weights = weights_fit_int32(tot.data(), ncon, feas.data(), over.data(), K);
     }
-    RefineStats rs = greedy_refine(g, d_part, rp, d_heavy, nh, h.E.arena(), h.st(), h.E.host_scratch());
+    RefineStats rs = fm ? fm_refine(g, d_part, rp, d_heavy, nh, h.E.arena(), h.st(), h.E.host_scratch())
+                        : greedy_refine(g, d_part, rp, d_heavy, nh, h.E.arena(), h.st(), h.E.host_scratch());
     unsigned long long* acc = h.E.arena().alloc<unsigned long long>(1);
     cut_and_weights(g, d_part, nparts, acc, nullptr, h.st());
     download(h.E, part, d_part, (size_t)n);
@@ -710,6 +709,18 @@ int RMETIS_GPU_GreedyRefine(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t*
     }
     return METIS_OK;
   });
+}
+
+int RMETIS_GPU_GreedyRefine(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
+                            const idx_t* adjwgt, idx_t* part, idx_t nparts, const double* targets,
+                            const double* ubvec, idx_t niter, idx_t* cut, int64_t* stats) {
+  return refine_entry(false, n, ncon, xadj, adjncy, vwgt, adjwgt, part, nparts, targets, ubvec, niter, cut, stats);
+}
+
+int RMETIS_GPU_FmRefine(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
+                        const idx_t* adjwgt, idx_t* part, idx_t nparts, const double* targets, const double* ubvec,
+                        idx_t niter, idx_t* cut, int64_t* stats) {
+  return refine_entry(true, n, ncon, xadj, adjncy, vwgt, adjwgt, part, nparts, targets, ubvec, niter, cut, stats);
 }
 
 }  // extern "C"

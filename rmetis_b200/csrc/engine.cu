@@ -406,6 +406,13 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
     }
 
     // ---- refinement at the coarsest level and on the way up (kway.rs:72-92) ----
+    // refine_level (kway.rs:145-162): Greedy, or FM through refine_kway
+    // (src/refine/mod.rs:26-38).
+    auto refine_level = [&](int rtype, const DGraph& lg, idx_t* lpart, const RefineParams& lrp, const idx_t* hl,
+                            int32_t nh) {
+      return rtype == 1 ? greedy_refine(lg, lpart, lrp, hl, nh, arena_, st, h_scratch_)
+                        : fm_refine(lg, lpart, lrp, hl, nh, arena_, st, h_scratch_);
+    };
     RefineParams rp;
     rp.k = k;
     rp.niter = o.niter;
@@ -415,7 +422,7 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
     rp.fused_max_n = o.fused_max_n;
     rp.collect_stats = trace != nullptr;
     {
-      RefineStats rs = greedy_refine(cg, part, rp, heavy_lists[L], heavy_counts[L], arena_, st, h_scratch_);
+      RefineStats rs = refine_level(o.rtype, cg, part, rp, heavy_lists[L], heavy_counts[L]);
       local.refine_passes += rs.passes;
       local.refine_moves += rs.moves;
       local.decide_rounds += rs.decide_iters;
@@ -428,7 +435,7 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
       rp.feas_max = feas_of(i);
       rp.over_thr = over_of(i);
       rp.small_weights = small[i];
-      RefineStats rs = greedy_refine(fg, part, rp, heavy_lists[i], heavy_counts[i], arena_, st, h_scratch_);
+      RefineStats rs = refine_level(o.rtype, fg, part, rp, heavy_lists[i], heavy_counts[i]);
       local.refine_passes += rs.passes;
       local.refine_moves += rs.moves;
       local.decide_rounds += rs.decide_iters;

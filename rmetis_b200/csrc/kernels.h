@@ -166,6 +166,14 @@ struct RefineStats {
 RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, const idx_t* heavy,
                           int32_t nheavy, Arena& arena, cudaStream_t st, int32_t* h_scratch);
 
+// fm_kway_refine (src/refine/fm_kway.rs:12-158): up to niter passes of
+// positive-gain moves of local-maximum vertices in rounds, each move's target
+// feasible, moved vertices locked for the pass; stops after a pass without a
+// move. part is updated in place. Stats: passes, moves, rounds with movers,
+// selected movers.
+RefineStats fm_refine(const DGraph& g, idx_t* part, const RefineParams& rp, const idx_t* heavy, int32_t nheavy,
+                      Arena& arena, cudaStream_t st, int32_t* h_scratch);
+
 // Gain table of one pass (boundary_vertices + compute_move_gain,
 // src/graph/mod.rs:164-171, src/refine/greedy.rs:197-218): per vertex the
 // boundary flag, w_from and the explicit candidate list sorted by

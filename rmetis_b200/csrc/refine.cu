@@ -1597,4 +1597,176 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
   return stats;
 }
 
+// ---------------------------------------------------------------------------
+// k-way FM refinement (src/refine/fm_kway.rs:12-158).
+//
+// The reference pops boundary vertices from a priority queue keyed by the
+// gain of their best move (the adjacent part with the largest positive gain,
+// lowest id on ties), moves each one whose target stays feasible, locks it
+// for the rest of the pass and re-evaluates its unlocked neighbours; a vertex
+// whose move is infeasible leaves the queue until a neighbour moves. Every
+// move has a positive exact gain, so the cut falls with each move and the
+// reference's rollback to the best prefix never undoes one. Passes repeat
+// while one moves something (at most niter).
+//
+// Here a pass runs in rounds. Each round recomputes the gain table of the
+// current partition (k_gain: every vertex's best move, exact), and selects
+// every free vertex whose move beats the moves of all its free neighbours in
+// the queue's order (gain, then lower id): an independent set of local
+// maxima, so no two movers of a round are adjacent and each move changes the
+// cut by exactly its gain. The selected moves go through the greedy walk with
+// one candidate each (k_walk_prep/classify/walk_reg, cut mode: the candidate
+// if it stays feasible under the part weights of the moves before it, in
+// vertex order), which applies them to part and pw. A selected vertex that
+// moved is locked; one that did not is dropped until a neighbour moves. The
+// pass ends at a round that selects nothing. Cut monotonicity, the
+// destination-only feasibility test and the fixed point at the end (no free
+// vertex with a feasible positive-gain move) are the reference's; the order
+// of moves among non-adjacent vertices differs, so partitions are compared
+// by quality, not bit for bit.
+// ---------------------------------------------------------------------------
+constexpr int kFmFree = 0, kFmLocked = 1, kFmDropped = 2;
+constexpr int kFmRoundsPerCheck = 4;   // rounds queued between two reads of the round counters
+constexpr int kFmMaxRounds = 512;      // bound on the rounds of one pass
+
+__device__ __forceinline__ int32_t fm_gain_of(int32_t v, const idx_t* __restrict__ xadj,
+                                              const idx_t* __restrict__ mover, const idx_t* __restrict__ ncand,
+                                              const idx_t* __restrict__ cand_g, const int32_t* __restrict__ state) {
+  if (state[v] != kFmFree || !mover[v] || ncand[v] <= 0) return 0;
+  const int32_t g = cand_g[xadj[v]];
+  return g > 0 ? g : 0;
+}
+
+// sel[v] = 1 when v's best move has a positive gain above every free
+// neighbour's (equal gains: the lower id first). sel doubles as the
+// candidate count the walk reads (the best move only).
+__global__ void k_fm_select(int32_t n, const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                            const idx_t* __restrict__ mover, const idx_t* __restrict__ ncand,
+                            const idx_t* __restrict__ cand_g, const int32_t* __restrict__ state,
+                            idx_t* __restrict__ sel) {
+  RMB_GRID_STRIDE(v, n) {
+    const int32_t gv = fm_gain_of((int32_t)v, xadj, mover, ncand, cand_g, state);
+    int32_t out = 0;
+    if (gv > 0) {
+      out = 1;
+      const int32_t s = xadj[v], e = xadj[v + 1];
+      for (int32_t j = s; j < e; ++j) {
+        const int32_t u = adj[j];
+        if (u == (int32_t)v) continue;
+        const int32_t gu = fm_gain_of(u, xadj, mover, ncand, cand_g, state);
+        if (gu > gv || (gu == gv && u < (int32_t)v)) {
+          out = 0;
+          break;
+        }
+      }
+    }
+    sel[v] = out;
+  }
+}
+
+// After the walk: a selected vertex that took its move is locked and frees
+// its dropped neighbours (the reference re-queues the unlocked neighbours of
+// a moved vertex); one that did not is dropped.
+__global__ void k_fm_after(const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
+                           const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                           const idx_t* __restrict__ part, const idx_t* __restrict__ cand_p,
+                           int32_t* __restrict__ state) {
+  const int32_t nm = *nm_dev;
+  RMB_GRID_STRIDE(i, nm) {
+    const int32_t v = movers[i];
+    const int32_t s = xadj[v], e = xadj[v + 1];
+    if (part[v] == cand_p[s]) {
+      state[v] = kFmLocked;
+      for (int32_t j = s; j < e; ++j) {
+        const int32_t u = adj[j];
+        if (state[u] == kFmDropped) state[u] = kFmFree;
+      }
+    } else {
+      state[v] = kFmDropped;
+    }
+  }
+}
+
+RefineStats fm_refine(const DGraph& g, idx_t* part, const RefineParams& rp, const idx_t* heavy, int32_t nheavy,
+                      Arena& arena, cudaStream_t st, int32_t* h_scratch) {
+  if (g.ncon > kMaxCon) throw Error(-2, "ncon above the supported maximum of 8");
+  RefineStats stats;
+  const int k = rp.k;
+  const int32_t K = k * g.ncon;
+  Arena::Mark mk = arena.mark();
+  long long* pw = arena.alloc<long long>((size_t)K);
+  long long* in_max = arena.alloc<long long>((size_t)K);
+  long long* out_max = arena.alloc<long long>((size_t)K);
+  idx_t* mover = arena.alloc<idx_t>((size_t)g.n);
+  idx_t* ncand = arena.alloc<idx_t>((size_t)g.n);
+  idx_t* wfrom = arena.alloc<idx_t>((size_t)g.n);
+  idx_t* zero = arena.alloc<idx_t>((size_t)g.n);
+  idx_t* sel = arena.alloc<idx_t>((size_t)g.n);
+  int32_t* state = arena.alloc<int32_t>((size_t)g.n);
+  idx_t* cand_p = arena.alloc<idx_t>((size_t)g.m + 1);
+  idx_t* cand_g = arena.alloc<idx_t>((size_t)g.m + 1);
+  idx_t* movers = arena.alloc<idx_t>((size_t)g.n);
+  // Per round: [2*r] selected movers, [2*r+1] moves.
+  int32_t* counters = arena.alloc<int32_t>(2 * (size_t)kFmMaxRounds);
+  int32_t* long_flag = arena.alloc<int32_t>(1);
+  MoverRecs r;
+  r.pv = arena.alloc<int32_t>((size_t)g.n);
+  r.ne = arena.alloc<int32_t>((size_t)g.n);
+  r.wf = arena.alloc<int32_t>((size_t)g.n);
+  r.coff = arena.alloc<int32_t>((size_t)g.n);
+  r.known = arena.alloc<int32_t>((size_t)g.n);
+  r.cp = arena.alloc<int32_t>((size_t)g.n * kInline);
+  r.cg = arena.alloc<int32_t>((size_t)g.n * kInline);
+  r.vw = arena.alloc<int32_t>((size_t)g.n * g.ncon);
+  r.np = arena.alloc<int32_t>((size_t)g.n);
+  int32_t* ghist = nullptr;
+  if (nheavy > 0 && k > kGainHist) ghist = arena.alloc<int32_t>((size_t)k * 256 * 4);
+  RMB_CUDA(cudaMemsetAsync(long_flag, 0, sizeof(int32_t), st));
+  RMB_CUDA(cudaMemsetAsync(in_max, 0, sizeof(long long) * (size_t)K, st));
+  RMB_CUDA(cudaMemsetAsync(out_max, 0, sizeof(long long) * (size_t)K, st));
+  RMB_CUDA(cudaMemsetAsync(zero, 0, sizeof(idx_t) * (size_t)g.n, st));
+  partition_weights_only(g, part, k, pw, st);
+  const int nb = grid_for(g.n, 256);
+  std::vector<int32_t> hc(2 * (size_t)kFmMaxRounds);
+  for (int pass = 0; pass < rp.niter; ++pass) {  // fm_kway.rs:23-27
+    RMB_CUDA(cudaMemsetAsync(state, 0, sizeof(int32_t) * (size_t)g.n, st));
+    RMB_CUDA(cudaMemsetAsync(counters, 0, sizeof(int32_t) * 2 * (size_t)kFmMaxRounds, st));
+    int64_t pass_moves = 0;
+    int rounds = 0;
+    bool done = false;
+    while (!done && rounds < kFmMaxRounds) {
+      const int r0 = rounds;
+      for (int q = 0; q < kFmRoundsPerCheck && rounds < kFmMaxRounds; ++q, ++rounds) {
+        int32_t* nm_dev = counters + 2 * rounds;
+        // A round after one that selected nothing finds nothing either: the
+        // gain kernel then only clears the mover flags.
+        const int32_t* stop = rounds > 0 ? counters + 2 * (rounds - 1) : nullptr;
+        launch_gain<kCut>(g, part, k, nullptr, nullptr, mover, ncand, wfrom, cand_p, cand_g, heavy, nheavy, ghist,
+                          st, stop);
+        k_fm_select<<<nb, 256, 0, st>>>(g.n, g.xadj, g.adjncy, mover, ncand, cand_g, state, sel);
+        RMB_LAUNCH_CHECK();
+        compact_flags(sel, g.n, movers, nm_dev, arena, st);
+        launch_walk<kCut>(g.n, nm_dev, movers, g, part, k, sel, zero, cand_p, cand_g, r, pw, rp.feas_max,
+                          rp.over_thr, in_max, out_max, nm_dev + 1, rp.small_weights, long_flag, st);
+        k_fm_after<<<nb, 256, 0, st>>>(nm_dev, movers, g.xadj, g.adjncy, part, cand_p, state);
+        RMB_LAUNCH_CHECK();
+      }
+      RMB_CUDA(cudaMemcpyAsync(hc.data() + 2 * r0, counters + 2 * r0, sizeof(int32_t) * 2 * (rounds - r0),
+                               cudaMemcpyDeviceToHost, st));
+      RMB_CUDA(cudaStreamSynchronize(st));
+      for (int q = r0; q < rounds; ++q) {
+        stats.movers += hc[2 * q];
+        pass_moves += hc[2 * q + 1];
+        if (hc[2 * q] > 0) stats.decide_iters += 1;
+        if (hc[2 * q] == 0) done = true;
+      }
+    }
+    stats.passes += 1;
+    stats.moves += pass_moves;
+    if (pass_moves == 0) break;  // fm_kway_pass returned false
+  }
+  arena.reset_to(mk);
+  return stats;
+}
+
 }  // namespace rmb

@@ -120,9 +120,9 @@ def test_async_error_codes(rmb):
     import rmetis_b200 as rmb_mod
     x, a = G.grid2d(10, 10)
     g = graph_of(rmb, x, a)
-    fm = rmb_mod.Options(rtype=rmb_mod.RType.Fm, seed=1)
-    with pytest.raises(rmb_mod.InputError):
-        rmb.submit_kway(g, 4, options=fm).wait()
+    bad = rmb_mod.Graph(4, 1, np.array([0, 2, 4, 6, 8]), np.array([1, 3, 0, 2, 1, 3, 0, 0]), validate=False)
+    with pytest.raises(rmb_mod.InputError):                    # asymmetric: found by the device validation
+        rmb.submit_kway(bad, 2, options=rmb_mod.Options(rtype=rmb_mod.RType.Greedy, seed=1)).wait()
     lib = rmb._lib.load()
     assert lib.RMETIS_GPU_WaitKway(123456789) == -2
     assert lib.RMETIS_GPU_PollKway(123456789) == -2

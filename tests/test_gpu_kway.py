@@ -129,7 +129,7 @@ def test_kway_errors(rmb):
     cyc = (np.array([0, 2, 4, 6, 8]), np.array([1, 3, 0, 2, 1, 3, 0, 2]))
     assert call_c_abi(rmb, *cyc, 10, options=greedy_options())[0] == -2        # nparts > n
     assert call_c_abi(rmb, *cyc, 1, options=greedy_options())[0] == -2         # nparts < 2
-    assert call_c_abi(rmb, *cyc, 2, options=None)[0] == -2                     # default rtype = Fm
+    assert call_c_abi(rmb, *cyc, 2, options=None)[0] == 1                      # default rtype = Fm runs
     bad = (np.array([0, 2, 4, 6, 8]), np.array([1, 3, 0, 2, 1, 3, 0, 0]))     # asymmetric
     assert call_c_abi(rmb, *bad, 2, options=greedy_options())[0] == -2
     loop = (np.array([0, 2, 4, 6, 8]), np.array([0, 3, 0, 2, 1, 3, 0, 2]))    # self-loop
@@ -144,8 +144,8 @@ def test_python_api_mirror(rmb, oracle):
     g = rmb.Graph.new_unweighted(len(x) - 1, x, a)
     res = rmb.part_graph_kway(g, 4, options=rmb.Options(rtype=rmb.RType.Greedy, seed=2))
     assert res.objval == g.edge_cut(res.part) == oracle.edge_cut(x, a, None, res.part)
-    with pytest.raises(rmb.InputError):
-        rmb.part_graph_kway(g, 4, options=rmb.Options(seed=2))  # Fm is not on the GPU path
+    fm = rmb.part_graph_kway(g, 4, options=rmb.Options(seed=2))  # rtype Fm, the default
+    assert fm.objval == g.edge_cut(fm.part) and ((fm.part >= 0) & (fm.part < 4)).all()
     with pytest.raises(rmb.InputError):
         rmb.part_graph_kway(g, 2000, options=rmb.Options(rtype=rmb.RType.Greedy))
 
