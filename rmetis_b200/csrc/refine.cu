@@ -1612,9 +1612,11 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
 // Here a pass runs in rounds. Each round recomputes the gain table of the
 // current partition (k_gain: every vertex's best move, exact), and selects
 // every free vertex whose move beats the moves of all its free neighbours in
-// the queue's order (gain, then lower id): an independent set of local
-// maxima, so no two movers of a round are adjacent and each move changes the
-// cut by exactly its gain. The selected moves go through the greedy walk with
+// the queue's order (gain, then lower id) among its neighbours in other
+// parts: local maxima, so no two movers of a round in different parts are
+// adjacent and the cut falls at least by the sum of the round's gains (two
+// adjacent movers of one part can only do better than their gains say). The
+// selected moves go through the greedy walk with
 // one candidate each (k_walk_prep/classify/walk_reg, cut mode: the candidate
 // if it stays feasible under the part weights of the moves before it, in
 // vertex order), which applies them to part and pw. A selected vertex that
@@ -1637,22 +1639,26 @@ __device__ __forceinline__ int32_t fm_gain_of(int32_t v, const idx_t* __restrict
   return g > 0 ? g : 0;
 }
 
-// sel[v] = 1 when v's best move has a positive gain above every free
-// neighbour's (equal gains: the lower id first). sel doubles as the
-// candidate count the walk reads (the best move only).
+// sel[v] = 1 when v's best move has a positive gain above the move of every
+// free neighbour in another part (equal gains: the lower id first). Two
+// movers of the same part may move together: the edge between them was
+// counted as a loss by both gains, and whatever parts they reach it costs at
+// most that, so the cut falls at least by the sum of the gains. sel doubles
+// as the candidate count the walk reads (the best move only).
 __global__ void k_fm_select(int32_t n, const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
-                            const idx_t* __restrict__ mover, const idx_t* __restrict__ ncand,
-                            const idx_t* __restrict__ cand_g, const int32_t* __restrict__ state,
-                            idx_t* __restrict__ sel) {
+                            const idx_t* __restrict__ part, const idx_t* __restrict__ mover,
+                            const idx_t* __restrict__ ncand, const idx_t* __restrict__ cand_g,
+                            const int32_t* __restrict__ state, idx_t* __restrict__ sel) {
   RMB_GRID_STRIDE(v, n) {
     const int32_t gv = fm_gain_of((int32_t)v, xadj, mover, ncand, cand_g, state);
     int32_t out = 0;
     if (gv > 0) {
       out = 1;
+      const int32_t pv = part[v];
       const int32_t s = xadj[v], e = xadj[v + 1];
       for (int32_t j = s; j < e; ++j) {
         const int32_t u = adj[j];
-        if (u == (int32_t)v) continue;
+        if (u == (int32_t)v || part[u] == pv) continue;
         const int32_t gu = fm_gain_of(u, xadj, mover, ncand, cand_g, state);
         if (gu > gv || (gu == gv && u < (int32_t)v)) {
           out = 0;
@@ -1665,12 +1671,14 @@ __global__ void k_fm_select(int32_t n, const idx_t* __restrict__ xadj, const idx
 }
 
 // After the walk: a selected vertex that took its move is locked and frees
-// its dropped neighbours (the reference re-queues the unlocked neighbours of
-// a moved vertex); one that did not is dropped.
+// its dropped neighbours that were not selected this round (the reference
+// re-queues the unlocked neighbours of a moved vertex); a selected vertex
+// that did not move is dropped. Each selected vertex's state is written by
+// its own thread only, so the result does not depend on thread order.
 __global__ void k_fm_after(const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
                            const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
                            const idx_t* __restrict__ part, const idx_t* __restrict__ cand_p,
-                           int32_t* __restrict__ state) {
+                           const idx_t* __restrict__ sel, int32_t* __restrict__ state) {
   const int32_t nm = *nm_dev;
   RMB_GRID_STRIDE(i, nm) {
     const int32_t v = movers[i];
@@ -1679,7 +1687,7 @@ __global__ void k_fm_after(const int32_t* __restrict__ nm_dev, const idx_t* __re
       state[v] = kFmLocked;
       for (int32_t j = s; j < e; ++j) {
         const int32_t u = adj[j];
-        if (state[u] == kFmDropped) state[u] = kFmFree;
+        if (!sel[u] && state[u] == kFmDropped) state[u] = kFmFree;
       }
     } else {
       state[v] = kFmDropped;
@@ -1743,12 +1751,12 @@ RefineStats fm_refine(const DGraph& g, idx_t* part, const RefineParams& rp, cons
         const int32_t* stop = rounds > 0 ? counters + 2 * (rounds - 1) : nullptr;
         launch_gain<kCut>(g, part, k, nullptr, nullptr, mover, ncand, wfrom, cand_p, cand_g, heavy, nheavy, ghist,
                           st, stop);
-        k_fm_select<<<nb, 256, 0, st>>>(g.n, g.xadj, g.adjncy, mover, ncand, cand_g, state, sel);
+        k_fm_select<<<nb, 256, 0, st>>>(g.n, g.xadj, g.adjncy, part, mover, ncand, cand_g, state, sel);
         RMB_LAUNCH_CHECK();
         compact_flags(sel, g.n, movers, nm_dev, arena, st);
         launch_walk<kCut>(g.n, nm_dev, movers, g, part, k, sel, zero, cand_p, cand_g, r, pw, rp.feas_max,
                           rp.over_thr, in_max, out_max, nm_dev + 1, rp.small_weights, long_flag, st);
-        k_fm_after<<<nb, 256, 0, st>>>(nm_dev, movers, g.xadj, g.adjncy, part, cand_p, state);
+        k_fm_after<<<nb, 256, 0, st>>>(nm_dev, movers, g.xadj, g.adjncy, part, cand_p, sel, state);
         RMB_LAUNCH_CHECK();
       }
       RMB_CUDA(cudaMemcpyAsync(hc.data() + 2 * r0, counters + 2 * r0, sizeof(int32_t) * 2 * (rounds - r0),
