@@ -57,6 +57,10 @@ WORKLOADS = {
                    "ufactor=30, ncuts=1, seed=7"),
     "grid2d_64": (lambda: G.grid2d(64, 64) + (None, None), 8, 1,
                   "2D 5-point grid 64x64, unit weights, nparts=8, Shem+Greedy, ufactor=30, ncuts=1, seed=1"),
+    # a smaller case of the 128^3 workload for profiler captures
+    "grid3d_64": (lambda: G.grid3d(64, weights_seed=7), 64, 7,
+                  "3D 7-point grid 64^3, vwgt U{1..4}, adjwgt U{1..10}, nparts=64, Shem+Greedy, "
+                  "ufactor=30, ncuts=1, seed=7"),
 }
 EXTRA_WORKLOADS = ("rmat_seeds", "rgg_batch", "serving")
 # Kernel families of RMETIS_GPU_GetProfile, in its slot order.
@@ -65,6 +69,7 @@ PROF_NAMES = ["k_gain", "k_walk", "k_match_propose", "k_contract_thread", "k_cut
 CPU_SAMPLE = {
     "grid3d_128": (lambda: G.grid3d(64, weights_seed=7), "3D 7-point grid 64^3 (same weight laws), nparts=64"),
     "grid2d_64": (lambda: G.grid2d(64, 64) + (None, None), "2D grid 64x64, nparts=8"),
+    "grid3d_64": (lambda: G.grid3d(64, weights_seed=7), "3D 7-point grid 64^3 (the workload itself), nparts=64"),
 }
 
 
