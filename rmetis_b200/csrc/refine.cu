@@ -53,8 +53,10 @@ __device__ void gain_body(Lanes L, const idx_t* __restrict__ xadj, const idx_t* 
                           const idx_t* __restrict__ adjwgt, int32_t n, int32_t ncon, const idx_t* __restrict__ part,
                           int32_t k, const long long* __restrict__ pw0, const long long* __restrict__ over_thr,
                           idx_t* __restrict__ mover, idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom,
-                          idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g) {
+                          idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g,
+                          const idx_t* __restrict__ only = nullptr) {
   RMB_FOR(v, n, L) {
+    if (only && !only[v]) continue;  // entries of vertices outside `only` stay as they are
     const int32_t s = xadj[v], e = xadj[v + 1];
     if (e - s > kHeavyDegree) continue;  // warp path
     const int32_t pv = part[v];
@@ -170,7 +172,8 @@ __global__ void k_gain(const idx_t* __restrict__ xadj, const idx_t* __restrict__
                        const idx_t* __restrict__ adjwgt, int32_t n, int32_t ncon, const idx_t* __restrict__ part,
                        int32_t k, const long long* __restrict__ pw0, const long long* __restrict__ over_thr,
                        idx_t* __restrict__ mover, idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom,
-                       idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g, const int32_t* __restrict__ stop) {
+                       idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g, const int32_t* __restrict__ stop,
+                       const idx_t* __restrict__ only) {
   // stop: moves of the previous cut pass. None means this pass would find the
   // same movers and make no move either (the reference stops there): no movers.
   if (stop && *stop == 0) {
@@ -178,7 +181,7 @@ __global__ void k_gain(const idx_t* __restrict__ xadj, const idx_t* __restrict__
     return;
   }
   gain_body<HAS_W, MODE>(grid_lanes(), xadj, adj, adjwgt, n, ncon, part, k, pw0, over_thr, mover, ncand, wfrom,
-                         cand_p, cand_g);
+                         cand_p, cand_g, only);
 }
 
 constexpr int kGainHist = 2048;  // dense per-warp part histogram in shared memory
@@ -197,11 +200,12 @@ __device__ void gain_heavy_body(int32_t gw, int32_t nw, int32_t* hist, const idx
                                 const idx_t* __restrict__ part, int32_t k, const long long* __restrict__ pw0,
                                 const long long* __restrict__ over_thr, idx_t* __restrict__ mover,
                                 idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom, idx_t* __restrict__ cand_p,
-                                idx_t* __restrict__ cand_g) {
+                                idx_t* __restrict__ cand_g, const idx_t* __restrict__ only = nullptr) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   for (int32_t hi = gw; hi < nheavy; hi += nw) {
     const int32_t v = heavy[hi];
+    if (only && !only[v]) continue;  // warp-uniform: every lane reads the same flag
     const int32_t s = xadj[v], e = xadj[v + 1];
     const int32_t pv = part[v];
     if (MODE == kRepair) {
@@ -267,7 +271,7 @@ __global__ void k_gain_heavy(const idx_t* __restrict__ xadj, const idx_t* __rest
                              const long long* __restrict__ pw0, const long long* __restrict__ over_thr,
                              idx_t* __restrict__ mover, idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom,
                              idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g, int32_t* __restrict__ ghist,
-                             const int32_t* __restrict__ stop) {
+                             const int32_t* __restrict__ stop, const idx_t* __restrict__ only) {
   if (stop && *stop == 0) return;  // k_gain has cleared every mover flag
   __shared__ int32_t sh_all[4][kGainHist];
   const int wib = threadIdx.x >> 5;
@@ -275,7 +279,7 @@ __global__ void k_gain_heavy(const idx_t* __restrict__ xadj, const idx_t* __rest
   const int32_t nw = gridDim.x * (blockDim.x >> 5);
   int32_t* hist = (k <= kGainHist) ? sh_all[wib] : ghist + (int64_t)gw * k;
   gain_heavy_body<HAS_W, MODE>(gw, nw, hist, xadj, adj, adjwgt, heavy, nheavy, ncon, part, k, pw0, over_thr, mover,
-                               ncand, wfrom, cand_p, cand_g);
+                               ncand, wfrom, cand_p, cand_g, only);
 }
 
 
@@ -1231,28 +1235,32 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_reg(const int32_t* __rest
 template <int MODE>
 static int launch_gain(const DGraph& g, const idx_t* part, int k, const long long* pw0, const long long* over_thr,
                        idx_t* mover, idx_t* ncand, idx_t* wfrom, idx_t* cand_p, idx_t* cand_g, const idx_t* heavy,
-                       int32_t nheavy, int32_t* ghist, cudaStream_t st, const int32_t* stop = nullptr) {
+                       int32_t nheavy, int32_t* ghist, cudaStream_t st, const int32_t* stop = nullptr,
+                       const idx_t* only = nullptr) {
   const int blocks = grid_for(g.n, 256);
   // Algorithmic bytes of a full pass: xadj, part (own + neighbour gathers),
   // adjncy, adjwgt, mover flag.
-  const double bytes = 12.0 * g.n + (g.adjwgt ? 12.0 : 8.0) * (double)g.m;
+  // (A launch limited to the vertices of `only` counts only its flag scan.)
+  const double bytes = only ? 4.0 * g.n : 12.0 * g.n + (g.adjwgt ? 12.0 : 8.0) * (double)g.m;
   const int ph = MODE == kCut ? profiler().begin(kProfGain, st) : -1;
   if (g.adjwgt)
     k_gain<true, MODE><<<blocks, 256, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, g.n, g.ncon, part, k, pw0, over_thr,
-                                                mover, ncand, wfrom, cand_p, cand_g, stop);
+                                                mover, ncand, wfrom, cand_p, cand_g, stop, only);
   else
     k_gain<false, MODE><<<blocks, 256, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, g.n, g.ncon, part, k, pw0, over_thr,
-                                                 mover, ncand, wfrom, cand_p, cand_g, stop);
+                                                 mover, ncand, wfrom, cand_p, cand_g, stop, only);
   RMB_LAUNCH_CHECK();
   profiler().end(ph, st, bytes);
   if (nheavy > 0) {
     const int hb = grid_for(nheavy, 4, 256);
     if (g.adjwgt)
       k_gain_heavy<true, MODE><<<hb, 128, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, heavy, nheavy, g.ncon, part, k, pw0,
-                                                    over_thr, mover, ncand, wfrom, cand_p, cand_g, ghist, stop);
+                                                    over_thr, mover, ncand, wfrom, cand_p, cand_g, ghist, stop,
+                                                    only);
     else
       k_gain_heavy<false, MODE><<<hb, 128, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, heavy, nheavy, g.ncon, part, k, pw0,
-                                                     over_thr, mover, ncand, wfrom, cand_p, cand_g, ghist, stop);
+                                                     over_thr, mover, ncand, wfrom, cand_p, cand_g, ghist, stop,
+                                                     only);
     RMB_LAUNCH_CHECK();
   }
   return ph;
@@ -1609,8 +1617,10 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
 // reference's rollback to the best prefix never undoes one. Passes repeat
 // while one moves something (at most niter).
 //
-// Here a pass runs in rounds. Each round recomputes the gain table of the
-// current partition (k_gain: every vertex's best move, exact), and selects
+// Here a pass runs in rounds. Each round brings the gain table up to date
+// with the current partition (k_gain: every vertex's best move, exact; after
+// the first round of a pass only for the vertices next to the last round's
+// moves, the others' entries being unchanged), and selects
 // every free vertex whose move beats the moves of all its free neighbours in
 // the queue's order (gain, then lower id) among its neighbours in other
 // parts: local maxima, so no two movers of a round in different parts are
@@ -1620,7 +1630,9 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
 // one candidate each (k_walk_prep/classify/walk_reg, cut mode: the candidate
 // if it stays feasible under the part weights of the moves before it, in
 // vertex order), which applies them to part and pw. A selected vertex that
-// moved is locked; one that did not is dropped until a neighbour moves. The
+// moved is locked; one that did not is dropped until a neighbour moves. Only
+// vertices within two hops of a round's moves and drops can change their
+// selection in the next round, so later rounds select among those alone. The
 // pass ends at a round that selects nothing. Cut monotonicity, the
 // destination-only feasibility test and the fixed point at the end (no free
 // vertex with a feasible positive-gain move) are the reference's; the order
@@ -1645,11 +1657,19 @@ __device__ __forceinline__ int32_t fm_gain_of(int32_t v, const idx_t* __restrict
 // counted as a loss by both gains, and whatever parts they reach it costs at
 // most that, so the cut falls at least by the sum of the gains. sel doubles
 // as the candidate count the walk reads (the best move only).
+// active (rounds after the first of a pass): only vertices within two hops
+// of the last round's changes can change their selection; the others were
+// not selected then and are not now.
 __global__ void k_fm_select(int32_t n, const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
                             const idx_t* __restrict__ part, const idx_t* __restrict__ mover,
                             const idx_t* __restrict__ ncand, const idx_t* __restrict__ cand_g,
-                            const int32_t* __restrict__ state, idx_t* __restrict__ sel) {
+                            const int32_t* __restrict__ state, const idx_t* __restrict__ active,
+                            idx_t* __restrict__ sel) {
   RMB_GRID_STRIDE(v, n) {
+    if (active && !active[v]) {
+      sel[v] = 0;
+      continue;
+    }
     const int32_t gv = fm_gain_of((int32_t)v, xadj, mover, ncand, cand_g, state);
     int32_t out = 0;
     if (gv > 0) {
@@ -1675,23 +1695,43 @@ __global__ void k_fm_select(int32_t n, const idx_t* __restrict__ xadj, const idx
 // re-queues the unlocked neighbours of a moved vertex); a selected vertex
 // that did not move is dropped. Each selected vertex's state is written by
 // its own thread only, so the result does not depend on thread order.
+// changed (for the next round; zero on entry): every vertex whose best move
+// may differ now (a moved vertex and its neighbours) or whose state changed
+// (a dropped one).
 __global__ void k_fm_after(const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
                            const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
                            const idx_t* __restrict__ part, const idx_t* __restrict__ cand_p,
-                           const idx_t* __restrict__ sel, int32_t* __restrict__ state) {
+                           const idx_t* __restrict__ sel, int32_t* __restrict__ state,
+                           idx_t* __restrict__ changed) {
   const int32_t nm = *nm_dev;
   RMB_GRID_STRIDE(i, nm) {
     const int32_t v = movers[i];
     const int32_t s = xadj[v], e = xadj[v + 1];
+    changed[v] = 1;
     if (part[v] == cand_p[s]) {
       state[v] = kFmLocked;
       for (int32_t j = s; j < e; ++j) {
         const int32_t u = adj[j];
+        changed[u] = 1;
         if (!sel[u] && state[u] == kFmDropped) state[u] = kFmFree;
       }
     } else {
       state[v] = kFmDropped;
     }
+  }
+}
+
+// active_next = changed and their neighbours (zero on entry). Also clears the
+// flags the round just used (changed_cur, active_cur) for the round after next.
+__global__ void k_fm_spread(int32_t n, const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                            const idx_t* __restrict__ changed, idx_t* __restrict__ active_next,
+                            idx_t* __restrict__ changed_cur, idx_t* __restrict__ active_cur) {
+  RMB_GRID_STRIDE(v, n) {
+    changed_cur[v] = 0;
+    active_cur[v] = 0;
+    if (!changed[v]) continue;
+    active_next[v] = 1;
+    for (int32_t j = xadj[v]; j < xadj[v + 1]; ++j) active_next[adj[j]] = 1;
   }
 }
 
@@ -1711,6 +1751,10 @@ RefineStats fm_refine(const DGraph& g, idx_t* part, const RefineParams& rp, cons
   idx_t* zero = arena.alloc<idx_t>((size_t)g.n);
   idx_t* sel = arena.alloc<idx_t>((size_t)g.n);
   int32_t* state = arena.alloc<int32_t>((size_t)g.n);
+  // Two sets of round flags, used alternately: [0] changed, [1] active.
+  idx_t* flags[2][2];
+  for (int b = 0; b < 2; ++b)
+    for (int f = 0; f < 2; ++f) flags[b][f] = arena.alloc<idx_t>((size_t)g.n);
   idx_t* cand_p = arena.alloc<idx_t>((size_t)g.m + 1);
   idx_t* cand_g = arena.alloc<idx_t>((size_t)g.m + 1);
   idx_t* movers = arena.alloc<idx_t>((size_t)g.n);
@@ -1739,6 +1783,8 @@ RefineStats fm_refine(const DGraph& g, idx_t* part, const RefineParams& rp, cons
   for (int pass = 0; pass < rp.niter; ++pass) {  // fm_kway.rs:23-27
     RMB_CUDA(cudaMemsetAsync(state, 0, sizeof(int32_t) * (size_t)g.n, st));
     RMB_CUDA(cudaMemsetAsync(counters, 0, sizeof(int32_t) * 2 * (size_t)kFmMaxRounds, st));
+    for (int b = 0; b < 2; ++b)
+      for (int f = 0; f < 2; ++f) RMB_CUDA(cudaMemsetAsync(flags[b][f], 0, sizeof(idx_t) * (size_t)g.n, st));
     int64_t pass_moves = 0;
     int rounds = 0;
     bool done = false;
@@ -1749,14 +1795,21 @@ RefineStats fm_refine(const DGraph& g, idx_t* part, const RefineParams& rp, cons
         // A round after one that selected nothing finds nothing either: the
         // gain kernel then only clears the mover flags.
         const int32_t* stop = rounds > 0 ? counters + 2 * (rounds - 1) : nullptr;
+        // The first round of a pass evaluates every vertex; later rounds only
+        // the ones the previous round's changes can reach.
+        idx_t* const* cur = flags[rounds & 1];
+        idx_t* const* nxt = flags[(rounds + 1) & 1];
         launch_gain<kCut>(g, part, k, nullptr, nullptr, mover, ncand, wfrom, cand_p, cand_g, heavy, nheavy, ghist,
-                          st, stop);
-        k_fm_select<<<nb, 256, 0, st>>>(g.n, g.xadj, g.adjncy, part, mover, ncand, cand_g, state, sel);
+                          st, stop, rounds > 0 ? cur[0] : nullptr);
+        k_fm_select<<<nb, 256, 0, st>>>(g.n, g.xadj, g.adjncy, part, mover, ncand, cand_g, state,
+                                        rounds > 0 ? cur[1] : nullptr, sel);
         RMB_LAUNCH_CHECK();
         compact_flags(sel, g.n, movers, nm_dev, arena, st);
         launch_walk<kCut>(g.n, nm_dev, movers, g, part, k, sel, zero, cand_p, cand_g, r, pw, rp.feas_max,
                           rp.over_thr, in_max, out_max, nm_dev + 1, rp.small_weights, long_flag, st);
-        k_fm_after<<<nb, 256, 0, st>>>(nm_dev, movers, g.xadj, g.adjncy, part, cand_p, sel, state);
+        k_fm_after<<<nb, 256, 0, st>>>(nm_dev, movers, g.xadj, g.adjncy, part, cand_p, sel, state, nxt[0]);
+        RMB_LAUNCH_CHECK();
+        k_fm_spread<<<nb, 256, 0, st>>>(g.n, g.xadj, g.adjncy, nxt[0], nxt[1], cur[0], cur[1]);
         RMB_LAUNCH_CHECK();
       }
       RMB_CUDA(cudaMemcpyAsync(hc.data() + 2 * r0, counters + 2 * r0, sizeof(int32_t) * 2 * (rounds - r0),
