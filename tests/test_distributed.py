@@ -34,7 +34,7 @@ def _graph():
     return rmb.Graph(len(x) - 1, 1, x, a, vwgt=v, adjwgt=w)
 
 
-def _worker_ncuts(rank, world, port, ncuts, out_dir):
+def _worker_ncuts(rank, world, port, ncuts, out_dir, rtype="greedy"):
     import torch.distributed as dist
     import rmetis_b200 as rmb
     from rmetis_b200 import distributed as D
@@ -43,7 +43,8 @@ def _worker_ncuts(rank, world, port, ncuts, out_dir):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         g = _graph()
-        o = rmb.Options(rtype=rmb.RType.Greedy, seed=5, ncuts=ncuts, iptype=rmb.IpType.Random)
+        rt = rmb.RType.Fm if rtype == "fm" else rmb.RType.Greedy
+        o = rmb.Options(rtype=rt, seed=5, ncuts=ncuts, iptype=rmb.IpType.Random)
         res = D.part_graph_kway_ranks(g, 6, options=o, partition=_oracle_partition)
         np.save(os.path.join(out_dir, f"part{rank}.npy"), res.part)
         np.save(os.path.join(out_dir, f"obj{rank}.npy"), np.array([res.objval]))
@@ -51,10 +52,10 @@ def _worker_ncuts(rank, world, port, ncuts, out_dir):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world,ncuts", [(2, 5), (3, 7), (2, 1)])
-def test_ncuts_striped_over_ranks(tmp_path, world, ncuts):
+@pytest.mark.parametrize("world,ncuts,rtype", [(2, 5, "greedy"), (3, 7, "greedy"), (2, 1, "greedy"), (2, 4, "fm")])
+def test_ncuts_striped_over_ranks(tmp_path, world, ncuts, rtype):
     import rmetis_b200 as rmb
-    mp.spawn(_worker_ncuts, args=(world, _free_port(), ncuts, str(tmp_path)), nprocs=world, join=True)
+    mp.spawn(_worker_ncuts, args=(world, _free_port(), ncuts, str(tmp_path), rtype), nprocs=world, join=True)
     parts = [np.load(tmp_path / f"part{r}.npy") for r in range(world)]
     objs = [int(np.load(tmp_path / f"obj{r}.npy")[0]) for r in range(world)]
     assert len(set(objs)) == 1 and all((p == parts[0]).all() for p in parts)
@@ -62,7 +63,8 @@ def test_ncuts_striped_over_ranks(tmp_path, world, ncuts):
     g = _graph()
     runs = []
     for a in range(ncuts):
-        o = rmb.Options(rtype=rmb.RType.Greedy, seed=5 + a, ncuts=1, iptype=rmb.IpType.Random)
+        rt = rmb.RType.Fm if rtype == "fm" else rmb.RType.Greedy
+        o = rmb.Options(rtype=rt, seed=5 + a, ncuts=1, iptype=rmb.IpType.Random)
         runs.append(_oracle_partition(g, 6, None, None, o))
     local = {}
     for r in range(world):
