@@ -41,8 +41,9 @@ def lib():
         _lib.orc_greedy_refine.restype = ctypes.c_int32
         _lib.orc_fm_kway_refine.restype = ctypes.c_int32
         _lib.orc_rng_gen_range.restype = ctypes.c_uint64
+        _lib.orc_fm2_refine.restype = ctypes.c_int32
         for name in ("orc_validate_csr", "orc_SetDefaultOptions", "orc_PartGraphKway",
-                     "orc_PartGraphKway_script"):
+                     "orc_PartGraphKway_script", "orc_PartGraphRecursive"):
             getattr(_lib, name).restype = ctypes.c_int
     return _lib
 
@@ -223,6 +224,36 @@ def set_default_options():
     opts = np.zeros(40, dtype=np.int32)
     rc = lib().orc_SetDefaultOptions(_p(opts, I32P))
     return rc, opts
+
+
+def fm2_refine(xadj, adjncy, part, tpwgts, ubvec, niter, vwgt=None, adjwgt=None, ncon=1):
+    """Restated 2-way fm_refine (src/refine/fm.rs:12-28). Returns (part, cut)."""
+    xadj = _i32(xadj); adjncy = _i32(adjncy); vwgt = _i32(vwgt); adjwgt = _i32(adjwgt)
+    part = np.array(part, dtype=np.int32)
+    tp = np.ascontiguousarray(tpwgts, dtype=np.float64)
+    ub = np.ascontiguousarray(ubvec, dtype=np.float64)
+    cut = lib().orc_fm2_refine(ctypes.c_int64(len(xadj) - 1), ctypes.c_int64(ncon), _p(xadj, I32P),
+                               _p(adjncy, I32P), _p(vwgt, I32P), _p(adjwgt, I32P), _p(part, I32P), _p(tp, F64P),
+                               _p(ub, F64P), ctypes.c_int64(niter))
+    return part, int(cut)
+
+
+def part_graph_recursive(xadj, adjncy, nparts, vwgt=None, adjwgt=None, ncon=1, tpwgts=None, ubvec=None,
+                         options=None):
+    """Restated RMETIS_PartGraphRecursive (src/ffi/c_api.rs:27-53,
+    src/partition/recursive.rs:12-187). Returns (rc, part, objval)."""
+    xadj = _i32(xadj); adjncy = _i32(adjncy); vwgt = _i32(vwgt); adjwgt = _i32(adjwgt)
+    n = len(xadj) - 1
+    part = np.zeros(n, dtype=np.int32)
+    obj = ctypes.c_int32(0)
+    nv = ctypes.c_int32(n); nc = ctypes.c_int32(ncon); npr = ctypes.c_int32(nparts)
+    tp = None if tpwgts is None else np.ascontiguousarray(tpwgts, dtype=np.float32)
+    ub = None if ubvec is None else np.ascontiguousarray(ubvec, dtype=np.float32)
+    op = None if options is None else _i32(options)
+    rc = lib().orc_PartGraphRecursive(ctypes.byref(nv), ctypes.byref(nc), _p(xadj, I32P), _p(adjncy, I32P),
+                                      _p(vwgt, I32P), None, _p(adjwgt, I32P), ctypes.byref(npr), _p(tp, F32P),
+                                      _p(ub, F32P), _p(op, I32P), ctypes.byref(obj), _p(part, I32P))
+    return rc, part, int(obj.value)
 
 
 def part_graph_kway(xadj, adjncy, nparts, vwgt=None, adjwgt=None, ncon=1, tpwgts=None, ubvec=None,

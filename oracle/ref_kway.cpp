@@ -822,6 +822,260 @@ int partition_kway(const Graph& graph, size_t nparts, const float* tpwgts, const
   return 1;
 }
 
+// ---------------------------------------------------------------------------
+// Recursive bisection (src/partition/recursive.rs:12-187) with its 2-way
+// refinement (src/refine/mod.rs:12-23: Greedy, or FM of src/refine/fm.rs).
+// ---------------------------------------------------------------------------
+
+// Graph::extract_subgraph (src/graph/mod.rs:209-273): the vertices of
+// `target` in ascending id, their edges inside it in CSR order.
+Graph extract_subgraph(const Graph& g, const Idx* part, Idx target, std::vector<size_t>& new_to_old) {
+  new_to_old.clear();
+  for (size_t v = 0; v < g.nvtxs; ++v)
+    if (part[v] == target) new_to_old.push_back(v);
+  const size_t sn = new_to_old.size();
+  std::vector<size_t> old_to_new(g.nvtxs, std::numeric_limits<size_t>::max());
+  for (size_t i = 0; i < sn; ++i) old_to_new[new_to_old[i]] = i;
+  Graph s;
+  s.nvtxs = sn;
+  s.ncon = g.ncon;
+  s.xadj.assign(sn + 1, 0);
+  s.has_adjwgt = g.has_adjwgt;
+  s.has_vwgt = g.has_vwgt;
+  s.has_vsize = g.has_vsize;
+  for (size_t i = 0; i < sn; ++i) {
+    const size_t old = new_to_old[i];
+    for (Idx j = g.xadj[old]; j < g.xadj[old + 1]; ++j) {
+      const size_t u = (size_t)g.adjncy[j];
+      if (part[u] == target) {
+        s.adjncy.push_back((Idx)old_to_new[u]);
+        if (g.has_adjwgt) s.adjwgt.push_back(g.edge_weight_at((size_t)j));
+      }
+    }
+    s.xadj[i + 1] = (Idx)s.adjncy.size();
+    if (g.has_vwgt)
+      for (size_t c = 0; c < g.ncon; ++c) s.vwgt.push_back(g.vwgt[old * g.ncon + c]);
+    if (g.has_vsize) s.vsize.push_back(g.vsize[old]);
+  }
+  return s;
+}
+
+// fm_refine / fm_pass (src/refine/fm.rs:12-127): every popped boundary
+// vertex moves to the other side if that side stays feasible, whatever its
+// gain; the pass then rolls back to the best cut seen. The queue's order among
+// equal gains follows the k-way FM restatement (lowest vertex id first; the
+// priority_queue crate's heap order is not restated). Note the reference's
+// `improved` test compares with the cut before the rollback (fm.rs:118).
+bool fm2_pass(const Graph& g, std::vector<Idx>& part, std::vector<Idx>& pw, const double* tpwgts,
+              const double* ubvec) {
+  const size_t n = g.nvtxs, ncon = g.ncon;
+  std::vector<Idx> gains(n);
+  for (size_t v = 0; v < n; ++v) gains[v] = compute_move_gain(g, v, part.data(), part[v], 1 - part[v]);
+  auto cmp = [](const std::pair<Idx, size_t>& a, const std::pair<Idx, size_t>& b) {
+    if (a.first != b.first) return a.first > b.first;
+    return a.second < b.second;
+  };
+  std::set<std::pair<Idx, size_t>, decltype(cmp)> pq(cmp);
+  std::vector<Idx> key(n);
+  std::vector<char> queued(n, 0);
+  auto on_boundary = [&](size_t v) {
+    for (Idx j = g.xadj[v]; j < g.xadj[v + 1]; ++j)
+      if (part[g.adjncy[j]] != part[v]) return true;
+    return false;
+  };
+  auto push = [&](size_t v, Idx k) {
+    if (queued[v]) pq.erase({key[v], v});
+    key[v] = k;
+    queued[v] = 1;
+    pq.insert({k, v});
+  };
+  for (size_t v = 0; v < n; ++v)
+    if (on_boundary(v)) push(v, gains[v]);
+  std::vector<char> locked(n, 0);
+  struct Move { size_t v; Idx from; };
+  std::vector<Move> moves;
+  Idx cut = g.edge_cut(part.data());
+  Idx best_cut = cut;
+  size_t best_len = 0;
+  while (!pq.empty()) {
+    auto top = *pq.begin();
+    pq.erase(pq.begin());
+    const size_t v = top.second;
+    const Idx gain = top.first;
+    queued[v] = 0;
+    if (locked[v]) continue;
+    const Idx from = part[v], to = 1 - from;
+    bool feasible = true;
+    for (size_t c = 0; c < ncon; ++c) {
+      Idx new_w = (Idx)((uint32_t)pw[(size_t)to * ncon + c] + (uint32_t)g.vwgt_at(v, c));
+      if (!((double)new_w <= tpwgts[(size_t)to * ncon + c] * ubvec[c])) { feasible = false; break; }
+    }
+    if (!feasible) continue;
+    part[v] = to;
+    for (size_t c = 0; c < ncon; ++c) {
+      const uint32_t w = (uint32_t)g.vwgt_at(v, c);
+      pw[(size_t)from * ncon + c] = (Idx)((uint32_t)pw[(size_t)from * ncon + c] - w);
+      pw[(size_t)to * ncon + c] = (Idx)((uint32_t)pw[(size_t)to * ncon + c] + w);
+    }
+    locked[v] = 1;
+    moves.push_back({v, from});
+    cut = (Idx)((uint32_t)cut - (uint32_t)gain);
+    if (cut < best_cut) { best_cut = cut; best_len = moves.size(); }
+    for (Idx j = g.xadj[v]; j < g.xadj[v + 1]; ++j) {
+      const size_t u = (size_t)g.adjncy[j];
+      if (locked[u]) continue;
+      gains[u] = compute_move_gain(g, u, part.data(), part[u], 1 - part[u]);
+      if (queued[u]) push(u, gains[u]);
+      else if (on_boundary(u)) push(u, gains[u]);
+    }
+  }
+  const bool improved = best_len > 0 && best_cut < g.edge_cut(part.data());
+  for (size_t i = moves.size(); i-- > best_len;) {
+    const Move& m = moves[i];
+    const Idx cur = part[m.v];
+    for (size_t c = 0; c < ncon; ++c) {
+      const uint32_t w = (uint32_t)g.vwgt_at(m.v, c);
+      pw[(size_t)cur * ncon + c] = (Idx)((uint32_t)pw[(size_t)cur * ncon + c] - w);
+      pw[(size_t)m.from * ncon + c] = (Idx)((uint32_t)pw[(size_t)m.from * ncon + c] + w);
+    }
+    part[m.v] = m.from;
+  }
+  return improved;
+}
+
+Idx fm2_refine(const Graph& g, std::vector<Idx>& part, const double* tpwgts, const double* ubvec, size_t niter) {
+  std::vector<Idx> pw = g.partition_weights(part.data(), 2);
+  for (size_t it = 0; it < niter; ++it)
+    if (!fm2_pass(g, part, pw, tpwgts, ubvec)) break;
+  return g.edge_cut(part.data());
+}
+
+// refine_2way (src/refine/mod.rs:12-23)
+void refine_2way(const Graph& g, std::vector<Idx>& part, const double* t, const double* ub, const Options& opt) {
+  if (opt.rtype == 1) greedy_refine(g, part, 2, t, ub, (size_t)opt.niter, nullptr);
+  else fm2_refine(g, part, t, ub, (size_t)opt.niter);
+}
+
+// coarsen (src/coarsen/mod.rs:24-71) with one rank.
+void coarsen_levels(const Graph& graph, size_t nparts, const Options& opt, SmallRng& rng, std::vector<Graph>& levels,
+                    std::vector<std::vector<size_t>>& cmaps) {
+  const size_t limit = std::max<size_t>(20 * nparts, 20);
+  levels.reserve(128);
+  const Graph* current = &graph;
+  for (;;) {
+    std::vector<size_t> matching = opt.ctype == 0 ? random_matching(*current, rng) : shem_matching(*current, rng);
+    std::vector<size_t> cmap;
+    Graph cg = current->build_coarse_graph(matching, cmap);
+    const float ratio = (float)cg.nvtxs / (float)current->nvtxs;
+    levels.push_back(std::move(cg));
+    cmaps.push_back(std::move(cmap));
+    const Graph& last = levels.back();
+    if (last.nvtxs <= limit || ratio > 0.95f) break;
+    current = &levels.back();
+  }
+}
+
+// multilevel_bisect (src/partition/recursive.rs:133-187). Returns -4 when the
+// grow step would need more distinct seeds than the coarsest graph has
+// vertices (the reference's seed draw never ends there).
+int multilevel_bisect(const Graph& graph, const float* tpwgts2, const double* ub, const Options& opt, SmallRng& rng,
+                      std::vector<Idx>& part) {
+  if (graph.nvtxs <= 2) {
+    part.resize(graph.nvtxs);
+    for (size_t v = 0; v < graph.nvtxs; ++v) part[v] = (Idx)v;
+    return 1;
+  }
+  std::vector<Graph> levels;
+  std::vector<std::vector<size_t>> cmaps;
+  coarsen_levels(graph, 2, opt, rng, levels, cmaps);
+  const Graph& coarsest = levels.empty() ? graph : levels.back();
+  std::vector<double> ct = coarsest.compute_target_weights(2, tpwgts2);
+  if (opt.iptype == 1) {
+    part = random_partition(coarsest, 2, rng);
+  } else {
+    if (coarsest.nvtxs < 2) return -4;
+    part = grow_partition(coarsest, 2, ct.data(), &rng, nullptr, nullptr);
+  }
+  refine_2way(coarsest, part, ct.data(), ub, opt);
+  for (size_t i = levels.size(); i-- > 0;) {
+    const Graph& fine = (i == 0) ? graph : levels[i - 1];
+    std::vector<Idx> fine_part(fine.nvtxs);
+    for (size_t v = 0; v < fine.nvtxs; ++v) fine_part[v] = part[cmaps[i][v]];
+    std::vector<double> t = fine.compute_target_weights(2, tpwgts2);
+    refine_2way(fine, fine_part, t.data(), ub, opt);
+    part = std::move(fine_part);
+  }
+  return 1;
+}
+
+// rb_recurse (src/partition/recursive.rs:61-131). Real arithmetic is f32 as
+// in the reference (sums in index order).
+int rb_recurse(const Graph& graph, size_t nparts, size_t offset, const std::vector<float>& tpwgts, const double* ub,
+               const Options& opt, SmallRng& rng, std::vector<Idx>& part) {
+  if (nparts == 1) {
+    for (size_t v = 0; v < graph.nvtxs; ++v) part[v] = (Idx)offset;
+    return 1;
+  }
+  if (graph.nvtxs <= nparts) {
+    for (size_t v = 0; v < graph.nvtxs; ++v) part[v] = (Idx)(offset + std::min(v, nparts - 1));
+    return 1;
+  }
+  const size_t k1 = nparts / 2, k2 = nparts - k1, ncon = graph.ncon;
+  std::vector<float> lw(ncon, 0.0f), rw(ncon, 0.0f);
+  for (size_t c = 0; c < ncon; ++c) {
+    for (size_t i = c; i < k1 * ncon; i += ncon) lw[c] += tpwgts[i];
+    for (size_t i = k1 * ncon + c; i < nparts * ncon; i += ncon) rw[c] += tpwgts[i];
+  }
+  const float total = lw[0] + rw[0];
+  std::vector<float> bis;
+  for (size_t c = 0; c < ncon; ++c) bis.push_back(lw[c] / total);
+  for (size_t c = 0; c < ncon; ++c) bis.push_back(rw[c] / total);
+  std::vector<Idx> bp;
+  int rc = multilevel_bisect(graph, bis.data(), ub, opt, rng, bp);
+  if (rc != 1) return rc;
+  std::vector<size_t> n2o0, n2o1;
+  Graph g0 = extract_subgraph(graph, bp.data(), 0, n2o0);
+  Graph g1 = extract_subgraph(graph, bp.data(), 1, n2o1);
+  std::vector<float> ltp, rtp;
+  for (size_t i = 0; i < k1 * ncon; ++i) ltp.push_back(tpwgts[i] / lw[0]);
+  for (size_t i = k1 * ncon; i < nparts * ncon; ++i) rtp.push_back(tpwgts[i] / rw[0]);
+  std::vector<Idx> sp0(g0.nvtxs, 0), sp1(g1.nvtxs, 0);
+  rc = rb_recurse(g0, k1, 0, ltp, ub, opt, rng, sp0);
+  if (rc != 1) return rc;
+  rc = rb_recurse(g1, k2, 0, rtp, ub, opt, rng, sp1);
+  if (rc != 1) return rc;
+  for (size_t i = 0; i < n2o0.size(); ++i) part[n2o0[i]] = sp0[i] + (Idx)offset;
+  for (size_t i = 0; i < n2o1.size(); ++i) part[n2o1[i]] = sp1[i] + (Idx)(offset + k1);
+  return 1;
+}
+
+// partition_recursive (src/partition/recursive.rs:12-57): one RNG for the
+// whole recursion, seeded with options.seed (entropy when 0).
+int partition_recursive(const Graph& graph, size_t nparts, const float* tpwgts, const float* ubvec, const Options& opt,
+                        std::vector<Idx>& part, Idx& obj) {
+  if (nparts < 2) return -2;
+  if (nparts > graph.nvtxs) return -2;
+  uint64_t seed;
+  if (opt.seed == 0) {
+    std::random_device rd;
+    seed = ((uint64_t)rd() << 32) ^ (uint64_t)rd();
+  } else {
+    seed = opt.seed;
+  }
+  SmallRng rng = SmallRng::seed_from_u64(seed);
+  const size_t ncon = graph.ncon;
+  std::vector<float> tp;
+  if (tpwgts) tp.assign(tpwgts, tpwgts + nparts * ncon);
+  else tp.assign(nparts * ncon, 1.0f / (float)nparts);
+  std::vector<double> ub(ncon);
+  for (size_t c = 0; c < ncon; ++c) ub[c] = ubvec ? (double)ubvec[c] : 1.0 + (double)opt.ufactor / 1000.0;
+  part.assign(graph.nvtxs, 0);
+  int rc = rb_recurse(graph, nparts, 0, tp, ub.data(), opt, rng, part);
+  if (rc != 1) return rc;
+  obj = graph.edge_cut(part.data());
+  return 1;
+}
+
 Graph make_graph(int64_t n, int64_t ncon, const Idx* xadj, const Idx* adjncy, const Idx* vwgt,
                  const Idx* adjwgt, const Idx* vsize) {
   Graph g;
@@ -1001,6 +1255,16 @@ Idx orc_fm_kway_refine(int64_t n, int64_t ncon, const Idx* xadj, const Idx* adjn
   return cut;
 }
 
+// fm_refine (src/refine/fm.rs:12-28) on a 2-way partition; returns the cut.
+Idx orc_fm2_refine(int64_t n, int64_t ncon, const Idx* xadj, const Idx* adjncy, const Idx* vwgt, const Idx* adjwgt,
+                   Idx* part, const double* tpwgts, const double* ubvec, int64_t niter) {
+  Graph g = make_graph(n, ncon, xadj, adjncy, vwgt, adjwgt, nullptr);
+  std::vector<Idx> p(part, part + n);
+  Idx cut = fm2_refine(g, p, tpwgts, ubvec, (size_t)niter);
+  std::memcpy(part, p.data(), n * sizeof(Idx));
+  return cut;
+}
+
 // Restated RMETIS_SetDefaultOptions (src/ffi/c_api.rs:15-23).
 int orc_SetDefaultOptions(Idx* options) {
   if (!options) return -2;
@@ -1050,6 +1314,31 @@ int orc_PartGraphKway_script(const Idx* nvtxs, const Idx* ncon, const Idx* xadj,
       stats_out[2 + 2 * i] = st.level_m[i];
     }
   }
+  return 1;
+}
+
+// Restated RMETIS_PartGraphRecursive (src/ffi/c_api.rs:27-53, c_partition_impl
+// :140-209 with kway = false).
+int orc_PartGraphRecursive(const Idx* nvtxs, const Idx* ncon, const Idx* xadj, const Idx* adjncy, const Idx* vwgt,
+                           const Idx* vsize, const Idx* adjwgt, const Idx* nparts, const float* tpwgts,
+                           const float* ubvec, const Idx* options, Idx* objval, Idx* part) {
+  if (!nvtxs || !ncon || !xadj || !adjncy || !nparts || !part) return -2;
+  int64_t n = *nvtxs, nc = *ncon, np = *nparts;
+  if (n <= 0 || nc <= 0 || np < 2) return -2;
+  int64_t ne = xadj[n];
+  if (ne < 0) return -2;
+  Options o;
+  if (options && options[0] != -1) o = from_raw(options);
+  if (validate_csr((size_t)n, (size_t)nc, xadj, (size_t)n + 1, adjncy, (size_t)ne, vwgt,
+                   vwgt ? (size_t)(n * nc) : 0, adjwgt, adjwgt ? (size_t)ne : 0) != 0)
+    return -2;
+  Graph g = make_graph(n, nc, xadj, adjncy, vwgt, adjwgt, vsize);
+  std::vector<Idx> best;
+  Idx obj = 0;
+  int rc = partition_recursive(g, (size_t)np, tpwgts, ubvec, o, best, obj);
+  if (rc != 1) return rc;
+  std::memcpy(part, best.data(), n * sizeof(Idx));
+  if (objval) *objval = obj;
   return 1;
 }
 

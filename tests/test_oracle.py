@@ -357,3 +357,56 @@ def test_kway_default_options_run_fm(oracle):     # c_api.rs:217-219: NULL optio
     xadj, adj = grid_graph(8, 8)
     rc, part, obj = oracle.part_graph_kway(xadj, adj, 4, options=None)
     assert rc == 1 and obj == oracle.edge_cut(xadj, adj, None, part)
+
+
+# ---- recursive.rs / fm.rs (recursive bisection, 2-way FM) -------------------
+
+def _recursive_options(seed, rtype=0):
+    import rmetis_b200 as rmb
+    o = rmb.Options.for_recursive()               # types.rs:99-106: MetisRb, Fm, ufactor 1
+    o.seed = seed
+    o.rtype = rmb.RType(rtype)
+    return o.c_array()
+
+
+def test_fm2_does_not_increase_cut(oracle):        # fm.rs:145-159
+    x = np.array([0, 2, 4, 6, 8, 10, 12]); a = np.array([1, 5, 0, 2, 1, 3, 2, 4, 3, 5, 4, 0])
+    part0 = [0, 0, 0, 1, 1, 1]
+    before = oracle.edge_cut(x, a, None, part0)
+    part, cut = oracle.fm2_refine(x, a, part0, [3.0, 3.0], [1.05], 10)
+    assert cut <= before and cut == oracle.edge_cut(x, a, None, part)
+
+
+def test_recursive_cycle4_k2(oracle):             # correctness.rs:130-137
+    rc, part, obj = oracle.part_graph_recursive(*CYCLE4, 2, options=_recursive_options(7))
+    assert rc == 1 and ((part >= 0) & (part < 2)).all()
+    assert _balanced(oracle, *CYCLE4, part, 2, 5)
+
+
+@pytest.mark.parametrize("k", [4, 8])
+def test_recursive_grid4x4(oracle, k):            # correctness.rs:139-153
+    xadj, adj = grid4x4()
+    rc, part, obj = oracle.part_graph_recursive(xadj, adj, k, options=_recursive_options(42))
+    assert rc == 1 and ((part >= 0) & (part < k)).all()
+    assert obj == oracle.edge_cut(xadj, adj, None, part)
+
+
+def test_recursive_deterministic(oracle):         # correctness.rs:189-197
+    xadj, adj = grid4x4()
+    r1 = oracle.part_graph_recursive(xadj, adj, 4, options=_recursive_options(99))
+    r2 = oracle.part_graph_recursive(xadj, adj, 4, options=_recursive_options(99))
+    assert r1[0] == 1 and r1[2] == r2[2] and (r1[1] == r2[1]).all()
+
+
+@pytest.mark.parametrize("rtype", [0, 1])
+def test_recursive_properties(oracle, rtype):
+    """Every part used, objval equals the edge cut, the error rules of
+    partition_recursive (recursive.rs:19-26), with either 2-way refinement."""
+    from rmetis_b200 import generators as G
+    x, a, v, w = G.grid3d(12, 10, 8, weights_seed=2)
+    for k in (2, 3, 7, 16):
+        rc, part, obj = oracle.part_graph_recursive(x, a, k, vwgt=v, adjwgt=w, options=_recursive_options(5, rtype))
+        assert rc == 1 and obj == oracle.edge_cut(x, a, w, part)
+        assert sorted(set(part.tolist())) == list(range(k))
+    assert oracle.part_graph_recursive(*CYCLE4, 10, options=_recursive_options(1))[0] == -2
+    assert oracle.part_graph_recursive(*CYCLE4, 1, options=_recursive_options(1))[0] == -2
