@@ -7,6 +7,7 @@
  *   RMETIS_SetDefaultOptions   replaces src/ffi/c_api.rs:15-23
  *   RMETIS_PartGraphKway       replaces src/ffi/c_api.rs:56-81 (+ c_partition_impl :140-209,
  *                              parse_options :211-222)
+ *   RMETIS_PartGraphRecursive  replaces src/ffi/c_api.rs:27-53 (same helpers)
  *
  * The k-way path computes on the GPU (CType Shem/Rm, IpType Grow/Random/MetisRb,
  * RType Greedy and Fm). Greedy is refined pass for pass as the reference does;
@@ -81,6 +82,24 @@ RMETIS_API int RMETIS_PartGraphKway(const idx_t *nvtxs, const idx_t *ncon, const
                          const idx_t *vwgt, const idx_t *vsize, const idx_t *adjwgt, const idx_t *nparts,
                          const real_t *tpwgts, const real_t *ubvec, const idx_t *options, idx_t *objval,
                          idx_t *part);
+
+/* Multilevel recursive bisection (src/ffi/c_api.rs:27-53 with
+ * src/partition/recursive.rs:12-187). Same arguments, ownership and return
+ * codes as RMETIS_PartGraphKway; the options are decoded the same way, and the
+ * reference's Options::for_recursive() (iptype MetisRb, rtype Fm, ufactor 1)
+ * is what its callers pass. The recursion, the f32 target arithmetic and the
+ * subgraph extraction follow the reference on the host; each bisection is a
+ * 2-way multilevel partition on the GPU (coarsening to 40 vertices, grow
+ * trials, refinement). Differences: rtype Fm refines a bisection with the
+ * k-way FM rule (positive-gain moves) rather than the reference's 2-way FM
+ * (src/refine/fm.rs, which also makes negative moves and rolls back), and
+ * bisection i runs with seed + i where the reference draws all bisections
+ * from one generator; partitions match the reference's in quality, not bit
+ * for bit. */
+RMETIS_API int RMETIS_PartGraphRecursive(const idx_t *nvtxs, const idx_t *ncon, const idx_t *xadj,
+                                         const idx_t *adjncy, const idx_t *vwgt, const idx_t *vsize,
+                                         const idx_t *adjwgt, const idx_t *nparts, const real_t *tpwgts,
+                                         const real_t *ubvec, const idx_t *options, idx_t *objval, idx_t *part);
 
 /* ---- GPU extensions ---------------------------------------------------- */
 

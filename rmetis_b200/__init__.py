@@ -19,7 +19,8 @@ from ._lib import F32P, F64P, I32P, I64P
 
 __all__ = [
     "CType", "IpType", "RType", "ObjType", "Options", "Graph", "PartitionResult", "MetisError", "InputError",
-    "OutOfMemoryError", "InternalError", "part_graph_kway", "set_default_options", "METIS_OK",
+    "OutOfMemoryError", "InternalError", "part_graph_kway", "part_graph_recursive", "set_default_options",
+    "METIS_OK",
     "METIS_ERROR_INPUT", "METIS_ERROR_MEMORY", "METIS_ERROR", "METIS_NOPTIONS",
 ]
 
@@ -332,6 +333,31 @@ def part_graph_kway(graph: Graph, nparts: int, tpwgts=None, ubvec=None, options:
                                           _p(graph.vwgt), _p(graph.vsize), _p(graph.adjwgt), ctypes.byref(npr),
                                           _p(tp, F32P), _p(ub, F32P), _p(opts), ctypes.byref(obj), _p(part))
     _raise_for(rc, "part_graph_kway")
+    return PartitionResult(part=part, objval=int(obj.value))
+
+
+def part_graph_recursive(graph: Graph, nparts: int, tpwgts=None, ubvec=None, options: Options | None = None
+                         ) -> PartitionResult:
+    """Multilevel recursive bisection (src/lib.rs part_graph_recursive,
+    src/partition/recursive.rs:12-187): the reference's recursion and target
+    arithmetic, each bisection a 2-way multilevel partition on the GPU. Pass
+    Options.for_recursive() for the reference's defaults of this call."""
+    options = options or Options()
+    if nparts < 2:
+        raise InputError(f"nparts must be >= 2, got {nparts}")
+    if nparts > graph.nvtxs:
+        raise InputError(f"nparts={nparts} > nvtxs={graph.nvtxs}")
+    opts = options.c_array()
+    part = np.zeros(graph.nvtxs, dtype=np.int32)
+    obj = ctypes.c_int32(0)
+    nv = ctypes.c_int32(graph.nvtxs); nc = ctypes.c_int32(graph.ncon); npr = ctypes.c_int32(nparts)
+    tp = None if tpwgts is None else np.ascontiguousarray(tpwgts, dtype=np.float32)
+    ub = None if ubvec is None else np.ascontiguousarray(ubvec, dtype=np.float32)
+    rc = _lib.load().RMETIS_PartGraphRecursive(ctypes.byref(nv), ctypes.byref(nc), _p(graph.xadj),
+                                               _p(graph.adjncy), _p(graph.vwgt), _p(graph.vsize), _p(graph.adjwgt),
+                                               ctypes.byref(npr), _p(tp, F32P), _p(ub, F32P), _p(opts),
+                                               ctypes.byref(obj), _p(part))
+    _raise_for(rc, "part_graph_recursive")
     return PartitionResult(part=part, objval=int(obj.value))
 
 

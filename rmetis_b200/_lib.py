@@ -18,6 +18,7 @@ VP = ctypes.c_void_p
 SIGNATURES = {
     "RMETIS_SetDefaultOptions": [I32P],
     "RMETIS_PartGraphKway": [I32P, I32P, I32P, I32P, I32P, I32P, I32P, I32P, F32P, F32P, I32P, I32P, I32P],
+    "RMETIS_PartGraphRecursive": [I32P, I32P, I32P, I32P, I32P, I32P, I32P, I32P, F32P, F32P, I32P, I32P, I32P],
     "RMETIS_GPU_PartGraphKwayDevice": [I32P, I32P, VP, VP, VP, VP, I32P, F32P, F32P, I32P, I32P, VP],
     "RMETIS_GPU_SetStream": [VP],
     "RMETIS_GPU_SetTuning": [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int],

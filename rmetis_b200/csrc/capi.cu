@@ -198,6 +198,195 @@ DGraph dgraph(HostCall& h, idx_t n, idx_t ncon, const idx_t* xadj, const idx_t* 
   return g;
 }
 
+// ---- recursive bisection (src/partition/recursive.rs:12-187) --------------
+// The recursion, the target arithmetic (f32, as the reference's Real) and the
+// subgraph extraction run on the host; every bisection with more than two
+// vertices and at least one edge is a 2-way multilevel partition on the GPU
+// (coarsening, grow trials and refinement of the engine).
+struct HostGraph {
+  int32_t n = 0;
+  int32_t ncon = 1;
+  std::vector<idx_t> xadj{0}, adj, vwgt, adjw;
+  bool has_vw = false, has_w = false;
+  idx_t vw(int32_t v, int c) const { return has_vw ? vwgt[(size_t)v * ncon + c] : 1; }
+};
+
+// Graph::extract_subgraph (src/graph/mod.rs:209-273).
+HostGraph extract_sub(const HostGraph& g, const std::vector<idx_t>& part, idx_t target, std::vector<int32_t>& n2o) {
+  n2o.clear();
+  for (int32_t v = 0; v < g.n; ++v)
+    if (part[v] == target) n2o.push_back(v);
+  std::vector<int32_t> o2n(g.n, -1);
+  for (size_t i = 0; i < n2o.size(); ++i) o2n[n2o[i]] = (int32_t)i;
+  HostGraph s;
+  s.n = (int32_t)n2o.size();
+  s.ncon = g.ncon;
+  s.has_vw = g.has_vw;
+  s.has_w = g.has_w;
+  s.xadj.assign((size_t)s.n + 1, 0);
+  for (int32_t i = 0; i < s.n; ++i) {
+    const int32_t old = n2o[i];
+    for (idx_t j = g.xadj[old]; j < g.xadj[old + 1]; ++j) {
+      const idx_t u = g.adj[j];
+      if (part[u] != target) continue;
+      s.adj.push_back(o2n[u]);
+      if (g.has_w) s.adjw.push_back(g.adjw[j]);
+    }
+    s.xadj[(size_t)i + 1] = (idx_t)s.adj.size();
+    if (g.has_vw)
+      for (int c = 0; c < g.ncon; ++c) s.vwgt.push_back(g.vwgt[(size_t)old * g.ncon + c]);
+  }
+  return s;
+}
+
+// multilevel_bisect (recursive.rs:133-187) on the GPU. A bisection without
+// edges has cut 0 whatever it does; it is split on the host in vertex order,
+// filling side 0 up to its target on constraint 0.
+void bisect(Engine& E, const HostGraph& g, const std::vector<float>& tp2, const real_t* ubvec, const KwayOptions& o,
+            uint64_t seed, std::vector<idx_t>& part) {
+  part.assign((size_t)g.n, 0);
+  if (g.n <= 2) {  // recursive.rs:141-144
+    for (int32_t v = 0; v < g.n; ++v) part[v] = v;
+    return;
+  }
+  if (g.xadj[g.n] == 0) {
+    double tot = 0;
+    for (int32_t v = 0; v < g.n; ++v) tot += g.vw(v, 0);
+    const double t0 = (double)tp2[0] * tot;
+    double w0 = 0;
+    for (int32_t v = 0; v < g.n; ++v) {
+      if (w0 + g.vw(v, 0) <= t0) {
+        w0 += g.vw(v, 0);
+      } else {
+        part[v] = 1;
+      }
+    }
+    return;
+  }
+  Arena::Mark mk = E.arena().mark();
+  struct Rewind {
+    Engine& E;
+    Arena::Mark m;
+    ~Rewind() { E.arena().reset_to(m); }
+  } rw{E, mk};
+  DGraph dg;
+  dg.n = g.n;
+  dg.m = g.xadj[g.n];
+  dg.ncon = g.ncon;
+  dg.xadj = upload(E, g.xadj.data(), (size_t)g.n + 1);
+  dg.adjncy = upload(E, g.adj.data(), (size_t)dg.m);
+  dg.adjwgt = g.has_w ? upload(E, g.adjw.data(), (size_t)dg.m) : nullptr;
+  dg.vwgt = g.has_vw ? upload(E, g.vwgt.data(), (size_t)g.n * g.ncon) : nullptr;
+  idx_t* d_part = E.arena().alloc<idx_t>((size_t)g.n);
+  KwayOptions ob = o;
+  ob.seed = seed;
+  ob.ncuts = 1;
+  ob.parallel_attempts = 0;
+  int32_t obj = 0;
+  E.partition_kway(dg, 2, tp2.data(), ubvec, ob, d_part, &obj, nullptr);
+  download(E, part.data(), d_part, (size_t)g.n);
+  RMB_CUDA(cudaStreamSynchronize(E.stream()));
+}
+
+// rb_recurse (recursive.rs:61-131). The reference draws every bisection's
+// random choices from one generator; here bisection i (in the recursion's
+// order) runs with seed + i (0 stays 0: an entropy seed per bisection).
+void rb_recurse(Engine& E, const HostGraph& g, int32_t nparts, int32_t offset, const std::vector<float>& tp,
+                const real_t* ubvec, const KwayOptions& o, uint64_t& counter, std::vector<idx_t>& part) {
+  if (nparts == 1) {
+    for (int32_t v = 0; v < g.n; ++v) part[v] = offset;
+    return;
+  }
+  if (g.n <= nparts) {
+    for (int32_t v = 0; v < g.n; ++v) part[v] = offset + std::min(v, nparts - 1);
+    return;
+  }
+  const int32_t k1 = nparts / 2, k2 = nparts - k1, nc = g.ncon;
+  std::vector<float> lw(nc, 0.0f), rw(nc, 0.0f);
+  for (int c = 0; c < nc; ++c) {
+    for (int32_t i = c; i < k1 * nc; i += nc) lw[c] += tp[i];
+    for (int32_t i = k1 * nc + c; i < nparts * nc; i += nc) rw[c] += tp[i];
+  }
+  const float total = lw[0] + rw[0];
+  std::vector<float> bis;
+  for (int c = 0; c < nc; ++c) bis.push_back(lw[c] / total);
+  for (int c = 0; c < nc; ++c) bis.push_back(rw[c] / total);
+  std::vector<idx_t> bp;
+  const uint64_t seed = o.seed == 0 ? 0 : o.seed + counter;
+  ++counter;
+  bisect(E, g, bis, ubvec, o, seed, bp);
+  std::vector<int32_t> n2o0, n2o1;
+  HostGraph g0 = extract_sub(g, bp, 0, n2o0);
+  HostGraph g1 = extract_sub(g, bp, 1, n2o1);
+  std::vector<float> ltp, rtp;
+  for (int32_t i = 0; i < k1 * nc; ++i) ltp.push_back(tp[i] / lw[0]);
+  for (int32_t i = k1 * nc; i < nparts * nc; ++i) rtp.push_back(tp[i] / rw[0]);
+  std::vector<idx_t> sp0((size_t)g0.n, 0), sp1((size_t)g1.n, 0);
+  rb_recurse(E, g0, k1, 0, ltp, ubvec, o, counter, sp0);
+  rb_recurse(E, g1, k2, 0, rtp, ubvec, o, counter, sp1);
+  for (size_t i = 0; i < n2o0.size(); ++i) part[n2o0[i]] = sp0[i] + offset;
+  for (size_t i = 0; i < n2o1.size(); ++i) part[n2o1[i]] = sp1[i] + offset + k1;
+}
+
+int recursive_host(const idx_t* nvtxs, const idx_t* ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
+                   const idx_t* adjwgt, const idx_t* nparts, const real_t* tpwgts, const real_t* ubvec,
+                   const idx_t* options, idx_t* objval, idx_t* part) {
+  // Mandatory pointers and scalar checks (src/ffi/c_api.rs:157-167).
+  if (!nvtxs || !ncon || !xadj || !adjncy || !nparts || !part) return METIS_ERROR_INPUT;
+  const int32_t n = *nvtxs, nc = *ncon, np = *nparts;
+  if (n <= 0 || nc <= 0 || np < 2) return METIS_ERROR_INPUT;
+  if (xadj[0] != 0 || xadj[n] < 0) return METIS_ERROR_INPUT;
+  if (nc > 8) return METIS_ERROR_INPUT;
+  const int64_t ne = xadj[n];
+  KwayOptions o = parse_options(options);
+  apply_tuning(o);
+  Engine& E = engine_for_current_device();
+  std::lock_guard<std::mutex> lk(E.mu);
+  {
+    // validate_csr (src/graph/validate.rs:16-142) on the device, as Graph::new does.
+    Arena::Mark mk = E.arena().mark();
+    struct Rewind {
+      Engine& E;
+      Arena::Mark m;
+      ~Rewind() { E.arena().reset_to(m); }
+    } rw{E, mk};
+    DGraph g;
+    g.n = n;
+    g.m = ne;
+    g.ncon = nc;
+    g.xadj = upload(E, xadj, (size_t)n + 1);
+    g.adjncy = upload(E, adjncy, (size_t)ne);
+    g.vwgt = upload(E, vwgt, (size_t)n * nc);
+    g.adjwgt = upload(E, adjwgt, (size_t)ne);
+    if (validate_device(g, E.arena(), E.stream(), E.host_scratch()) != 0)
+      throw Error(METIS_ERROR_INPUT, "graph failed validation");
+  }
+  if (np > n) return METIS_ERROR_INPUT;  // recursive.rs:22-26
+  HostGraph g;
+  g.n = n;
+  g.ncon = nc;
+  g.xadj.assign(xadj, xadj + n + 1);
+  g.adj.assign(adjncy, adjncy + ne);
+  g.has_vw = vwgt != nullptr;
+  g.has_w = adjwgt != nullptr;
+  if (vwgt) g.vwgt.assign(vwgt, vwgt + (size_t)n * nc);
+  if (adjwgt) g.adjw.assign(adjwgt, adjwgt + ne);
+  std::vector<float> tp;
+  if (tpwgts) tp.assign(tpwgts, tpwgts + (size_t)np * nc);
+  else tp.assign((size_t)np * nc, 1.0f / (float)np);  // recursive.rs:38-43
+  std::vector<idx_t> out((size_t)n, 0);
+  uint64_t counter = 0;
+  rb_recurse(E, g, np, 0, tp, ubvec, o, counter, out);
+  // edge_cut (src/graph/mod.rs:123-137): i32 sum over both directions, / 2.
+  uint32_t cut = 0;
+  for (int32_t v = 0; v < n; ++v)
+    for (idx_t j = xadj[v]; j < xadj[v + 1]; ++j)
+      if (out[adjncy[j]] != out[v]) cut += (uint32_t)(adjwgt ? adjwgt[j] : 1);
+  std::memcpy(part, out.data(), sizeof(idx_t) * (size_t)n);
+  if (objval) *objval = (idx_t)cut / 2;
+  return METIS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -230,6 +419,16 @@ int RMETIS_PartGraphKway(const idx_t* nvtxs, const idx_t* ncon, const idx_t* xad
   return guarded([&] {
     return kway_host(nvtxs, ncon, xadj, adjncy, vwgt, adjwgt, nparts, tpwgts, ubvec, options, objval, part,
                      nullptr);
+  });
+}
+
+int RMETIS_PartGraphRecursive(const idx_t* nvtxs, const idx_t* ncon, const idx_t* xadj, const idx_t* adjncy,
+                              const idx_t* vwgt, const idx_t* vsize, const idx_t* adjwgt, const idx_t* nparts,
+                              const real_t* tpwgts, const real_t* ubvec, const idx_t* options, idx_t* objval,
+                              idx_t* part) {
+  (void)vsize;  // carried by the reference's subgraphs but never read
+  return guarded([&] {
+    return recursive_host(nvtxs, ncon, xadj, adjncy, vwgt, adjwgt, nparts, tpwgts, ubvec, options, objval, part);
   });
 }
 

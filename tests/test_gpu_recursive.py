@@ -1,0 +1,103 @@
+"""Recursive bisection (RMETIS_PartGraphRecursive, src/partition/recursive.rs)
+through the C ABI: the reference's own cases (tests/correctness.rs:130-153,
+189-197), validity, objval, determinism and error codes on larger graphs, and
+the cut against the oracle's restatement of the reference (each bisection on
+the GPU is a 2-way multilevel partition with the engine's matching, grow
+trials and refinement, so partitions are compared by quality)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from rmetis_b200 import generators as G
+
+pytestmark = pytest.mark.gpu
+
+CYCLE4 = (np.array([0, 2, 4, 6, 8], np.int32), np.array([1, 3, 0, 2, 1, 3, 0, 2], np.int32))
+
+
+def _opts(seed, rtype=None):
+    import rmetis_b200 as rmb
+    o = rmb.Options.for_recursive()           # iptype MetisRb, rtype Fm, ufactor 1 (src/types.rs:99-106)
+    o.seed = seed
+    if rtype is not None:
+        o.rtype = rtype
+    return o
+
+
+def _grid4x4():
+    return G.grid2d(4, 4)
+
+
+def _c_abi(rmb, x, a, k, options, vwgt=None, adjwgt=None):
+    lib = rmb._lib.load()
+    I32P = ctypes.POINTER(ctypes.c_int32)
+    n = len(x) - 1
+    keep = [np.ascontiguousarray(t, np.int32) if t is not None else None for t in (x, a, vwgt, adjwgt, options)]
+    p = lambda t: None if t is None else t.ctypes.data_as(I32P)
+    part = np.full(n, -7, np.int32)
+    obj = ctypes.c_int32(-1)
+    nv, nc, npr = ctypes.c_int32(n), ctypes.c_int32(1), ctypes.c_int32(k)
+    rc = lib.RMETIS_PartGraphRecursive(ctypes.byref(nv), ctypes.byref(nc), p(keep[0]), p(keep[1]), p(keep[2]),
+                                       None, p(keep[3]), ctypes.byref(npr), None, None, p(keep[4]),
+                                       ctypes.byref(obj), part.ctypes.data_as(I32P))
+    return rc, part, obj.value
+
+
+def test_recursive_reference_cases(rmb, oracle):
+    import rmetis_b200 as rmb_mod
+    g = rmb_mod.Graph.new_unweighted(4, *CYCLE4)
+    r = rmb_mod.part_graph_recursive(g, 2, options=_opts(7))               # correctness.rs:130-137
+    assert ((r.part >= 0) & (r.part < 2)).all()
+    pw = np.bincount(r.part, minlength=2)
+    assert (pw <= 4 * 1.005 / 2 + 1.0).all()                                 # correctness.rs:68-79, ufactor 5
+    x, a = _grid4x4()
+    g16 = rmb_mod.Graph.new_unweighted(16, x, a)
+    for k in (4, 8):                                                         # correctness.rs:139-153
+        r = rmb_mod.part_graph_recursive(g16, k, options=_opts(42))
+        assert ((r.part >= 0) & (r.part < k)).all() and r.objval == oracle.edge_cut(x, a, None, r.part)
+    r1 = rmb_mod.part_graph_recursive(g16, 4, options=_opts(99))              # correctness.rs:189-197
+    r2 = rmb_mod.part_graph_recursive(g16, 4, options=_opts(99))
+    assert r1.objval == r2.objval and (r1.part == r2.part).all()
+
+
+def test_recursive_errors(rmb):
+    o = _opts(1).c_array()
+    assert _c_abi(rmb, *CYCLE4, 10, o)[0] == -2                              # nparts > nvtxs (recursive.rs:22-26)
+    assert _c_abi(rmb, *CYCLE4, 1, o)[0] == -2                               # nparts < 2 (c_api.rs:167)
+    bad = (np.array([0, 2, 4, 6, 8]), np.array([1, 3, 0, 2, 1, 3, 0, 0]))   # asymmetric: validation
+    assert _c_abi(rmb, *bad, 2, o)[0] == -2
+
+
+CASES = [
+    ("grid2d_30", lambda: G.grid2d(30, 30) + (None, None), 4),
+    ("grid2d_30_k7", lambda: G.grid2d(30, 30) + (None, None), 7),
+    ("grid3d_w", lambda: G.grid3d(12, 10, 8, weights_seed=2), 16),
+    ("rgg_3k", lambda: (lambda r: (r[0], r[1], None, r[2]))(G.rgg2d(3000, 9)), 5),
+]
+
+
+@pytest.mark.parametrize("rtype", ["greedy", "fm"])
+def test_recursive_valid_deterministic_and_quality(rmb, oracle, rtype, capsys):
+    import rmetis_b200 as rmb_mod
+    rt = rmb_mod.RType.Greedy if rtype == "greedy" else rmb_mod.RType.Fm
+    gpu_sum = ref_sum = 0
+    for name, make, k in CASES:
+        x, a, v, w = make()
+        n = len(x) - 1
+        g = rmb_mod.Graph(n, 1, x, a, vwgt=v, adjwgt=w)
+        for seed in (3, 4, 5):
+            o = _opts(seed, rt)
+            r = rmb_mod.part_graph_recursive(g, k, options=o)
+            assert ((r.part >= 0) & (r.part < k)).all()
+            assert r.objval == oracle.edge_cut(x, a, w, r.part)
+            assert len(set(r.part.tolist())) == k
+            again = rmb_mod.part_graph_recursive(g, k, options=o)
+            assert again.objval == r.objval and (again.part == r.part).all()
+            rc, _, robj = oracle.part_graph_recursive(x, a, k, vwgt=v, adjwgt=w, options=o.c_array())
+            assert rc == 1
+            gpu_sum += r.objval
+            ref_sum += robj
+    with capsys.disabled():
+        print(f"\nrecursive {rtype}: GPU summed cut {gpu_sum}, oracle {ref_sum}, ratio {gpu_sum / ref_sum:.3f}")
+    assert gpu_sum <= 2.0 * ref_sum, (gpu_sum, ref_sum)
