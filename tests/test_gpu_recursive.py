@@ -100,4 +100,5 @@ def test_recursive_valid_deterministic_and_quality(rmb, oracle, rtype, capsys):
             ref_sum += robj
     with capsys.disabled():
         print(f"\nrecursive {rtype}: GPU summed cut {gpu_sum}, oracle {ref_sum}, ratio {gpu_sum / ref_sum:.3f}")
-    assert gpu_sum <= 2.0 * ref_sum, (gpu_sum, ref_sum)
+    # Measured on a B200: greedy 17,451 vs 22,990 (0.76), fm 11,453 vs 18,203 (0.63).
+    assert gpu_sum <= 1.05 * ref_sum, (gpu_sum, ref_sum)
