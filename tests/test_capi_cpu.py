@@ -38,7 +38,11 @@ def test_set_default_options_null(rmb):
     assert rmb._lib.load().RMETIS_SetDefaultOptions(None) == -2
 
 
-def _call(lib, n, ncon, xadj, adj, nparts, part, options=None, vwgt=None, adjwgt=None, null=()):
+ENTRIES = ["RMETIS_PartGraphKway", "RMETIS_PartGraphRecursive"]  # c_api.rs:56-81 and :27-53
+
+
+def _call(lib, n, ncon, xadj, adj, nparts, part, options=None, vwgt=None, adjwgt=None, null=(),
+          entry="RMETIS_PartGraphKway"):
     I32P = ctypes.POINTER(ctypes.c_int32)
     nv = ctypes.c_int32(n); nc = ctypes.c_int32(ncon); npr = ctypes.c_int32(nparts)
     p = lambda a: None if a is None else np.ascontiguousarray(a, np.int32).ctypes.data_as(I32P)
@@ -47,27 +51,30 @@ def _call(lib, n, ncon, xadj, adj, nparts, part, options=None, vwgt=None, adjwgt
                 objval=None, part=part.ctypes.data_as(I32P))
     for k in null:
         args[k] = None
-    return lib.RMETIS_PartGraphKway(*args.values())
+    return getattr(lib, entry)(*args.values())
 
 
+@pytest.mark.parametrize("entry", ENTRIES)
 @pytest.mark.parametrize("missing", ["nvtxs", "ncon", "xadj", "adjncy", "nparts", "part"])
-def test_null_required_pointer_is_input_error(rmb, missing):
+def test_null_required_pointer_is_input_error(rmb, missing, entry):
     xadj = np.array([0, 2, 4, 6, 8]); adj = np.array([1, 3, 0, 2, 1, 3, 0, 2])
     part = np.zeros(4, np.int32)
-    assert _call(rmb._lib.load(), 4, 1, xadj, adj, 2, part, greedy_options(), null=(missing,)) == -2
+    assert _call(rmb._lib.load(), 4, 1, xadj, adj, 2, part, greedy_options(), null=(missing,), entry=entry) == -2
 
 
+@pytest.mark.parametrize("entry", ENTRIES)
 @pytest.mark.parametrize("n,ncon,nparts", [(0, 1, 2), (4, 0, 2), (4, 1, 1), (4, 1, -3)])
-def test_scalar_input_errors(rmb, n, ncon, nparts):
+def test_scalar_input_errors(rmb, n, ncon, nparts, entry):
     xadj = np.array([0, 2, 4, 6, 8]); adj = np.array([1, 3, 0, 2, 1, 3, 0, 2])
     part = np.zeros(4, np.int32)
-    assert _call(rmb._lib.load(), n, ncon, xadj, adj, nparts, part, greedy_options()) == -2
+    assert _call(rmb._lib.load(), n, ncon, xadj, adj, nparts, part, greedy_options(), entry=entry) == -2
 
 
-def test_bad_xadj0_is_input_error(rmb):
+@pytest.mark.parametrize("entry", ENTRIES)
+def test_bad_xadj0_is_input_error(rmb, entry):
     part = np.zeros(4, np.int32)
     assert _call(rmb._lib.load(), 4, 1, np.array([1, 2, 4, 6, 8]), np.array([1, 3, 0, 2, 1, 3, 0, 2]), 2, part,
-                 greedy_options()) == -2
+                 greedy_options(), entry=entry) == -2
 
 
 def test_options_codec_roundtrip(rmb):
