@@ -1,7 +1,7 @@
 """ctypes wrapper over the oracle (the CPU restatement in ref_kway.cpp).
 
 Test infrastructure only: tests/, __graft_entry__.smoke() and bench.py's CPU
-legs use it as the checker. The product (rmetis_b200) never imports it.
+legs use it to check the CUDA path. The product (rmetis_b200) never imports it.
 """
 from __future__ import annotations
 

@@ -1,7 +1,7 @@
 // Oracle: CPU restatement of rmetis's multilevel k-way hot path.
 //
-// TEST INFRASTRUCTURE ONLY. This file is the checker for the CUDA path in
-// rmetis_b200/. Only tests/, __graft_entry__.smoke() and bench.py's
+// TEST INFRASTRUCTURE ONLY. This file is the CPU reference that the CUDA path in
+// rmetis_b200/ is compared with. Only tests/, __graft_entry__.smoke() and bench.py's
 // cpu_baseline / --impl reference legs load it; the product never links it.
 //
 // It restates, function by function and quirks included, the Rust reference
