@@ -43,7 +43,7 @@ def lib():
         _lib.orc_rng_gen_range.restype = ctypes.c_uint64
         _lib.orc_fm2_refine.restype = ctypes.c_int32
         for name in ("orc_validate_csr", "orc_SetDefaultOptions", "orc_PartGraphKway",
-                     "orc_PartGraphKway_script", "orc_PartGraphRecursive"):
+                     "orc_PartGraphKway_script", "orc_PartGraphRecursive", "orc_NodeND"):
             getattr(_lib, name).restype = ctypes.c_int
     return _lib
 
@@ -254,6 +254,20 @@ def part_graph_recursive(xadj, adjncy, nparts, vwgt=None, adjwgt=None, ncon=1, t
                                       _p(vwgt, I32P), None, _p(adjwgt, I32P), ctypes.byref(npr), _p(tp, F32P),
                                       _p(ub, F32P), _p(op, I32P), ctypes.byref(obj), _p(part, I32P))
     return rc, part, int(obj.value)
+
+
+def node_nd(xadj, adjncy, vwgt=None, options=None):
+    """Restated RMETIS_NodeND (src/ffi/c_api.rs:85-132, src/partition/nd.rs).
+    Returns (rc, perm, iperm)."""
+    xadj = _i32(xadj); adjncy = _i32(adjncy); vwgt = _i32(vwgt)
+    n = len(xadj) - 1
+    perm = np.zeros(n, dtype=np.int32)
+    iperm = np.zeros(n, dtype=np.int32)
+    nv = ctypes.c_int32(n)
+    op = None if options is None else _i32(options)
+    rc = lib().orc_NodeND(ctypes.byref(nv), _p(xadj, I32P), _p(adjncy, I32P), _p(vwgt, I32P), _p(op, I32P),
+                          _p(perm, I32P), _p(iperm, I32P))
+    return rc, perm, iperm
 
 
 def part_graph_kway(xadj, adjncy, nparts, vwgt=None, adjwgt=None, ncon=1, tpwgts=None, ubvec=None,

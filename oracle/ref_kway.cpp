@@ -1076,6 +1076,83 @@ int partition_recursive(const Graph& graph, size_t nparts, const float* tpwgts, 
   return 1;
 }
 
+// ---------------------------------------------------------------------------
+// Nested dissection (src/partition/nd.rs:15-110, src/separator/mod.rs:9-61).
+// ---------------------------------------------------------------------------
+
+// find_node_separator (src/separator/mod.rs:9-61): a recursive bisection with
+// targets (0.5, 0.5) and ub 1.05 (seeded from options.seed, not from the
+// caller's generator), then every vertex of the lighter side (constraint 0)
+// with a neighbour across becomes a separator vertex.
+void find_node_separator(const Graph& g, const Options& opt, std::vector<size_t>& left, std::vector<size_t>& right,
+                         std::vector<size_t>& sep) {
+  const float tp[2] = {0.5f, 0.5f};
+  const float ub[1] = {1.05f};
+  std::vector<Idx> part;
+  Idx obj = 0;
+  if (partition_recursive(g, 2, tp, ub, opt, part, obj) != 1) {
+    part.assign(g.nvtxs, 0);                                   // separator/mod.rs:22-27
+    for (size_t v = 0; v < g.nvtxs; ++v) part[v] = v < g.nvtxs / 2 ? 0 : 1;
+  }
+  std::vector<Idx> pw = g.partition_weights(part.data(), 2);
+  const Idx smaller = pw[0] <= pw[g.ncon] ? 0 : 1;
+  std::vector<char> in_sep(g.nvtxs, 0);
+  for (size_t v = 0; v < g.nvtxs; ++v) {
+    if (part[v] != smaller) continue;
+    for (Idx j = g.xadj[v]; j < g.xadj[v + 1]; ++j)
+      if (part[g.adjncy[j]] != part[v]) { in_sep[v] = 1; break; }
+  }
+  left.clear(); right.clear(); sep.clear();
+  for (size_t v = 0; v < g.nvtxs; ++v) {
+    if (in_sep[v]) sep.push_back(v);
+    else if (part[v] == smaller) left.push_back(v);
+    else right.push_back(v);
+  }
+}
+
+// nd_recurse (src/partition/nd.rs:51-110): small graphs (<= 100 vertices) and
+// degenerate separators (>= n/2) are numbered in order; otherwise the left
+// side, then the right side, then the separator.
+void nd_recurse(const Graph& g, const std::vector<size_t>& orig, const Options& opt, std::vector<Idx>& perm,
+                size_t& counter) {
+  const size_t n = g.nvtxs;
+  if (n <= 100) {
+    for (size_t o : orig) perm[o] = (Idx)counter++;
+    return;
+  }
+  std::vector<size_t> left, right, sep;
+  find_node_separator(g, opt, left, right, sep);
+  if (sep.size() >= n / 2) {
+    for (size_t o : orig) perm[o] = (Idx)counter++;
+    return;
+  }
+  std::vector<Idx> side(n, 2);
+  for (size_t v : left) side[v] = 0;
+  for (size_t v : right) side[v] = 1;
+  for (Idx s = 0; s < 2; ++s) {
+    if ((s == 0 ? left : right).empty()) continue;
+    std::vector<size_t> n2o;
+    Graph sub = extract_subgraph(g, side.data(), s, n2o);
+    std::vector<size_t> sub_orig(n2o.size());
+    for (size_t i = 0; i < n2o.size(); ++i) sub_orig[i] = orig[n2o[i]];
+    nd_recurse(sub, sub_orig, opt, perm, counter);
+  }
+  for (size_t v : sep) perm[orig[v]] = (Idx)counter++;
+}
+
+// node_nd (src/partition/nd.rs:15-43): perm[v] = new position of v,
+// iperm its inverse.
+void node_nd(const Graph& g, const Options& opt, std::vector<Idx>& perm, std::vector<Idx>& iperm) {
+  const size_t n = g.nvtxs;
+  perm.assign(n, 0);
+  iperm.assign(n, 0);
+  std::vector<size_t> orig(n);
+  for (size_t v = 0; v < n; ++v) orig[v] = v;
+  size_t counter = 0;
+  nd_recurse(g, orig, opt, perm, counter);
+  for (size_t v = 0; v < n; ++v) iperm[(size_t)perm[v]] = (Idx)v;
+}
+
 Graph make_graph(int64_t n, int64_t ncon, const Idx* xadj, const Idx* adjncy, const Idx* vwgt,
                  const Idx* adjwgt, const Idx* vsize) {
   Graph g;
@@ -1339,6 +1416,27 @@ int orc_PartGraphRecursive(const Idx* nvtxs, const Idx* ncon, const Idx* xadj, c
   if (rc != 1) return rc;
   std::memcpy(part, best.data(), n * sizeof(Idx));
   if (objval) *objval = obj;
+  return 1;
+}
+
+// Restated RMETIS_NodeND (src/ffi/c_api.rs:85-132): one constraint, vwgt
+// optional, perm and iperm written.
+int orc_NodeND(const Idx* nvtxs, const Idx* xadj, const Idx* adjncy, const Idx* vwgt, const Idx* options, Idx* perm,
+               Idx* iperm) {
+  if (!nvtxs || !xadj || !adjncy || !perm || !iperm) return -2;
+  int64_t n = *nvtxs;
+  if (n <= 0) return -2;
+  int64_t ne = xadj[n];
+  if (ne < 0) return -2;
+  Options o;
+  if (options && options[0] != -1) o = from_raw(options);
+  if (validate_csr((size_t)n, 1, xadj, (size_t)n + 1, adjncy, (size_t)ne, vwgt, vwgt ? (size_t)n : 0, nullptr, 0) != 0)
+    return -2;
+  Graph g = make_graph(n, 1, xadj, adjncy, vwgt, nullptr, nullptr);
+  std::vector<Idx> p, ip;
+  node_nd(g, o, p, ip);
+  std::memcpy(perm, p.data(), n * sizeof(Idx));
+  std::memcpy(iperm, ip.data(), n * sizeof(Idx));
   return 1;
 }
 

@@ -410,3 +410,56 @@ def test_recursive_properties(oracle, rtype):
         assert sorted(set(part.tolist())) == list(range(k))
     assert oracle.part_graph_recursive(*CYCLE4, 10, options=_recursive_options(1))[0] == -2
     assert oracle.part_graph_recursive(*CYCLE4, 1, options=_recursive_options(1))[0] == -2
+
+
+# ---- nd.rs / separator (nested dissection) ----------------------------------
+
+def _nd_valid(n, perm, iperm):                    # correctness.rs:81-94
+    assert len(perm) == n and len(iperm) == n
+    assert sorted(perm.tolist()) == list(range(n))
+    assert all(perm[iperm[v]] == v for v in range(n))
+
+
+def _default_options(seed):
+    import rmetis_b200 as rmb
+    o = rmb.Options()
+    o.seed = seed
+    return o.c_array()
+
+
+def test_nd_path10(oracle):                       # nd.rs:115-150
+    n = 10
+    x = [0]; a = []
+    for v in range(n):
+        if v > 0:
+            a.append(v - 1)
+        if v < n - 1:
+            a.append(v + 1)
+        x.append(len(a))
+    rc, perm, iperm = oracle.node_nd(np.array(x), np.array(a), options=_default_options(42))
+    assert rc == 1
+    _nd_valid(n, perm, iperm)
+
+
+def test_nd_cycle4_and_grid4x4(oracle):           # correctness.rs:159-176
+    rc, perm, iperm = oracle.node_nd(*CYCLE4, options=_default_options(1))
+    assert rc == 1
+    _nd_valid(4, perm, iperm)
+    xadj, adj = grid4x4()
+    rc, perm, iperm = oracle.node_nd(xadj, adj, options=_default_options(42))
+    assert rc == 1
+    _nd_valid(16, perm, iperm)
+
+
+def test_nd_separators_on_a_larger_grid(oracle):
+    """A 30x30 grid (900 > 100 vertices) goes through separators: still a
+    permutation, the same for the same seed, and the last positions hold the
+    top-level separator, which splits the grid."""
+    xadj, adj = grid_graph(30, 30)
+    rc, perm, iperm = oracle.node_nd(xadj, adj, options=_default_options(3))
+    assert rc == 1
+    _nd_valid(900, perm, iperm)
+    rc2, perm2, _ = oracle.node_nd(xadj, adj, options=_default_options(3))
+    assert (perm2 == perm).all()
+    assert (perm != np.arange(900)).any()    # separators moved to the end, not the plain order
+    assert oracle.node_nd(np.array([0, 1, 1, 0, 0]), np.array([1]))[0] == -2   # asymmetric: validation
