@@ -176,49 +176,81 @@ def cpu_baseline(workload: str, graph=None):
     dt = time.perf_counter() - t0
     assert rc == 1
     return {"value": len(a) / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{desc} (n={len(x) - 1}, m={len(a)}), 1 partition, {dt:.2f} s, cut {obj}"}
+            "sample": f"{desc} (n={len(x) - 1}, m={len(a)}), 1 partition, {dt:.2f} s, cut {obj}", "objval": obj}
 
 
 def run_reference(args):
-    """--impl reference: the oracle on all host cores (independent partitions
-    of a bounded sample in parallel threads; the reference's only parallel
-    axis is independent attempts)."""
+    """--impl reference: the oracle (CPU restatement of the reference's path)
+    on all host cores. The reference has no parallelism inside one partition
+    (rayon is declared but unused); its only parallel axis is independent
+    attempts (src/partition/kway.rs:54). So every timed step runs one
+    partition of the configured workload itself (the full graph, same k,
+    options and seed) in each of `cores` threads, and value = cores * m /
+    step time. Warm-up steps (untimed) run one partition of the bounded
+    sample per thread, so that the whole run stays within a few minutes."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from oracle import oracle as O
-    build, desc = CPU_SAMPLE[args.workload]
+    build, k, seed, desc = WORKLOADS[args.workload]
     x, a, v, w = build()
-    k, seed = WORKLOADS[args.workload][1], WORKLOADS[args.workload][2]
+    wx, wa, wv, ww = CPU_SAMPLE[args.workload][0]()
     threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
     O.lib()
+    objs = []
 
-    def one(i):
-        rc, _, obj = O.part_graph_kway(x, a, k, vwgt=v, adjwgt=w, options=kway_options(seed + i))
+    def one(graph):
+        gx, ga, gv, gw = graph
+        rc, _, obj = O.part_graph_kway(gx, ga, k, vwgt=gv, adjwgt=gw, options=kway_options(seed))
         assert rc == 1
         return obj
 
     times = []
     with cf.ThreadPoolExecutor(max_workers=threads) as ex:
         for step in range(args.warmup + args.steps):
+            graph = (wx, wa, wv, ww) if step < args.warmup else (x, a, v, w)
             t0 = time.perf_counter()
-            list(ex.map(one, range(threads)))
+            res = list(ex.map(one, [graph] * threads))
             dt = time.perf_counter() - t0
             if step >= args.warmup:
                 times.append(dt)
+                objs.append(res[0])
     ms = 1000.0 * statistics.mean(times)
     value = threads * len(a) / (ms / 1000.0)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": {"workload": WORKLOADS[args.workload][3].replace("Greedy", "Fm" if RTYPE["code"] == 0
-                                                                        else "Greedy"),
-                       "sample": desc, "n": len(x) - 1, "m": len(a), "rtype": RTYPE["name"]},
+            "config": _config(args.workload, len(x) - 1, len(a), k, args.gpus),
+            "objval": int(objs[0]),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{desc}: {threads} independent partitions per step in {threads} threads"},
+                             "sample": f"the workload itself (n={len(x) - 1}, m={len(a)}): {threads} independent "
+                                       f"partitions (same seed) per step in {threads} threads; warm-up steps on "
+                                       f"{CPU_SAMPLE[args.workload][1]}"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     line["repro"] = _repro()
     print(json.dumps(line))
+
+
+def _config(workload, n, m, k, world):
+    """The config object both arms print (identical for the same workload)."""
+    desc = WORKLOADS[workload][3]
+    if RTYPE["name"] == "fm":
+        desc = desc.replace("Greedy", "Fm")
+    return {"workload": desc, "name": workload, "n": n, "m": m, "nparts": k, "rtype": RTYPE["name"],
+            "parallelism": "replicas" if world > 1 else "single"}
+
+
+def balance_summary(x, v, part, k, ufactor=30):
+    """max over parts of pw / t (1.0 = exactly on target) and the largest
+    pw - floor(t * ub), the reference's feasibility limit (<= 0: within),
+    ncon = 1, computed with numpy."""
+    n = len(x) - 1
+    vw = np.ones(n, np.int64) if v is None else np.asarray(v, np.int64)
+    pw = np.bincount(np.asarray(part, np.int64), weights=vw, minlength=k).astype(np.int64)
+    t = float(vw.sum()) / k
+    lim = np.floor(t * (1.0 + ufactor / 1000.0))
+    return {"max_imbalance": float(pw.max() / t), "max_overshoot": int(pw.max() - lim),
+            "within_ufactor": bool(pw.max() <= lim)}
 
 
 # ---------------------------------------------------------------------------
@@ -704,8 +736,9 @@ def main():
     bytes_k = (ctypes.c_double * nprof)()
     lib.RMETIS_GPU_GetProfile(launches, ms_k, bytes_k, nprof + 1)
     launches_before = launches[nprof]
-    lib.RMETIS_GPU_SetProfiling(1)
 
+    # Timed steps: per-launch profiling off, so the step time carries no
+    # profiler events.
     sampler = ClockSampler(gpu_id_for(local_rank))
     sampler.start()
     time.sleep(0.3)
@@ -730,9 +763,31 @@ def main():
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     ms_local = float(np.mean(step_ms))
     lib.RMETIS_GPU_GetProfile(launches, ms_k, bytes_k, nprof + 1)
-    lib.RMETIS_GPU_SetProfiling(0)
     gpu_launches = int(launches[nprof] - launches_before)
     cut_val = int(obj.value)
+    part_host = dpart.cpu().numpy().copy()
+
+    # Separate profiled steps: CUDA events around every profiled launch on
+    # the engine's stream give the per-kernel breakdown and the roofline.
+    prof_steps = 2
+    l0 = [launches[i] for i in range(nprof)]
+    m0 = [ms_k[i] for i in range(nprof)]
+    b0 = [bytes_k[i] for i in range(nprof)]
+    lib.RMETIS_GPU_SetProfiling(1)
+    prof_ms = []
+    for i in range(prof_steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step_device()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        prof_ms.append(e0.elapsed_time(e1))
+    lib.RMETIS_GPU_GetProfile(launches, ms_k, bytes_k, nprof + 1)
+    lib.RMETIS_GPU_SetProfiling(0)
+    P_L = [launches[i] - l0[i] for i in range(nprof)]
+    P_M = [ms_k[i] - m0[i] for i in range(nprof)]
+    P_B = [bytes_k[i] - b0[i] for i in range(nprof)]
 
     # e2e through the drop-in C ABI with pinned host buffers
     pin = lambda arr: None if arr is None else torch.from_numpy(np.ascontiguousarray(arr, np.int32)).pin_memory()
@@ -774,9 +829,9 @@ def main():
         e2e_value = world * m / e2e_max
         peak, peak_kind = load_peaks()
         names = PROF_NAMES
-        dom = max(range(nprof), key=lambda i: ms_k[i] if bytes_k[i] > 0 else -1.0)
-        avg_ms = ms_k[dom] / max(1, launches[dom])
-        avg_bytes = bytes_k[dom] / max(1, launches[dom])
+        dom = max(range(nprof), key=lambda i: P_M[i] if P_B[i] > 0 else -1.0)
+        avg_ms = P_M[dom] / max(1, P_L[dom])
+        avg_bytes = P_B[dom] / max(1, P_L[dom])
         achieved = (avg_bytes / (avg_ms / 1000.0)) / 1e9 if avg_ms > 0 else 0.0
         traffic = None
         tpath = os.path.join(ROOT, "profiles", "traffic.json")
@@ -785,18 +840,19 @@ def main():
                 traffic = json.load(open(tpath)).get(args.workload, {}).get(names[dom])
             except Exception:
                 traffic = None
-        kernels = {names[i]: {"launches": int(launches[i]), "ms": round(ms_k[i] / args.steps, 4),
-                              "GBps": round(bytes_k[i] / (ms_k[i] / 1000.0) / 1e9, 1) if ms_k[i] > 0 and bytes_k[i] > 0
+        kernels = {names[i]: {"launches": int(P_L[i]) // prof_steps, "ms": round(P_M[i] / prof_steps, 4),
+                              "GBps": round(P_B[i] / (P_M[i] / 1000.0) / 1e9, 1) if P_M[i] > 0 and P_B[i] > 0
                               else None} for i in range(nprof)}
+        step_bytes = sum(P_B) / prof_steps
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": {"workload": desc, "name": args.workload, "n": n, "m": m, "nparts": k,
-                       "l2": "flushed before every timed step (256 MiB write)",
-                       "parallelism": "replicas" if world > 1 else "single", "tuning": TUNING,
-                       "rtype": RTYPE["name"]},
+            "config": _config(args.workload, n, m, k, world),
+            "l2": "flushed before every timed step (256 MiB write)",
+            "tuning": TUNING,
             "objval": cut_val,
+            "balance": balance_summary(x, v, part_host, k),
             "gpu_launches": gpu_launches,
             "gpu_launches_per_step": gpu_launches / args.steps,
             "e2e": {"value": e2e_value, "unit": UNIT, "ms_per_step": e2e_max * 1000.0,
@@ -805,14 +861,26 @@ def main():
                     "d2h_bytes_per_step": int(4 * n + 4)},
             "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                         "traffic": traffic, "bytes_per_launch": avg_bytes, "ms_per_launch": avg_ms},
+                         "traffic": traffic, "bytes_per_launch": avg_bytes, "ms_per_launch": avg_ms,
+                         "timing": f"CUDA events around each launch in {prof_steps} profiled steps after the "
+                                   "timed ones"},
+            "roofline_step": {"bound": "hbm", "bytes_per_step": step_bytes,
+                              "achieved": step_bytes / (ms_max / 1000.0) / 1e9, "peak": peak, "unit": "GB/s",
+                              "frac": step_bytes / (ms_max / 1000.0) / 1e9 / peak, "peak_source": peak_kind,
+                              "bytes": "algorithmic bytes of the profiled kernel families (gain tables, "
+                                       "matching round 0, contraction, grow, single-block levels, coarse "
+                                       "tail, cut), per step"},
+            "profiled_ms_per_step": float(np.mean(prof_ms)),
             "kernels_per_step": kernels,
             "clocks": clocks,
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.workload, graph=(x, a, v, w))
+            ref_cut = int(line["cpu_baseline"].pop("objval"))
+            line["quality"] = {"objval": cut_val, "oracle_objval": ref_cut, "ratio": cut_val / max(1, ref_cut),
+                               "seed": seed}
         line["repro"] = _repro()
-    print(json.dumps(line))
+        print(json.dumps(line))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -144,10 +144,6 @@ void Engine::thresholds(const std::vector<std::vector<int32_t>>& totals, int k, 
   RMB_CUDA(cudaMemcpyAsync(d_thr, h_thr_, sizeof(long long) * need, cudaMemcpyHostToDevice, stream_));
 }
 
-__global__ void k_random_part(int32_t n, int32_t k, uint64_t seed, idx_t* part) {
-  RMB_GRID_STRIDE(v, n) { part[v] = (idx_t)(mix64(seed ^ (uint64_t)v * 0x9e3779b97f4a7c15ULL) % (uint64_t)k); }
-}
-
 int Engine::partition_kway(const DGraph& g0, int nparts, const float* tpwgts, const float* ubvec,
                            const KwayOptions& o, idx_t* part_out, int32_t* objval, KwayTrace* trace) {
   cudaStream_t st = stream_;
@@ -369,8 +365,14 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
     const DGraph& cg = levels.back();
     idx_t* part = arena_.alloc<idx_t>((size_t)cg.n);
     if (o.iptype == 1) {
-      k_random_part<<<grid_for(cg.n, 256), 256, 0, st>>>(cg.n, k, mix64(seed64 ^ 0x52414e44ULL), part);
-      RMB_LAUNCH_CHECK();
+      // random_partition (src/initial/random.rs:8-10): every vertex draws
+      // gen_range(0..k), rand 0.8's widening-multiply sampler, from the
+      // attempt's xoshiro256++ stream.
+      HostRng rng(mix64(seed64 ^ 0x52414e44ULL));
+      std::vector<int32_t> hp((size_t)cg.n);
+      for (auto& p : hp) p = (int32_t)rng.below((uint64_t)k);
+      RMB_CUDA(cudaMemcpyAsync(part, hp.data(), sizeof(int32_t) * hp.size(), cudaMemcpyHostToDevice, st));
+      RMB_CUDA(cudaStreamSynchronize(st));
     } else {
       const int T = std::max(1, o.grow_trials);
       std::vector<int32_t> seeds((size_t)T * k);
