@@ -65,7 +65,7 @@ WORKLOADS = {
 EXTRA_WORKLOADS = ("rmat_seeds", "rgg_batch", "serving")
 # Kernel families of RMETIS_GPU_GetProfile, in its slot order.
 PROF_NAMES = ["k_gain", "k_walk", "k_match_propose", "k_contract_thread", "k_cut", "k_grow", "k_refine_level",
-              "k_coarsen_tail"]
+              "k_coarsen_tail", "k_admit"]
 CPU_SAMPLE = {
     "grid3d_128": (lambda: G.grid3d(64, weights_seed=7), "3D 7-point grid 64^3 (same weight laws), nparts=64"),
     "grid2d_64": (lambda: G.grid2d(64, 64) + (None, None), "2D grid 64x64, nparts=8"),

@@ -129,6 +129,19 @@ RMETIS_API int RMETIS_GPU_SetStream(void *stream);
 RMETIS_API int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weights,
                                     int parallel_attempts, int fused_max_n, int tail_max_n);
 
+/* How greedy cut passes decide (no counterpart in the reference, whose pass
+ * is sequential, src/refine/greedy.rs:126-190). Levels with at most
+ * exact_max_n vertices (default 65536) decide every pass exactly as the
+ * reference's sequential pass does; larger levels decide each cut pass by
+ * parallel admission in one launch: every mover takes its best positive-gain
+ * part that its move alone keeps feasible, and each part admits the longest
+ * prefix (by vertex id) of its incoming moves that fits its limit given the
+ * admitted moves out of it. Balance holds as in the reference (every part
+ * that receives a move ends within floor(t*ub)); the decisions differ, so
+ * results are compared by quality. -1 = exact everywhere. Returns
+ * METIS_ERROR_INPUT for values below -1. */
+RMETIS_API int RMETIS_GPU_SetRefineMode(int exact_max_n);
+
 /* The last two knobs of RMETIS_GPU_SetTuning for jobs that share the device
  * with other jobs: the graphs of RMETIS_GPU_PartGraphKwayBatch and requests of
  * RMETIS_GPU_SubmitKway (no counterpart in the reference). A single-block
@@ -240,7 +253,10 @@ RMETIS_API int RMETIS_GPU_GrowPartition(idx_t n, idx_t ncon, const idx_t *xadj, 
 /* greedy_refine (src/refine/greedy.rs:12-22, :36-193): part updated in place;
  * targets[nparts*ncon] and ubvec[ncon] in f64 as the reference passes them.
  * *cut receives the edge cut afterwards; stats (optional, 4 entries): passes,
- * moves, decision rounds, movers. */
+ * moves, decision rounds, movers. Every pass is the reference's sequential
+ * pass bit for bit, except the cut passes of a graph with more vertices than
+ * the RMETIS_GPU_SetRefineMode threshold (default 65536), which decide by
+ * parallel admission. */
 RMETIS_API int RMETIS_GPU_GreedyRefine(idx_t n, idx_t ncon, const idx_t *xadj, const idx_t *adjncy, const idx_t *vwgt,
                             const idx_t *adjwgt, idx_t *part, idx_t nparts, const double *targets,
                             const double *ubvec, idx_t niter, idx_t *cut, int64_t *stats);

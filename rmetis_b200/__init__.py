@@ -395,6 +395,13 @@ def set_tuning(grow_trials: int = -1, match_rounds: int = -1, summed_unit_weight
                                                 fused_max_n, tail_max_n), "set_tuning")
 
 
+def set_refine_mode(exact_max_n: int = 65536):
+    """Levels with at most exact_max_n vertices decide greedy cut passes
+    exactly as the reference's sequential pass; larger levels by parallel
+    admission (-1: exact everywhere)."""
+    _raise_for(_lib.load().RMETIS_GPU_SetRefineMode(exact_max_n), "set_refine_mode")
+
+
 def set_pool_tuning(fused_max_n: int = -2, tail_max_n: int = -2):
     """Launch-shape knobs for batch graphs and submitted requests, which share
     the device with other jobs (-1 = the set_tuning value, -2 leaves a knob

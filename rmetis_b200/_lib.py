@@ -23,6 +23,7 @@ SIGNATURES = {
     "RMETIS_GPU_SetStream": [VP],
     "RMETIS_GPU_SetTuning": [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int],
     "RMETIS_GPU_SetPoolTuning": [ctypes.c_int, ctypes.c_int],
+    "RMETIS_GPU_SetRefineMode": [ctypes.c_int],
     "RMETIS_GPU_SetProfiling": [ctypes.c_int],
     "RMETIS_GPU_GetProfile": [I64P, F64P, F64P, ctypes.c_int],
     "RMETIS_GPU_PartGraphKwayTrace": [I32P, I32P, I32P, I32P, I32P, I32P, I32P, F32P, F32P, I32P, I32P, I32P,

@@ -1,0 +1,485 @@
+// Parallel admission of a greedy cut pass: the production form of the
+// reference's pass on large levels.
+//
+// Reference (src/refine/greedy.rs:126-190): boundary vertices in ascending id
+// each take the feasible part with the best positive gain (gains from the
+// start-of-pass part vector, feasibility pw[p] + vw <= t[p]*ub under the part
+// weights left by the moves before it), and the moves apply together after
+// the pass. Only the part weights chain the decisions together.
+//
+// Here a pass is decided in two launches:
+//  1. pick (all movers in parallel): every mover takes the best positive-gain
+//     candidate that is feasible under the start-of-pass weights (its move
+//     alone);
+//  then one block:
+//  2. groups the picks by target part, in ascending vertex id (stable ranks),
+//     and sums their weights along each part's in-list;
+//  3. admission: a part keeps the longest prefix of its in-list whose weight
+//     fits its budget feas - pw + (weight of its admitted out-moves). A part
+//     that drops in-moves keeps their movers at home, which lowers the
+//     out-credit of those movers' parts: repeat until no budget changes (the
+//     admitted set only shrinks, so this ends). At the fixed point every part
+//     that receives a move ends within its limit, as after the reference's
+//     pass. Should the bound on the rounds be reached first, every part keeps
+//     only what fits without any out-credit, which is within the limit
+//     whatever else moves;
+//  4. apply the admitted moves to part and pw.
+// Everything is integer and ordered by vertex id, so the result is the same
+// on every run. The decisions differ from the reference's sequential ones
+// (a part may take a vertex whose room appears only through moves of higher
+// ids), so partitions built this way are compared by quality; the exact
+// sequential walk (refine.cu) stays the path of small levels and of the
+// checkers that replay a pass bit for bit.
+#include "kernels.h"
+#include "prof.h"
+
+namespace rmb {
+
+namespace {
+
+constexpr int kAdmitThreads = 1024;
+constexpr int kAdmitWarps = kAdmitThreads / 32;
+constexpr int kAdmitMaxRounds = 64;
+
+__device__ __forceinline__ int32_t vweight(const idx_t* vwgt, int32_t v, int32_t ncon, int c) {
+  return vwgt ? vwgt[(int64_t)v * ncon + c] : 1;
+}
+
+// ---------------------------------------------------------------------------
+// Picks (all movers at once): the best positive-gain part that the move alone
+// keeps feasible under the start-of-pass weights, or -1 (greedy.rs:131-155).
+// Writes per mover its target, source part and weights, so that the
+// single-block admission reads them coalesced.
+// ---------------------------------------------------------------------------
+struct PickArgs {
+  const int32_t* nm_dev;
+  const idx_t* movers;
+  const idx_t* xadj;
+  const idx_t* ncand;
+  const idx_t* wfrom;
+  const idx_t* cand_p;
+  const idx_t* cand_g;
+  const idx_t* vwgt;
+  const idx_t* part;
+  const long long* pw;
+  const long long* feas;
+  int32_t ncon;
+  int32_t k;
+  int32_t* tgt;
+  int32_t* src;
+  int32_t* w;  // [nm][ncon]
+};
+
+__global__ void k_admit_pick(PickArgs A) {
+  const int32_t nm = *A.nm_dev;
+  const int32_t ncon = A.ncon;
+  RMB_GRID_STRIDE(j, nm) {
+    const int32_t v = A.movers[j];
+    const int32_t pv = A.part[v];
+    const int32_t s = A.xadj[v];
+    const int32_t ne = A.ncand[v];
+    const int32_t ig = (int32_t)(0u - (uint32_t)A.wfrom[v]);
+    int32_t vw[8];
+    for (int c = 0; c < ncon; ++c) {
+      vw[c] = vweight(A.vwgt, v, ncon, c);
+      A.w[(int64_t)j * ncon + c] = vw[c];
+    }
+    auto feasible = [&](int32_t p) {
+      for (int c = 0; c < ncon; ++c)
+        if (A.pw[(int64_t)p * ncon + c] + vw[c] > A.feas[(int64_t)p * ncon + c]) return false;
+      return true;
+    };
+    int32_t t = -1;
+    if (ig <= 0) {
+      // Candidates are sorted by (gain desc, part asc); parts outside the
+      // list have gain ig <= 0 and never qualify.
+      for (int32_t i = 0; i < ne; ++i) {
+        if (A.cand_g[s + i] <= 0) break;
+        const int32_t p = A.cand_p[s + i];
+        if (feasible(p)) {
+          t = p;
+          break;
+        }
+      }
+    } else {
+      // Negative edge weights: every part outside the list has the positive
+      // gain ig. All parts in ascending order; strict > keeps the lowest.
+      int32_t bestg = 0;
+      for (int32_t p = 0; p < A.k; ++p) {
+        if (p == pv) continue;
+        int32_t gp = ig;
+        for (int32_t i = 0; i < ne; ++i)
+          if (A.cand_p[s + i] == p) {
+            gp = A.cand_g[s + i];
+            break;
+          }
+        if (gp > bestg && feasible(p)) {
+          t = p;
+          bestg = gp;
+        }
+      }
+    }
+    A.tgt[j] = t;
+    A.src[j] = pv;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The admission of one pass in one block.
+// ---------------------------------------------------------------------------
+struct AdmitArgs {
+  const int32_t* nm_dev;
+  const idx_t* movers;
+  int32_t ncon;
+  int32_t k;
+  idx_t* part;
+  long long* pw;
+  const long long* feas;
+  int32_t* nmoves;
+  int32_t* rounds_out;  // admission rounds used (diagnostics), may be null
+  const int32_t* tgt;
+  const int32_t* src;
+  const int32_t* w;
+  int32_t* rank;
+  long long* pref_g;    // [nm][ncon] running weight sums in grouped order (when shared memory is short)
+  int32_t* src_g;       // [nm] source part in grouped order (same)
+};
+
+// Shared-memory layout (dynamic), in bytes; the staging area of the grouped
+// order takes the rest of kAdmitMaxSmem.
+struct AdmitSmem {
+  size_t pw, feas, out, wcnt, run, off, cut, lo, hi, stage, total;
+  int64_t cap;  // grouped positions that fit in shared memory
+  __host__ __device__ AdmitSmem(int k, int ncon) {
+    const size_t K = (size_t)k * ncon;
+    size_t o = 0;
+    pw = o;   o += 8 * K;
+    feas = o; o += 8 * K;
+    out = o;  o += 8 * K;
+    wcnt = o; o += 4 * (size_t)kAdmitWarps * k;
+    run = o;  o += 4 * (size_t)k;
+    off = o;  o += 4 * ((size_t)k + 1);
+    cut = o;  o += 4 * (size_t)k;
+    lo = o;   o += 4 * (size_t)k;
+    hi = o;   o += 4 * (size_t)k;
+    stage = (o + 15) & ~(size_t)15;
+    total = stage;
+    const size_t per = 8 * (size_t)ncon + 4;
+    cap = stage < kAdmitMaxSmem ? (int64_t)((kAdmitMaxSmem - stage) / per) : 0;
+  }
+};
+
+// Sum of the first i in-moves of part p on constraint c.
+__device__ __forceinline__ long long inlist_sum(const long long* pref, int32_t ncon, int32_t off_p, int32_t i,
+                                                int c) {
+  if (i == 0) return 0;
+  const long long hi = pref[(int64_t)(off_p + i - 1) * ncon + c];
+  const long long lo = off_p > 0 ? pref[(int64_t)(off_p - 1) * ncon + c] : 0;
+  return hi - lo;
+}
+
+// Largest i <= imax whose first i in-moves fit budget[c] on every
+// constraint (the sums grow with i: vertex weights are positive).
+__device__ int32_t fit_prefix(const long long* pref, int32_t ncon, int32_t off_p, int32_t imax,
+                              const long long* budget) {
+  for (int c = 0; c < ncon; ++c)
+    if (budget[c] < 0) return 0;
+  int32_t lo = 0, hi = imax;
+  while (lo < hi) {
+    const int32_t mid = lo + (hi - lo + 1) / 2;
+    bool ok = true;
+    for (int c = 0; c < ncon && ok; ++c)
+      if (inlist_sum(pref, ncon, off_p, mid, c) > budget[c]) ok = false;
+    if (ok) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kAdmitThreads, 1) k_admit(AdmitArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const AdmitSmem L(A.k, A.ncon);
+  long long* pw_s = reinterpret_cast<long long*>(smem + L.pw);
+  long long* feas_s = reinterpret_cast<long long*>(smem + L.feas);
+  long long* out_s = reinterpret_cast<long long*>(smem + L.out);
+  int32_t* wcnt = reinterpret_cast<int32_t*>(smem + L.wcnt);  // [warp][k]
+  int32_t* run = reinterpret_cast<int32_t*>(smem + L.run);
+  int32_t* off = reinterpret_cast<int32_t*>(smem + L.off);
+  int32_t* cut = reinterpret_cast<int32_t*>(smem + L.cut);
+  int32_t* rlo = reinterpret_cast<int32_t*>(smem + L.lo);
+  int32_t* rhi = reinterpret_cast<int32_t*>(smem + L.hi);
+  __shared__ long long wsum[kAdmitWarps][2];
+  __shared__ int32_t flag;
+  __shared__ int32_t warp_tot[kAdmitWarps];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int32_t k = A.k, ncon = A.ncon;
+  const int32_t K = k * ncon;
+  const int32_t nm = *A.nm_dev;
+  for (int32_t i = tid; i < K; i += kAdmitThreads) {
+    pw_s[i] = A.pw[i];
+    feas_s[i] = A.feas[i];
+    out_s[i] = 0;
+  }
+  for (int32_t i = tid; i < kAdmitWarps * k; i += kAdmitThreads) wcnt[i] = 0;
+  for (int32_t i = tid; i < k; i += kAdmitThreads) run[i] = 0;
+  __syncthreads();
+  if (nm == 0) {
+    if (tid == 0) {
+      *A.nmoves = 0;
+      if (A.rounds_out) *A.rounds_out = 0;
+    }
+    return;
+  }
+
+  // ---- stable ranks per target (ascending mover order) and out-weights ----
+  for (int32_t base = 0; base < nm; base += kAdmitThreads) {
+    const int32_t j = base + tid;
+    const int32_t t = j < nm ? A.tgt[j] : -1;
+    if (t >= 0) {
+      const int32_t sp = A.src[j];
+      for (int c = 0; c < ncon; ++c) atomic_add_i64(&out_s[sp * ncon + c], A.w[(int64_t)j * ncon + c]);
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, t);
+    const unsigned before = peers & lanemask_lt();
+    const int32_t rin = __popc(before);
+    if (t >= 0 && before == 0) wcnt[warp * k + t] = __popc(peers);
+    __syncthreads();
+    // Per target: bases of the warps in order (entries without movers stay 0).
+    for (int32_t p = tid; p < k; p += kAdmitThreads) {
+      int32_t acc = run[p];
+      for (int w = 0; w < kAdmitWarps; ++w) {
+        const int32_t c = wcnt[w * k + p];
+        if (c) {
+          wcnt[w * k + p] = acc;
+          acc += c;
+        }
+      }
+      run[p] = acc;
+    }
+    __syncthreads();
+    if (t >= 0) A.rank[j] = wcnt[warp * k + t] + rin;
+    __syncwarp();
+    if (t >= 0 && before == 0) wcnt[warp * k + t] = 0;
+    __syncthreads();
+  }
+
+  // ---- offsets of the in-lists: exclusive scan of the counts over parts ----
+  {
+    int32_t carry = 0;
+    for (int32_t p0 = 0; p0 < k; p0 += kAdmitThreads) {
+      const int32_t p = p0 + tid;
+      const int32_t c = p < k ? run[p] : 0;
+      int32_t x = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (lane == 31) warp_tot[warp] = x;
+      __syncthreads();
+      if (warp == 0) {
+        int32_t s = warp_tot[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int32_t y = __shfl_up_sync(0xffffffffu, s, o);
+          if (lane >= o) s += y;
+        }
+        warp_tot[lane] = s;  // inclusive over warps
+      }
+      __syncthreads();
+      const int32_t wbase = warp > 0 ? warp_tot[warp - 1] : 0;
+      if (p < k) {
+        off[p] = carry + wbase + x - c;
+        cut[p] = c;
+      }
+      const int32_t tile_total = warp_tot[kAdmitWarps - 1];
+      __syncthreads();
+      carry += tile_total;
+    }
+    if (tid == 0) off[k] = carry;
+    __syncthreads();
+  }
+  const int32_t total = off[k];
+
+  // ---- grouped order: source part and weights at each in-list position,
+  // then running weight sums along it (shared memory when it fits) ----
+  const bool in_smem = total <= L.cap;
+  long long* pref = in_smem ? reinterpret_cast<long long*>(smem + L.stage) : A.pref_g;
+  int32_t* gsrc = in_smem ? reinterpret_cast<int32_t*>(smem + L.stage + 8 * (size_t)ncon * (size_t)L.cap) : A.src_g;
+  for (int32_t j = tid; j < nm; j += kAdmitThreads) {
+    const int32_t t = A.tgt[j];
+    if (t >= 0) {
+      const int32_t pos = off[t] + A.rank[j];
+      gsrc[pos] = A.src[j];
+      for (int c = 0; c < ncon; ++c) pref[(int64_t)pos * ncon + c] = A.w[(int64_t)j * ncon + c];
+    }
+  }
+  __syncthreads();
+  for (int c = 0; c < ncon; ++c) {
+    long long carry = 0;
+    for (int32_t base = 0; base < total; base += kAdmitThreads) {
+      const int32_t pos = base + tid;
+      const long long w = pos < total ? pref[(int64_t)pos * ncon + c] : 0;
+      long long x = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (lane == 31) wsum[warp][0] = x;
+      __syncthreads();
+      if (warp == 0) {
+        long long s = wsum[lane][0];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const long long y = __shfl_up_sync(0xffffffffu, s, o);
+          if (lane >= o) s += y;
+        }
+        wsum[lane][1] = s;
+      }
+      __syncthreads();
+      const long long wbase = warp > 0 ? wsum[warp - 1][1] : 0;
+      if (pos < total) pref[(int64_t)pos * ncon + c] = carry + wbase + x;
+      const long long tile_total = wsum[kAdmitWarps - 1][1];
+      __syncthreads();
+      carry += tile_total;
+    }
+  }
+  __syncthreads();
+
+  // ---- admission rounds ----
+  int rounds = 0;
+  bool converged = false;
+  while (rounds < kAdmitMaxRounds) {
+    ++rounds;
+    if (tid == 0) flag = 0;
+    __syncthreads();
+    for (int32_t p = tid; p < k; p += kAdmitThreads) {
+      long long budget[8];
+      for (int c = 0; c < ncon; ++c) {
+        const int32_t x = p * ncon + c;
+        budget[c] = feas_s[x] - pw_s[x] + out_s[x];
+      }
+      const int32_t old = cut[p];
+      const int32_t now = old > 0 ? fit_prefix(pref, ncon, off[p], old, budget) : 0;
+      rlo[p] = now;
+      rhi[p] = old;
+      if (now < old) {
+        cut[p] = now;
+        flag = 1;
+      }
+    }
+    __syncthreads();
+    if (!flag) {
+      converged = true;
+      break;
+    }
+    // Movers dropped in this round stay home: their parts lose that
+    // out-credit. A warp walks each part's dropped range.
+    for (int32_t p = warp; p < k; p += kAdmitWarps) {
+      const int32_t o = off[p];
+      for (int32_t i = rlo[p] + lane; i < rhi[p]; i += 32) {
+        const int32_t pos = o + i;
+        const int32_t sp = gsrc[pos];
+        for (int c = 0; c < ncon; ++c) {
+          const long long wv = pref[(int64_t)pos * ncon + c] - (pos > 0 ? pref[(int64_t)(pos - 1) * ncon + c] : 0);
+          atomic_add_i64(&out_s[sp * ncon + c], -wv);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (!converged) {
+    // Keep only what fits with no out-credit at all.
+    for (int32_t p = tid; p < k; p += kAdmitThreads) {
+      long long budget[8];
+      for (int c = 0; c < ncon; ++c) budget[c] = feas_s[p * ncon + c] - pw_s[p * ncon + c];
+      if (cut[p] > 0) cut[p] = fit_prefix(pref, ncon, off[p], cut[p], budget);
+    }
+    __syncthreads();
+  }
+
+  // ---- apply the admitted moves ----
+  int32_t moved = 0;
+  for (int32_t j = tid; j < nm; j += kAdmitThreads) {
+    const int32_t t = A.tgt[j];
+    if (t >= 0 && A.rank[j] < cut[t]) {
+      const int32_t sp = A.src[j];
+      A.part[A.movers[j]] = t;
+      for (int c = 0; c < ncon; ++c) {
+        const long long wv = A.w[(int64_t)j * ncon + c];
+        atomic_add_i64(&pw_s[t * ncon + c], wv);
+        atomic_add_i64(&pw_s[sp * ncon + c], -wv);
+      }
+      ++moved;
+    }
+  }
+  moved = warp_sum(moved);
+  if (lane == 0) warp_tot[warp] = moved;
+  __syncthreads();
+  for (int32_t i = tid; i < K; i += kAdmitThreads) A.pw[i] = pw_s[i];
+  if (tid == 0) {
+    int32_t s = 0;
+    for (int w = 0; w < kAdmitWarps; ++w) s += warp_tot[w];
+    *A.nmoves = s;
+    if (A.rounds_out) *A.rounds_out = converged ? rounds : -rounds;
+  }
+}
+
+}  // namespace
+
+size_t admit_smem_bytes(int k, int ncon) { return AdmitSmem(k, ncon).total; }
+
+bool admit_supported(int k, int ncon) {
+  return k >= 2 && ncon >= 1 && ncon <= 8 && admit_smem_bytes(k, ncon) <= kAdmitMaxSmem;
+}
+
+int admit_cut_pass(const DGraph& g, int k, int32_t nmax, const int32_t* nm_dev, const idx_t* movers,
+                   const idx_t* ncand, const idx_t* wfrom, const idx_t* cand_p, const idx_t* cand_g, idx_t* part,
+                   long long* pw, const long long* feas, int32_t* nmoves, int32_t* rounds_out,
+                   const AdmitScratch& s, cudaStream_t st) {
+  const int ph = profiler().begin(kProfAdmit, st);
+  PickArgs P;
+  P.nm_dev = nm_dev;
+  P.movers = movers;
+  P.xadj = g.xadj;
+  P.ncand = ncand;
+  P.wfrom = wfrom;
+  P.cand_p = cand_p;
+  P.cand_g = cand_g;
+  P.vwgt = g.vwgt;
+  P.part = part;
+  P.pw = pw;
+  P.feas = feas;
+  P.ncon = g.ncon;
+  P.k = k;
+  P.tgt = s.tgt;
+  P.src = s.src;
+  P.w = s.w;
+  k_admit_pick<<<grid_for(nmax, 256, 148 * 4), 256, 0, st>>>(P);
+  RMB_LAUNCH_CHECK();
+  AdmitArgs A;
+  A.nm_dev = nm_dev;
+  A.movers = movers;
+  A.ncon = g.ncon;
+  A.k = k;
+  A.part = part;
+  A.pw = pw;
+  A.feas = feas;
+  A.nmoves = nmoves;
+  A.rounds_out = rounds_out;
+  A.tgt = s.tgt;
+  A.src = s.src;
+  A.w = s.w;
+  A.rank = s.rank;
+  A.pref_g = s.pref;
+  A.src_g = s.gsrc;
+  allow_dyn_smem((const void*)k_admit, kAdmitMaxSmem);
+  k_admit<<<1, kAdmitThreads, kAdmitMaxSmem, st>>>(A);
+  RMB_LAUNCH_CHECK();
+  profiler().end(ph, st, 0.0);
+  return ph;
+}
+
+}  // namespace rmb

@@ -41,6 +41,7 @@ struct Tuning {
   int parallel_attempts = 1;
   int fused_max_n = 4096;
   int tail_max_n = 4096;
+  int exact_max_n = 65536;
 };
 Tuning& tuning() {
   static Tuning t;
@@ -54,6 +55,7 @@ void apply_tuning(KwayOptions& o) {
   o.parallel_attempts = tuning().parallel_attempts;
   o.fused_max_n = tuning().fused_max_n;
   o.tail_max_n = tuning().tail_max_n;
+  o.exact_max_n = tuning().exact_max_n;
 }
 
 // Launch-shape knobs of jobs that share the device with other jobs (batch
@@ -483,6 +485,12 @@ int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weig
   return METIS_OK;
 }
 
+int RMETIS_GPU_SetRefineMode(int exact_max_n) {
+  if (exact_max_n < -1) return METIS_ERROR_INPUT;
+  tuning().exact_max_n = exact_max_n == -1 ? INT32_MAX : exact_max_n;
+  return METIS_OK;
+}
+
 int RMETIS_GPU_SetPoolTuning(int fused_max_n, int tail_max_n) {
   if (fused_max_n >= -1) pool_tuning().fused_max_n = fused_max_n;
   if (tail_max_n >= -1) pool_tuning().tail_max_n = tail_max_n;
@@ -884,6 +892,7 @@ static int refine_entry(bool fm, idx_t n, idx_t ncon, const idx_t* xadj, const i
     rp.over_thr = d_over;
     rp.collect_stats = stats != nullptr;
     rp.fused_max_n = tuning().fused_max_n;
+    if (!fm) rp.exact_max_n = tuning().exact_max_n;
     {
       std::vector<long long> tot(ncon, 0);
       for (int64_t v = 0; v < n; ++v)

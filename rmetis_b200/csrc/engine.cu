@@ -422,6 +422,8 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
     rp.over_thr = over_of(L);
     rp.small_weights = small[L];
     rp.fused_max_n = o.fused_max_n;
+    // A traced run replays bit for bit in the oracle: exact walks everywhere.
+    rp.exact_max_n = trace ? INT32_MAX : o.exact_max_n;
     rp.collect_stats = trace != nullptr;
     {
       RefineStats rs = refine_level(o.rtype, cg, part, rp, heavy_lists[L], heavy_counts[L]);

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <climits>
 
 #include "arena.h"
 #include "common.cuh"
@@ -139,6 +140,9 @@ struct RefineParams {
   // entries (and k <= 256, ncon <= 2) run all their passes in one
   // single-block launch (k_refine_level); 0 = never.
   int32_t fused_max_n = 0;
+  // Cut passes of levels with more vertices than this decide by parallel
+  // admission (admit.cu) instead of the exact sequential walk.
+  int32_t exact_max_n = INT32_MAX;
 };
 
 // True when the totals and thresholds allow 32-bit slacks in the walk.
@@ -181,5 +185,33 @@ RefineStats fm_refine(const DGraph& g, idx_t* part, const RefineParams& rp, cons
 void gain_table(const DGraph& g, const idx_t* part, int k, idx_t* boundary, idx_t* ncand,
                 idx_t* wfrom, idx_t* cand_p, idx_t* cand_g, const idx_t* heavy, int32_t nheavy,
                 cudaStream_t st);
+
+// ---- admit.cu -----------------------------------------------------------
+// Parallel admission of one greedy cut pass (src/refine/greedy.rs:126-190 in
+// a parallel form): picks, stable grouping by target part and a monotone
+// admission fixed point, all in one single-block launch. Scratch holds nm
+// entries each (pref: nm * ncon).
+constexpr size_t kAdmitMaxSmem = 200 * 1024;
+struct AdmitScratch {
+  int32_t* tgt = nullptr;      // [n] target of each mover (-1: none)
+  int32_t* src = nullptr;      // [n] its part
+  int32_t* w = nullptr;        // [n * ncon] its weights
+  int32_t* rank = nullptr;     // [n] its place in its target's in-list
+  long long* pref = nullptr;   // [n * ncon] running sums (when shared memory is short)
+  int32_t* gsrc = nullptr;     // [n] sources in grouped order (same)
+};
+size_t admit_smem_bytes(int k, int ncon);
+bool admit_supported(int k, int ncon);
+// Returns the profiler handle of the pass. nmax bounds the movers (grid
+// size); nmoves gets the moves applied, rounds_out (optional) the admission
+// rounds (negative: the bound was hit).
+int admit_cut_pass(const DGraph& g, int k, int32_t nmax, const int32_t* nm_dev, const idx_t* movers,
+                   const idx_t* ncand, const idx_t* wfrom, const idx_t* cand_p, const idx_t* cand_g, idx_t* part,
+                   long long* pw, const long long* feas, int32_t* nmoves, int32_t* rounds_out,
+                   const AdmitScratch& s, cudaStream_t st);
+
+// Opts a kernel in to `bytes` of dynamic shared memory on the current device
+// (once per kernel and device; safe from several host threads).
+void allow_dyn_smem(const void* kernel, size_t bytes);
 
 }  // namespace rmb

@@ -14,7 +14,8 @@ size_t footprint_bytes(int64_t n, int64_t m, int k, int ncon) {
   // and the grow trials on the coarsest graph; rounded up generously.
   const int64_t input = 4 * (n + 1) + 8 * m + 4 * n * ncon;
   const int64_t hierarchy = input * 3 / 2 + 16 * n;
-  const int64_t refine = 88 * n + 8 * m + 24 * (int64_t)k * ncon;
+  // (+ the parallel admission's per-mover target, rank, slot and sums)
+  const int64_t refine = 88 * n + 12 * n + 8 * n * ncon + 8 * m + 24 * (int64_t)k * ncon;
   const int64_t grow = 32 * (16 * std::max<int64_t>(20 * (int64_t)k, 20) * 4);
   return (size_t)(input + hierarchy + refine + grow + ((int64_t)64 << 20));
 }

@@ -19,6 +19,7 @@ enum ProfId {
   kProfGrow,          // k_grow
   kProfLevel,         // k_refine_level: all passes of a small level in one launch
   kProfTail,          // k_coarsen_tail: the remaining coarsening levels of a small graph
+  kProfAdmit,         // k_admit_pick + k_admit: one cut pass decided by parallel admission
   kProfCount
 };
 

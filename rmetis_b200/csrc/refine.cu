@@ -1276,9 +1276,7 @@ void gain_table(const DGraph& g, const idx_t* part, int k, idx_t* boundary, idx_
   if (ghist) RMB_CUDA(cudaFreeAsync(ghist, st));
 }
 
-// Opts a kernel in to `bytes` of dynamic shared memory on the current device
-// (once per kernel and device).
-static void allow_dyn_smem(const void* kernel, size_t bytes) {
+void allow_dyn_smem(const void* kernel, size_t bytes) {
   static std::mutex mu;
   static std::set<std::pair<const void*, int>> done;
   int dev = 0;
@@ -1505,6 +1503,19 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
   int32_t* ghist = nullptr;
   if (nheavy > 0 && (fused || k > kGainHist))
     ghist = arena.alloc<int32_t>((size_t)k * (fused ? kFusedThreads / 32 : 256 * 4));
+  // Cut passes of large levels decide by parallel admission (admit.cu).
+  const bool admit = !fused && g.n > rp.exact_max_n && admit_supported(k, g.ncon);
+  AdmitScratch as;
+  int32_t* rounds = nullptr;
+  if (admit) {
+    as.tgt = arena.alloc<int32_t>((size_t)g.n);
+    as.src = arena.alloc<int32_t>((size_t)g.n);
+    as.w = arena.alloc<int32_t>((size_t)g.n * g.ncon);
+    as.rank = arena.alloc<int32_t>((size_t)g.n);
+    as.pref = arena.alloc<long long>((size_t)g.n * g.ncon);
+    as.gsrc = arena.alloc<int32_t>((size_t)g.n);
+    rounds = arena.alloc<int32_t>((size_t)rp.niter + 1);
+  }
   std::vector<int> walk_handles, gain_handles;
   if (fused) {
     LevelRefine P;
@@ -1562,6 +1573,9 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
       walk_handles.push_back(launch_walk<kRepair>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r,
                                                   pw, rp.feas_max, rp.over_thr, in_max, out_max, nm_dev + 1,
                                                   rp.small_weights, long_flag, st));
+    else if (admit)
+      walk_handles.push_back(admit_cut_pass(g, k, g.n, nm_dev, movers, ncand, wfrom, cand_p, cand_g, part, pw,
+                                            rp.feas_max, nm_dev + 1, rounds + pass, as, st));
     else
       walk_handles.push_back(launch_walk<kCut>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r, pw,
                                                rp.feas_max, rp.over_thr, in_max, out_max, nm_dev + 1,
@@ -1576,8 +1590,12 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
                              cudaMemcpyDeviceToHost, st));
     RMB_CUDA(cudaStreamSynchronize(st));
     const double rec_bytes = 4.0 * (5 + 2 * kInline + g.ncon) + 4.0;
+    // An admission pass reads per mover its id, part, row offset, candidate
+    // count, w_from, its first candidate pair and weights, and writes its
+    // target, rank, grouped slot and running sums.
+    const double adm_bytes = 4.0 * (7 + g.ncon) + 4.0 * (4 + 2 * g.ncon);
     for (int pass = 0; pass <= rp.niter; ++pass)
-      profiler().set_bytes(walk_handles[pass], rec_bytes * h_scratch[2 * pass]);
+      profiler().set_bytes(walk_handles[pass], (admit && pass > 0 ? adm_bytes : rec_bytes) * h_scratch[2 * pass]);
     // A cut pass emptied by the one before it only clears the mover flags.
     for (int pass = 2; pass <= rp.niter; ++pass)
       if (h_scratch[2 * (pass - 1) + 1] == 0) {
@@ -1595,9 +1613,12 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
       stats.movers += nm;
       stats.moves += nmoves;
       stats.decide_iters += 1;
-      if (trace)
-        std::fprintf(stderr, "refine n=%d m=%lld k=%d pass=%d mode=%d movers=%d moves=%d\n", g.n, (long long)g.m, k,
-                     pass, pass == 0 ? 0 : 1, nm, nmoves);
+      if (trace) {
+        int32_t rr = 0;
+        if (admit && pass > 0) RMB_CUDA(cudaMemcpy(&rr, rounds + pass, sizeof(int32_t), cudaMemcpyDeviceToHost));
+        std::fprintf(stderr, "refine n=%d m=%lld k=%d pass=%d mode=%d movers=%d moves=%d admit_rounds=%d\n", g.n,
+                     (long long)g.m, k, pass, pass == 0 ? 0 : 1, nm, nmoves, rr);
+      }
       if (pass > 0 && nmoves == 0) break;
     }
   }
