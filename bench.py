@@ -671,6 +671,9 @@ def main():
     ap.add_argument("--rates", default="50,100,200,500", help="serving: arrival rates, requests/s")
     ap.add_argument("--rtype", default="greedy", choices=["greedy", "fm"],
                     help="refinement: greedy (the measured path) or fm (the reference's default rtype)")
+    ap.add_argument("--exact-max-n", type=int, default=None,
+                    help="largest level whose greedy cut passes decide sequentially (engine default 16384; "
+                         "-1 = every level)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
@@ -682,6 +685,10 @@ def main():
         run_reference(args)
         return
     _apply_tuning()
+    if args.exact_max_n is not None:
+        import rmetis_b200 as rmb
+        rmb.set_refine_mode(args.exact_max_n)
+        TUNING["exact_max_n"] = args.exact_max_n
     if args.workload in EXTRA_WORKLOADS:
         {"rmat_seeds": run_rmat_seeds, "rgg_batch": run_rgg_batch, "serving": run_serving}[args.workload](args)
         return

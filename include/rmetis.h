@@ -131,7 +131,7 @@ RMETIS_API int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summe
 
 /* How greedy cut passes decide (no counterpart in the reference, whose pass
  * is sequential, src/refine/greedy.rs:126-190). Levels with at most
- * exact_max_n vertices (default 65536) decide every pass exactly as the
+ * exact_max_n vertices (default 16384) decide every pass exactly as the
  * reference's sequential pass does; larger levels decide each cut pass by
  * parallel admission in one launch: every mover takes its best positive-gain
  * part that its move alone keeps feasible, and each part admits the longest
@@ -255,7 +255,7 @@ RMETIS_API int RMETIS_GPU_GrowPartition(idx_t n, idx_t ncon, const idx_t *xadj, 
  * *cut receives the edge cut afterwards; stats (optional, 4 entries): passes,
  * moves, decision rounds, movers. Every pass is the reference's sequential
  * pass bit for bit, except the cut passes of a graph with more vertices than
- * the RMETIS_GPU_SetRefineMode threshold (default 65536), which decide by
+ * the RMETIS_GPU_SetRefineMode threshold (default 16384), which decide by
  * parallel admission. */
 RMETIS_API int RMETIS_GPU_GreedyRefine(idx_t n, idx_t ncon, const idx_t *xadj, const idx_t *adjncy, const idx_t *vwgt,
                             const idx_t *adjwgt, idx_t *part, idx_t nparts, const double *targets,
@@ -276,10 +276,10 @@ RMETIS_API int RMETIS_GPU_FmRefine(idx_t n, idx_t ncon, const idx_t *xadj, const
 
 /* Edge cut and partition weights of a device-resident graph without any
  * allocation, for callers that cannot allocate device memory at the point of
- * the call (while recording a CUDA graph, under a host-owned fixed memory
- * budget, or in a loop that must not synchronise the device). No counterpart
- * in the reference: it is an additive variant of RMETIS_GPU_EdgeCut plus
- * RMETIS_GPU_PartitionWeights.
+ * the call (a host that gives the library a fixed memory budget or its own
+ * pool and forbids it to grow, or a loop where cudaMalloc/cudaFree would
+ * synchronise the device). No counterpart in the reference: it is an additive
+ * variant of RMETIS_GPU_EdgeCut plus RMETIS_GPU_PartitionWeights.
  * Inputs and outputs are device pointers on the current device: d_xadj[n+1],
  * d_adjncy/d_adjwgt[nnz] (d_adjwgt and d_vwgt may be NULL for unit weights),
  * d_part[n]; outputs *d_cut and d_pw[nparts*ncon]. The work is queued on
@@ -288,10 +288,13 @@ RMETIS_API int RMETIS_GPU_FmRefine(idx_t n, idx_t ncon, const idx_t *xadj, const
  * Scratch is a fixed array in device memory of the library (about 128 KiB per
  * GPU, kept until exit): nparts*ncon above 16384 returns METIS_ERROR_INPUT with
  * a message on stderr. The first call on a device looks up that array's device
- * address, so make it before any stream capture. All calls share the array and
- * each clears it first: calls that overlap on the GPU race and must be
- * serialised by the caller. Out-of-range indices are skipped and make
- * *d_cut = -1. */
+ * address, so make that first call before any stream capture. All calls share
+ * the array and each clears it first: calls that overlap on the GPU race and
+ * must be serialised by the caller. Out-of-range indices (in d_part, d_xadj or
+ * d_adjncy) are skipped and make *d_cut = -1; d_pw is then meaningless. A
+ * valid graph whose cut sum wraps to -1 in 32 bits (as the reference's i32 sum
+ * can) gives the same -1, so a caller that can meet such sums should check its
+ * inputs itself. */
 RMETIS_API int RMETIS_GPU_EdgeCutWeightsNoAlloc(idx_t n, idx_t ncon, int64_t nnz, const idx_t *d_xadj,
                                                 const idx_t *d_adjncy, const idx_t *d_adjwgt, const idx_t *d_vwgt,
                                                 const idx_t *d_part, idx_t nparts, idx_t *d_cut, idx_t *d_pw,

@@ -395,7 +395,7 @@ def set_tuning(grow_trials: int = -1, match_rounds: int = -1, summed_unit_weight
                                                 fused_max_n, tail_max_n), "set_tuning")
 
 
-def set_refine_mode(exact_max_n: int = 65536):
+def set_refine_mode(exact_max_n: int = 16384):
     """Levels with at most exact_max_n vertices decide greedy cut passes
     exactly as the reference's sequential pass; larger levels by parallel
     admission (-1: exact everywhere)."""

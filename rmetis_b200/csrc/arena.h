@@ -13,6 +13,16 @@
 
 namespace rmb {
 
+// Optional cap on the device workspace all arenas of a process hold on one
+// device (environment RMETIS_B200_ARENA_CAP, bytes; unset or 0 = none). An
+// allocation that would pass it fails like a cudaMalloc out of memory. It
+// emulates a smaller device, so that the out-of-memory handling of the worker
+// pool can be exercised without driving a GPU out of memory.
+size_t arena_cap_bytes();
+// Reserves (or, with a negative delta, returns) bytes against the cap of a
+// device; false when the reservation would pass the cap.
+bool arena_cap_reserve(int device, long long delta);
+
 class Arena {
  public:
   explicit Arena(size_t min_chunk = (size_t)256 << 20) : min_chunk_(min_chunk) {}
@@ -39,9 +49,14 @@ class Arena {
     }
     size_t sz = bytes > min_chunk_ ? bytes : min_chunk_;
     Chunk c;
+    if (arena_cap_bytes()) {
+      if (cudaGetDevice(&c.device) != cudaSuccess) throw Error(-4, "cudaGetDevice failed");
+      if (!arena_cap_reserve(c.device, (long long)sz)) throw Error(-3, "device workspace cap reached");
+    }
     cudaError_t e = cudaMalloc(&c.base, sz);
     if (e != cudaSuccess) {
       cudaGetLastError();
+      if (arena_cap_bytes()) arena_cap_reserve(c.device, -(long long)sz);
       throw Error(-3, "device workspace allocation failed");
     }
     c.size = sz;
@@ -70,7 +85,10 @@ class Arena {
     cur_ = 0;
   }
   void release() {
-    for (auto& c : chunks_) cudaFree(c.base);
+    for (auto& c : chunks_) {
+      cudaFree(c.base);
+      if (arena_cap_bytes()) arena_cap_reserve(c.device, -(long long)c.size);
+    }
     chunks_.clear();
     cur_ = 0;
   }
@@ -84,6 +102,7 @@ class Arena {
   struct Chunk {
     char* base = nullptr;
     size_t size = 0, top = 0;
+    int device = 0;
   };
   std::vector<Chunk> chunks_;
   size_t cur_ = 0;

@@ -41,7 +41,7 @@ struct Tuning {
   int parallel_attempts = 1;
   int fused_max_n = 4096;
   int tail_max_n = 4096;
-  int exact_max_n = 65536;
+  int exact_max_n = 16384;
 };
 Tuning& tuning() {
   static Tuning t;

@@ -366,13 +366,29 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
     idx_t* part = arena_.alloc<idx_t>((size_t)cg.n);
     if (o.iptype == 1) {
       // random_partition (src/initial/random.rs:8-10): every vertex draws
-      // gen_range(0..k), rand 0.8's widening-multiply sampler, from the
-      // attempt's xoshiro256++ stream.
-      HostRng rng(mix64(seed64 ^ 0x52414e44ULL));
-      std::vector<int32_t> hp((size_t)cg.n);
-      for (auto& p : hp) p = (int32_t)rng.below((uint64_t)k);
-      RMB_CUDA(cudaMemcpyAsync(part, hp.data(), sizeof(int32_t) * hp.size(), cudaMemcpyHostToDevice, st));
+      // gen_range(0..k), rand 0.8's widening-multiply sampler, from an
+      // xoshiro256++ stream. Like the grown partitions, grow_trials draws are
+      // made (one stream each) and the one with the lowest cut is kept.
+      const int T = std::max(1, o.grow_trials);
+      std::vector<int32_t> hp((size_t)T * cg.n);
+      for (int t = 0; t < T; ++t) {
+        HostRng rng(mix64(seed64 ^ 0x52414e44ULL ^ (0x9E3779B97F4A7C15ULL * (uint64_t)t)));
+        for (int32_t v = 0; v < cg.n; ++v) hp[(size_t)t * cg.n + v] = (int32_t)rng.below((uint64_t)k);
+      }
+      Arena::Mark rm = arena_.mark();
+      idx_t* d_parts = arena_.alloc<idx_t>(hp.size());
+      long long* d_cuts = arena_.alloc<long long>((size_t)T);
+      RMB_CUDA(cudaMemcpyAsync(d_parts, hp.data(), sizeof(int32_t) * hp.size(), cudaMemcpyHostToDevice, st));
+      trial_cuts(cg, d_parts, T, d_cuts, st);
+      std::vector<long long> cuts(T);
+      RMB_CUDA(cudaMemcpyAsync(cuts.data(), d_cuts, sizeof(long long) * T, cudaMemcpyDeviceToHost, st));
       RMB_CUDA(cudaStreamSynchronize(st));
+      int bt = 0;
+      for (int t = 1; t < T; ++t)
+        if (cuts[t] < cuts[bt]) bt = t;
+      RMB_CUDA(cudaMemcpyAsync(part, d_parts + (size_t)bt * cg.n, sizeof(idx_t) * cg.n, cudaMemcpyDeviceToDevice,
+                               st));
+      (void)rm;
     } else {
       const int T = std::max(1, o.grow_trials);
       std::vector<int32_t> seeds((size_t)T * k);

@@ -34,7 +34,7 @@ struct KwayOptions {
   int parallel_attempts = 1;    // 1: ncuts > 1 attempts run concurrently on the worker pool
   int fused_max_n = 4096;       // levels up to this size (and 4x its edges) refine in one launch
   int tail_max_n = 4096;        // from a level of at most this size, coarsening runs in one launch
-  int exact_max_n = 65536;      // larger levels decide cut passes by parallel admission
+  int exact_max_n = 16384;      // larger levels decide cut passes by parallel admission
 };
 
 // Per-kernel-family device time, measured with CUDA events on the engine's
@@ -149,6 +149,7 @@ class WorkerPool {
   int running_ = 0;
   bool stop_ = false;
   unsigned trim_epoch_ = 0;  // bumped when a job ran out of memory: workers free their workspace
+  std::vector<unsigned> worker_epoch_;  // the last epoch each worker has freed its workspace for
 };
 
 // The pool of a device, created on first use: RMETIS_B200_WORKERS threads

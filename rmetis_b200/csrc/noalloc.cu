@@ -1,8 +1,7 @@
 // Edge cut and partition weights with no allocation at all.
 //
 // Some callers cannot allocate device memory when they need these numbers:
-// code recording a CUDA graph (cudaMalloc is not a capturable operation),
-// hosts that hand a plugin a fixed memory budget or their own pool and forbid
+// hosts that give a plugin a fixed memory budget or their own pool and forbid
 // it to grow, and latency-sensitive loops where cudaMalloc/cudaFree would
 // synchronise the device. This entry point serves them: the caller passes
 // device inputs and outputs and a stream, and the only scratch (the 64-bit
@@ -13,7 +12,9 @@
 // about 128 KiB that every GPU which loads the library keeps until exit. All
 // calls on a device share the array; each call clears it first, so calls
 // that overlap on the GPU (other streams, or other host threads) race and
-// must be serialised by the caller.
+// must be serialised by the caller. The first call on a device looks up the
+// array's device address (cudaGetSymbolAddress), so that first call should
+// come before any stream capture.
 #include <cstdio>
 #include <mutex>
 
@@ -57,6 +58,12 @@ unsigned long long* noalloc_scratch_for_current_device(int* err) {
   return g_noalloc_ptr[dev];
 }
 
+// Part weights of a block are summed in shared memory when nparts * ncon is
+// at most this (one global atomic per part and block instead of one per
+// vertex: with few parts, as in a bisection, per-vertex atomics would all hit
+// the same few addresses).
+constexpr int kNoAllocSmemParts = 4096;
+
 // One pass: edge cut (sum of cross weights over both directions) and part
 // weights, accumulated in the scratch. Every index is bounds-checked against
 // n, nnz and nparts; an out-of-range entry is skipped and flagged.
@@ -64,6 +71,12 @@ __global__ void k_noalloc_cut_pw(const idx_t* __restrict__ xadj, const idx_t* __
                                  const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ vwgt, int32_t n,
                                  int64_t nnz, int32_t ncon, const idx_t* __restrict__ part, int32_t nparts,
                                  unsigned long long* __restrict__ scratch) {
+  __shared__ unsigned long long spw[kNoAllocSmemParts];
+  const int32_t K = nparts * ncon;
+  const bool local = K <= kNoAllocSmemParts;
+  if (local)
+    for (int32_t i = threadIdx.x; i < K; i += blockDim.x) spw[i] = 0;
+  __syncthreads();
   unsigned long long acc = 0;
   int bad = 0;
   RMB_GRID_STRIDE(v, n) {
@@ -74,7 +87,8 @@ __global__ void k_noalloc_cut_pw(const idx_t* __restrict__ xadj, const idx_t* __
     }
     for (int c = 0; c < ncon; ++c) {
       const long long w = vwgt ? vwgt[(int64_t)v * ncon + c] : 1;
-      atomicAdd(&scratch[kNoAllocHeader + (int64_t)pv * ncon + c], (unsigned long long)w);
+      if (local) atomicAdd(&spw[(int64_t)pv * ncon + c], (unsigned long long)w);
+      else atomicAdd(&scratch[kNoAllocHeader + (int64_t)pv * ncon + c], (unsigned long long)w);
     }
     int64_t s = xadj[v], e = xadj[v + 1];
     if (s < 0 || e > nnz || s > e) {
@@ -93,10 +107,16 @@ __global__ void k_noalloc_cut_pw(const idx_t* __restrict__ xadj, const idx_t* __
   acc = warp_sum(acc);
   if ((threadIdx.x & 31) == 0 && acc) atomicAdd(&scratch[0], acc);
   if (bad) scratch[1] = 1;
+  if (local) {
+    __syncthreads();
+    for (int32_t i = threadIdx.x; i < K; i += blockDim.x)
+      if (spw[i]) atomicAdd(&scratch[kNoAllocHeader + i], spw[i]);
+  }
 }
 
 // Outputs with the reference's i32 wrap-around: cut = (i32)sum / 2, pw as i32.
-// A flagged bad input makes the cut -1.
+// A flagged bad input makes the cut -1 (the part weights then hold the sums
+// of the well-formed entries only and mean nothing).
 __global__ void k_noalloc_finish(const unsigned long long* __restrict__ scratch, int32_t K, idx_t* __restrict__ cut,
                                  idx_t* __restrict__ pw) {
   RMB_GRID_STRIDE(i, K) { pw[i] = (idx_t)(uint32_t)scratch[kNoAllocHeader + i]; }

@@ -1,5 +1,7 @@
 // Worker pool: concurrent partitions on one device (the attempts of one call,
 // the graphs of a batch, asynchronous requests).
+#include <atomic>
+#include <cstdio>
 #include <algorithm>
 #include <cstdlib>
 #include <mutex>
@@ -20,7 +22,27 @@ size_t footprint_bytes(int64_t n, int64_t m, int k, int ncon) {
   return (size_t)(input + hierarchy + refine + grow + ((int64_t)64 << 20));
 }
 
-WorkerPool::WorkerPool(int device, int nworkers, size_t budget_bytes) : device_(device), budget_(budget_bytes) {
+size_t arena_cap_bytes() {
+  static const size_t cap = [] {
+    const char* e = std::getenv("RMETIS_B200_ARENA_CAP");
+    return e ? (size_t)std::strtoull(e, nullptr, 10) : (size_t)0;
+  }();
+  return cap;
+}
+
+bool arena_cap_reserve(int device, long long delta) {
+  static std::atomic<long long> used[64];
+  if (device < 0 || device >= 64) return false;
+  const long long now = used[device].fetch_add(delta) + delta;
+  if (delta > 0 && now > (long long)arena_cap_bytes()) {
+    used[device].fetch_sub(delta);
+    return false;
+  }
+  return true;
+}
+
+WorkerPool::WorkerPool(int device, int nworkers, size_t budget_bytes)
+    : device_(device), budget_(budget_bytes), worker_epoch_(nworkers, 0) {
   for (int i = 0; i < nworkers; ++i) threads_.emplace_back([this, i] { worker_main(i); });
 }
 
@@ -56,7 +78,6 @@ std::future<int> WorkerPool::submit(size_t footprint, std::function<int(Engine&)
 }
 
 void WorkerPool::worker_main(int idx) {
-  (void)idx;
   cudaSetDevice(device_);
   std::unique_ptr<Engine> engine;
   try {
@@ -77,12 +98,17 @@ void WorkerPool::worker_main(int idx) {
       std::unique_lock<std::mutex> lk(mu_);
       // Admission in submission order: the head starts when its footprint
       // fits next to the running jobs, or when nothing runs (a retried job
-      // only then).
+      // only then, and only once every worker has freed its workspace).
       cv_.wait(lk, [&] {
         if (stop_ || my_epoch != trim_epoch_) return true;
         if (queue_.empty()) return false;
         const Job& h = *queue_.front();
-        if (h.alone) return running_ == 0;
+        if (h.alone) {
+          if (running_ != 0) return false;
+          for (unsigned e : worker_epoch_)
+            if (e != trim_epoch_) return false;
+          return true;
+        }
         return running_ == 0 || in_use_ + h.footprint <= budget_;
       });
       if (stop_) return;
@@ -98,6 +124,11 @@ void WorkerPool::worker_main(int idx) {
     }
     if (trim) {
       free_workspace();
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        worker_epoch_[idx] = my_epoch;
+      }
+      cv_.notify_all();
       continue;
     }
     int rc = -4;
@@ -129,7 +160,10 @@ void WorkerPool::worker_main(int idx) {
     }
     if (retry) {
       free_workspace();
+      if (std::getenv("RMETIS_B200_VERBOSE"))
+        std::fprintf(stderr, "rmetis_b200: a job ran out of device memory beside others; retrying it alone\n");
       std::lock_guard<std::mutex> lk(mu_);
+      worker_epoch_[idx] = my_epoch;
       job->alone = true;
       queue_.push_front(std::move(job));
     }

@@ -19,7 +19,7 @@ from tests.test_gpu_quality import overshoot
 
 pytestmark = pytest.mark.gpu
 
-DEFAULT_EXACT_MAX_N = 65536
+DEFAULT_EXACT_MAX_N = 16384
 
 
 @pytest.fixture
