@@ -7,7 +7,7 @@
 // weights left by the moves before it), and the moves apply together after
 // the pass. Only the part weights chain the decisions together.
 //
-// Here a pass is decided in two launches:
+// Here a pass is decided in three launches:
 //  1. pick (all movers in parallel): every mover takes the best positive-gain
 //     candidate that is feasible under the start-of-pass weights (its move
 //     alone);
@@ -23,7 +23,9 @@
 //     pass. Should the bound on the rounds be reached first, every part keeps
 //     only what fits without any out-credit, which is within the limit
 //     whatever else moves;
-//  4. apply the admitted moves to part and pw.
+//  4. the new part weights (per part: + admitted in-moves - admitted
+//     out-moves); then, in parallel again, the admitted moves are applied to
+//     the part vector (k_admit_apply).
 // Everything is integer and ordered by vertex id, so the result is the same
 // on every run. The decisions differ from the reference's sequential ones
 // (a part may take a vertex whose room appears only through moves of higher
@@ -67,7 +69,8 @@ struct PickArgs {
   int32_t k;
   int32_t* tgt;
   int32_t* src;
-  int32_t* w;  // [nm][ncon]
+  int32_t* w;      // [nm][ncon]
+  long long* out;  // [k][ncon], zero on entry: weight of the picks out of each part
 };
 
 __global__ void k_admit_pick(PickArgs A) {
@@ -121,6 +124,21 @@ __global__ void k_admit_pick(PickArgs A) {
     }
     A.tgt[j] = t;
     A.src[j] = pv;
+    if (t >= 0)
+      for (int c = 0; c < ncon; ++c) atomic_add_i64(&A.out[(int64_t)pv * ncon + c], vw[c]);
+  }
+}
+
+// The admitted moves of a pass, applied to the part vector: mover j moves to
+// its target when its rank in the target's in-list is below the part's
+// admitted prefix.
+__global__ void k_admit_apply(const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
+                              const int32_t* __restrict__ tgt, const int32_t* __restrict__ rank,
+                              const int32_t* __restrict__ cut, idx_t* __restrict__ part) {
+  const int32_t nm = *nm_dev;
+  RMB_GRID_STRIDE(j, nm) {
+    const int32_t t = tgt[j];
+    if (t >= 0 && rank[j] < cut[t]) part[movers[j]] = t;
   }
 }
 
@@ -129,10 +147,8 @@ __global__ void k_admit_pick(PickArgs A) {
 // ---------------------------------------------------------------------------
 struct AdmitArgs {
   const int32_t* nm_dev;
-  const idx_t* movers;
   int32_t ncon;
   int32_t k;
-  idx_t* part;
   long long* pw;
   const long long* feas;
   int32_t* nmoves;
@@ -141,6 +157,8 @@ struct AdmitArgs {
   const int32_t* src;
   const int32_t* w;
   int32_t* rank;
+  long long* out_g;     // [k][ncon] out-weights of the picks; read, then cleared for the next pass
+  int32_t* cut_g;       // [k] admitted prefix per part, for the apply kernel
   long long* pref_g;    // [nm][ncon] running weight sums in grouped order (when shared memory is short)
   int32_t* src_g;       // [nm] source part in grouped order (same)
 };
@@ -156,7 +174,7 @@ struct AdmitSmem {
     pw = o;   o += 8 * K;
     feas = o; o += 8 * K;
     out = o;  o += 8 * K;
-    wcnt = o; o += 4 * (size_t)kAdmitWarps * k;
+    wcnt = o; o += 4 * (size_t)kAdmitWarps * (k + 1);  // rows padded against bank conflicts
     run = o;  o += 4 * (size_t)k;
     off = o;  o += 4 * ((size_t)k + 1);
     cut = o;  o += 4 * (size_t)k;
@@ -179,21 +197,36 @@ __device__ __forceinline__ long long inlist_sum(const long long* pref, int32_t n
 }
 
 // Largest i <= imax whose first i in-moves fit budget[c] on every
-// constraint (the sums grow with i: vertex weights are positive).
+// constraint (the sums grow with i: vertex weights are positive). The search
+// gallops down from imax: from one round to the next most prefixes stay or
+// lose a few entries.
 __device__ int32_t fit_prefix(const long long* pref, int32_t ncon, int32_t off_p, int32_t imax,
                               const long long* budget) {
   for (int c = 0; c < ncon; ++c)
     if (budget[c] < 0) return 0;
-  int32_t lo = 0, hi = imax;
-  while (lo < hi) {
-    const int32_t mid = lo + (hi - lo + 1) / 2;
-    bool ok = true;
-    for (int c = 0; c < ncon && ok; ++c)
-      if (inlist_sum(pref, ncon, off_p, mid, c) > budget[c]) ok = false;
-    if (ok) lo = mid;
-    else hi = mid - 1;
+  auto fits = [&](int32_t i) {
+    for (int c = 0; c < ncon; ++c)
+      if (inlist_sum(pref, ncon, off_p, i, c) > budget[c]) return false;
+    return true;
+  };
+  if (imax == 0 || fits(imax)) return imax;
+  int32_t bad = imax, good = 0, step = 1;  // fits(good) holds, fits(bad) does not
+  for (;;) {
+    const int32_t probe = bad - step;
+    if (probe <= 0) break;
+    if (fits(probe)) {
+      good = probe;
+      break;
+    }
+    bad = probe;
+    step <<= 1;
   }
-  return lo;
+  while (bad - good > 1) {
+    const int32_t mid = good + (bad - good) / 2;
+    if (fits(mid)) good = mid;
+    else bad = mid;
+  }
+  return good;
 }
 
 __global__ void __launch_bounds__(kAdmitThreads, 1) k_admit(AdmitArgs A) {
@@ -202,27 +235,30 @@ __global__ void __launch_bounds__(kAdmitThreads, 1) k_admit(AdmitArgs A) {
   long long* pw_s = reinterpret_cast<long long*>(smem + L.pw);
   long long* feas_s = reinterpret_cast<long long*>(smem + L.feas);
   long long* out_s = reinterpret_cast<long long*>(smem + L.out);
-  int32_t* wcnt = reinterpret_cast<int32_t*>(smem + L.wcnt);  // [warp][k]
+  int32_t* wcnt = reinterpret_cast<int32_t*>(smem + L.wcnt);  // [warp][k + 1]
   int32_t* run = reinterpret_cast<int32_t*>(smem + L.run);
   int32_t* off = reinterpret_cast<int32_t*>(smem + L.off);
   int32_t* cut = reinterpret_cast<int32_t*>(smem + L.cut);
   int32_t* rlo = reinterpret_cast<int32_t*>(smem + L.lo);
   int32_t* rhi = reinterpret_cast<int32_t*>(smem + L.hi);
   __shared__ long long wsum[kAdmitWarps][2];
-  __shared__ int32_t flag;
+  __shared__ int32_t flag[2];
   __shared__ int32_t warp_tot[kAdmitWarps];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int32_t k = A.k, ncon = A.ncon;
   const int32_t K = k * ncon;
+  const int32_t ks = k + 1;  // row stride of wcnt
   const int32_t nm = *A.nm_dev;
   for (int32_t i = tid; i < K; i += kAdmitThreads) {
     pw_s[i] = A.pw[i];
     feas_s[i] = A.feas[i];
-    out_s[i] = 0;
+    out_s[i] = A.out_g[i];
+    A.out_g[i] = 0;  // the next pass's picks sum into it again
   }
-  for (int32_t i = tid; i < kAdmitWarps * k; i += kAdmitThreads) wcnt[i] = 0;
+  for (int32_t i = tid; i < kAdmitWarps * ks; i += kAdmitThreads) wcnt[i] = 0;
   for (int32_t i = tid; i < k; i += kAdmitThreads) run[i] = 0;
+  if (tid < 2) flag[tid] = 0;
   __syncthreads();
   if (nm == 0) {
     if (tid == 0) {
@@ -232,37 +268,41 @@ __global__ void __launch_bounds__(kAdmitThreads, 1) k_admit(AdmitArgs A) {
     return;
   }
 
-  // ---- stable ranks per target (ascending mover order) and out-weights ----
+  // ---- stable ranks per target (ascending mover order), tile by tile; the
+  // next tile's targets are loaded while this one is ranked ----
+  int32_t t_next = tid < nm ? A.tgt[tid] : -1;
   for (int32_t base = 0; base < nm; base += kAdmitThreads) {
     const int32_t j = base + tid;
-    const int32_t t = j < nm ? A.tgt[j] : -1;
-    if (t >= 0) {
-      const int32_t sp = A.src[j];
-      for (int c = 0; c < ncon; ++c) atomic_add_i64(&out_s[sp * ncon + c], A.w[(int64_t)j * ncon + c]);
-    }
+    const int32_t t = t_next;
+    t_next = j + kAdmitThreads < nm ? A.tgt[j + kAdmitThreads] : -1;
     const unsigned peers = __match_any_sync(0xffffffffu, t);
     const unsigned before = peers & lanemask_lt();
     const int32_t rin = __popc(before);
-    if (t >= 0 && before == 0) wcnt[warp * k + t] = __popc(peers);
+    if (t >= 0 && before == 0) wcnt[warp * ks + t] = __popc(peers);
     __syncthreads();
-    // Per target: bases of the warps in order (entries without movers stay 0).
-    for (int32_t p = tid; p < k; p += kAdmitThreads) {
-      int32_t acc = run[p];
-      for (int w = 0; w < kAdmitWarps; ++w) {
-        const int32_t c = wcnt[w * k + p];
-        if (c) {
-          wcnt[w * k + p] = acc;
-          acc += c;
-        }
+    // Warp w scans targets w, w + 32, ...: lane l holds warp l's count, so a
+    // shuffle scan gives every warp its base (entries without movers stay 0).
+    for (int32_t p = warp; p < k; p += kAdmitWarps) {
+      const int32_t c = wcnt[lane * ks + p];
+      const int32_t base_p = run[p];
+      int32_t x = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
       }
-      run[p] = acc;
+      if (c) wcnt[lane * ks + p] = base_p + x - c;
+      __syncwarp();
+      if (lane == 31) run[p] = base_p + x;
     }
     __syncthreads();
-    if (t >= 0) A.rank[j] = wcnt[warp * k + t] + rin;
+    if (t >= 0) A.rank[j] = wcnt[warp * ks + t] + rin;
     __syncwarp();
-    if (t >= 0 && before == 0) wcnt[warp * k + t] = 0;
-    __syncthreads();
+    // Only this warp's leaders write its row again (next tile, after the
+    // first barrier), so no barrier is needed here.
+    if (t >= 0 && before == 0) wcnt[warp * ks + t] = 0;
   }
+  __syncthreads();
 
   // ---- offsets of the in-lists: exclusive scan of the counts over parts ----
   {
@@ -348,35 +388,10 @@ __global__ void __launch_bounds__(kAdmitThreads, 1) k_admit(AdmitArgs A) {
   }
   __syncthreads();
 
-  // ---- admission rounds ----
-  int rounds = 0;
-  bool converged = false;
-  while (rounds < kAdmitMaxRounds) {
-    ++rounds;
-    if (tid == 0) flag = 0;
-    __syncthreads();
-    for (int32_t p = tid; p < k; p += kAdmitThreads) {
-      long long budget[8];
-      for (int c = 0; c < ncon; ++c) {
-        const int32_t x = p * ncon + c;
-        budget[c] = feas_s[x] - pw_s[x] + out_s[x];
-      }
-      const int32_t old = cut[p];
-      const int32_t now = old > 0 ? fit_prefix(pref, ncon, off[p], old, budget) : 0;
-      rlo[p] = now;
-      rhi[p] = old;
-      if (now < old) {
-        cut[p] = now;
-        flag = 1;
-      }
-    }
-    __syncthreads();
-    if (!flag) {
-      converged = true;
-      break;
-    }
-    // Movers dropped in this round stay home: their parts lose that
-    // out-credit. A warp walks each part's dropped range.
+  // ---- admission rounds: new prefixes from the out-credit (barrier), then
+  // the dropped moves return their credit (barrier) ----
+  // A warp walks each part's dropped range [rlo, rhi).
+  auto return_credit = [&]() {
     for (int32_t p = warp; p < k; p += kAdmitWarps) {
       const int32_t o = off[p];
       for (int32_t i = rlo[p] + lane; i < rhi[p]; i += 32) {
@@ -388,37 +403,68 @@ __global__ void __launch_bounds__(kAdmitThreads, 1) k_admit(AdmitArgs A) {
         }
       }
     }
+  };
+  int rounds = 0;
+  bool converged = false;
+  while (rounds < kAdmitMaxRounds) {
+    const int fb = rounds & 1;
+    ++rounds;
+    for (int32_t p = tid; p < k; p += kAdmitThreads) {
+      long long budget[8];
+      for (int c = 0; c < ncon; ++c) {
+        const int32_t x = p * ncon + c;
+        budget[c] = feas_s[x] - pw_s[x] + out_s[x];
+      }
+      const int32_t old = cut[p];
+      const int32_t now = fit_prefix(pref, ncon, off[p], old, budget);
+      rlo[p] = now;
+      rhi[p] = old;
+      if (now < old) {
+        cut[p] = now;
+        flag[fb] = 1;
+      }
+    }
+    // The other flag was last read before the previous round's second
+    // barrier; clear it for the next round.
+    if (tid == 0) flag[fb ^ 1] = 0;
+    __syncthreads();
+    if (!flag[fb]) {
+      converged = true;
+      break;
+    }
+    return_credit();
     __syncthreads();
   }
   if (!converged) {
-    // Keep only what fits with no out-credit at all.
+    // Keep only what fits with no out-credit at all, and return the credit
+    // of what this drops, so that out_s holds the admitted out-weights.
     for (int32_t p = tid; p < k; p += kAdmitThreads) {
       long long budget[8];
       for (int c = 0; c < ncon; ++c) budget[c] = feas_s[p * ncon + c] - pw_s[p * ncon + c];
-      if (cut[p] > 0) cut[p] = fit_prefix(pref, ncon, off[p], cut[p], budget);
+      const int32_t old = cut[p];
+      const int32_t now = fit_prefix(pref, ncon, off[p], old, budget);
+      rlo[p] = now;
+      rhi[p] = old;
+      cut[p] = now;
     }
+    __syncthreads();
+    return_credit();
     __syncthreads();
   }
 
-  // ---- apply the admitted moves ----
+  // ---- new part weights: + the admitted in-moves, - the admitted out-moves ----
   int32_t moved = 0;
-  for (int32_t j = tid; j < nm; j += kAdmitThreads) {
-    const int32_t t = A.tgt[j];
-    if (t >= 0 && A.rank[j] < cut[t]) {
-      const int32_t sp = A.src[j];
-      A.part[A.movers[j]] = t;
-      for (int c = 0; c < ncon; ++c) {
-        const long long wv = A.w[(int64_t)j * ncon + c];
-        atomic_add_i64(&pw_s[t * ncon + c], wv);
-        atomic_add_i64(&pw_s[sp * ncon + c], -wv);
-      }
-      ++moved;
+  for (int32_t p = tid; p < k; p += kAdmitThreads) {
+    for (int c = 0; c < ncon; ++c) {
+      const int32_t x = p * ncon + c;
+      A.pw[x] = pw_s[x] + inlist_sum(pref, ncon, off[p], cut[p], c) - out_s[x];
     }
+    A.cut_g[p] = cut[p];
+    moved += cut[p];
   }
   moved = warp_sum(moved);
   if (lane == 0) warp_tot[warp] = moved;
   __syncthreads();
-  for (int32_t i = tid; i < K; i += kAdmitThreads) A.pw[i] = pw_s[i];
   if (tid == 0) {
     int32_t s = 0;
     for (int w = 0; w < kAdmitWarps; ++w) s += warp_tot[w];
@@ -457,14 +503,14 @@ int admit_cut_pass(const DGraph& g, int k, int32_t nmax, const int32_t* nm_dev, 
   P.tgt = s.tgt;
   P.src = s.src;
   P.w = s.w;
-  k_admit_pick<<<grid_for(nmax, 256, 148 * 4), 256, 0, st>>>(P);
+  P.out = s.out;
+  const int blocks = grid_for(nmax, 256, 148 * 4);
+  k_admit_pick<<<blocks, 256, 0, st>>>(P);
   RMB_LAUNCH_CHECK();
   AdmitArgs A;
   A.nm_dev = nm_dev;
-  A.movers = movers;
   A.ncon = g.ncon;
   A.k = k;
-  A.part = part;
   A.pw = pw;
   A.feas = feas;
   A.nmoves = nmoves;
@@ -473,10 +519,14 @@ int admit_cut_pass(const DGraph& g, int k, int32_t nmax, const int32_t* nm_dev, 
   A.src = s.src;
   A.w = s.w;
   A.rank = s.rank;
+  A.out_g = s.out;
+  A.cut_g = s.cut;
   A.pref_g = s.pref;
   A.src_g = s.gsrc;
   allow_dyn_smem((const void*)k_admit, kAdmitMaxSmem);
   k_admit<<<1, kAdmitThreads, kAdmitMaxSmem, st>>>(A);
+  RMB_LAUNCH_CHECK();
+  k_admit_apply<<<blocks, 256, 0, st>>>(nm_dev, movers, s.tgt, s.rank, s.cut, part);
   RMB_LAUNCH_CHECK();
   profiler().end(ph, st, 0.0);
   return ph;

@@ -199,6 +199,8 @@ struct AdmitScratch {
   int32_t* rank = nullptr;     // [n] its place in its target's in-list
   long long* pref = nullptr;   // [n * ncon] running sums (when shared memory is short)
   int32_t* gsrc = nullptr;     // [n] sources in grouped order (same)
+  long long* out = nullptr;    // [k * ncon] out-weights of a pass's picks: zero before the level's first pass
+  int32_t* cut = nullptr;      // [k] admitted prefix per part
 };
 size_t admit_smem_bytes(int k, int ncon);
 bool admit_supported(int k, int ncon);

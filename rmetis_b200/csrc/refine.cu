@@ -1514,6 +1514,9 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
     as.rank = arena.alloc<int32_t>((size_t)g.n);
     as.pref = arena.alloc<long long>((size_t)g.n * g.ncon);
     as.gsrc = arena.alloc<int32_t>((size_t)g.n);
+    as.out = arena.alloc<long long>((size_t)K);
+    as.cut = arena.alloc<int32_t>((size_t)k);
+    RMB_CUDA(cudaMemsetAsync(as.out, 0, sizeof(long long) * (size_t)K, st));
     rounds = arena.alloc<int32_t>((size_t)rp.niter + 1);
   }
   std::vector<int> walk_handles, gain_handles;

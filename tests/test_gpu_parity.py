@@ -13,6 +13,16 @@ from rmetis_b200 import generators as G
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(autouse=True)
+def exact_refinement(rmb):
+    """Every pass of RMETIS_GPU_GreedyRefine the reference's sequential pass:
+    levels above the refine-mode threshold (default 16384 vertices) would
+    otherwise decide their cut passes by parallel admission."""
+    rmb.set_refine_mode(-1)
+    yield
+    rmb.set_refine_mode(16384)
+
+
 def star_graph(n_leaves, hub_extra=0, seed=0):
     """A hub joined to every leaf, leaves chained in a path (heavy rows)."""
     n = n_leaves + 1
