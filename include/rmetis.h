@@ -8,6 +8,7 @@
  *   RMETIS_PartGraphKway       replaces src/ffi/c_api.rs:56-81 (+ c_partition_impl :140-209,
  *                              parse_options :211-222)
  *   RMETIS_PartGraphRecursive  replaces src/ffi/c_api.rs:27-53 (same helpers)
+ *   RMETIS_NodeND              replaces src/ffi/c_api.rs:84-132
  *
  * The k-way path computes on the GPU (CType Shem/Rm, IpType Grow/Random/MetisRb,
  * RType Greedy and Fm). Greedy is refined pass for pass as the reference does;
@@ -77,7 +78,9 @@ RMETIS_API int RMETIS_SetDefaultOptions(idx_t *options);
  * reference), adjwgt[xadj[n]] (unit), tpwgts[nparts*ncon] (1/nparts),
  * ubvec[ncon] (1 + ufactor/1000), options (defaults), objval (not written).
  * The caller owns all buffers; the library copies the inputs and writes only
- * part[0..n) and *objval. */
+ * part[0..n) and *objval. One difference from the reference, which has no
+ * such limit: ncon above 8 returns METIS_ERROR_INPUT (the refinement kernels
+ * hold at most 8 constraints per part). */
 RMETIS_API int RMETIS_PartGraphKway(const idx_t *nvtxs, const idx_t *ncon, const idx_t *xadj, const idx_t *adjncy,
                          const idx_t *vwgt, const idx_t *vsize, const idx_t *adjwgt, const idx_t *nparts,
                          const real_t *tpwgts, const real_t *ubvec, const idx_t *options, idx_t *objval,
@@ -90,16 +93,36 @@ RMETIS_API int RMETIS_PartGraphKway(const idx_t *nvtxs, const idx_t *ncon, const
  * is what its callers pass. The recursion, the f32 target arithmetic and the
  * subgraph extraction follow the reference on the host; each bisection is a
  * 2-way multilevel partition on the GPU (coarsening to 40 vertices, grow
- * trials, refinement). Differences: rtype Fm refines a bisection with the
- * k-way FM rule (positive-gain moves) rather than the reference's 2-way FM
- * (src/refine/fm.rs, which also makes negative moves and rolls back), and
- * bisection i runs with seed + i where the reference draws all bisections
- * from one generator; partitions match the reference's in quality, not bit
- * for bit. */
+ * trials, refinement), and the bisections of one recursion level run
+ * concurrently on the device's worker pool. Differences: rtype Fm refines a
+ * bisection with the k-way FM rule (positive-gain moves) rather than the
+ * reference's 2-way FM (src/refine/fm.rs, which also makes negative moves and
+ * rolls back), and the bisection at position h of the recursion tree (root 0,
+ * children 2h+1, 2h+2) runs with seed + h where the reference draws all
+ * bisections from one generator; partitions match the reference's in quality,
+ * not bit for bit. Graphs with more than 8 constraints return
+ * METIS_ERROR_INPUT (as RMETIS_PartGraphKway). */
 RMETIS_API int RMETIS_PartGraphRecursive(const idx_t *nvtxs, const idx_t *ncon, const idx_t *xadj,
                                          const idx_t *adjncy, const idx_t *vwgt, const idx_t *vsize,
                                          const idx_t *adjwgt, const idx_t *nparts, const real_t *tpwgts,
                                          const real_t *ubvec, const idx_t *options, idx_t *objval, idx_t *part);
+
+/* Nested dissection ordering (replaces src/ffi/c_api.rs:84-132, node_nd
+ * src/partition/nd.rs:16-111, find_node_separator src/separator/mod.rs:10-61).
+ * nvtxs, xadj, adjncy, perm and iperm are required (NULL or nvtxs <= 0 ->
+ * METIS_ERROR_INPUT); vwgt[nvtxs] and options are optional; a graph failing
+ * validation returns METIS_ERROR_INPUT. Writes perm[v] = new position of
+ * vertex v and iperm = its inverse. A graph of more than 100 vertices is
+ * bisected (targets 0.5/0.5, ubvec 1.05, the caller's options and seed), the
+ * boundary of the lighter side becomes the separator, and the two sides are
+ * ordered recursively (lighter side first) before the separator, as the
+ * reference does. Each bisection is a 2-way multilevel partition on the GPU;
+ * the bisections of one recursion level run concurrently on the device's
+ * worker pool. The bisections differ from the reference's (parallel matching,
+ * the k-way refinement rules for rtype Fm), so orderings match it in quality
+ * (separator sizes, fill), not bit for bit. */
+RMETIS_API int RMETIS_NodeND(const idx_t *nvtxs, const idx_t *xadj, const idx_t *adjncy, const idx_t *vwgt,
+                             const idx_t *options, idx_t *perm, idx_t *iperm);
 
 /* ---- GPU extensions ---------------------------------------------------- */
 
@@ -141,6 +164,14 @@ RMETIS_API int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summe
  * results are compared by quality. -1 = exact everywhere. Returns
  * METIS_ERROR_INPUT for values below -1. */
 RMETIS_API int RMETIS_GPU_SetRefineMode(int exact_max_n);
+
+/* Kernel shapes that never change a result (no counterpart in the
+ * reference): contract_thread_max (16 or 32) is the longest merged-row bound
+ * a single thread merges in registers during contraction (longer rows go to
+ * a warp each); gain_block (128, 256 or 512) is the block size of the
+ * gain-table kernel. -1 leaves a knob unchanged; other values return
+ * METIS_ERROR_INPUT. rmetis_b200/autotune.py measures them. */
+RMETIS_API int RMETIS_GPU_SetKernelShapes(int contract_thread_max, int gain_block);
 
 /* The last two knobs of RMETIS_GPU_SetTuning for jobs that share the device
  * with other jobs: the graphs of RMETIS_GPU_PartGraphKwayBatch and requests of

@@ -20,6 +20,7 @@ from ._lib import F32P, F64P, I32P, I64P
 __all__ = [
     "CType", "IpType", "RType", "ObjType", "Options", "Graph", "PartitionResult", "MetisError", "InputError",
     "OutOfMemoryError", "InternalError", "part_graph_kway", "part_graph_recursive", "set_default_options",
+    "node_nd", "NDResult",
     "METIS_OK",
     "METIS_ERROR_INPUT", "METIS_ERROR_MEMORY", "METIS_ERROR", "METIS_NOPTIONS",
 ]
@@ -402,6 +403,13 @@ def set_refine_mode(exact_max_n: int = 16384):
     _raise_for(_lib.load().RMETIS_GPU_SetRefineMode(exact_max_n), "set_refine_mode")
 
 
+def set_kernel_shapes(contract_thread_max: int = -1, gain_block: int = -1):
+    """Result-neutral kernel shapes: the longest merged-row bound one thread
+    merges in contraction (16 or 32) and the gain-table block size (128, 256
+    or 512); -1 leaves a knob unchanged."""
+    _raise_for(_lib.load().RMETIS_GPU_SetKernelShapes(contract_thread_max, gain_block), "set_kernel_shapes")
+
+
 def set_pool_tuning(fused_max_n: int = -2, tail_max_n: int = -2):
     """Launch-shape knobs for batch graphs and submitted requests, which share
     the device with other jobs (-1 = the set_tuning value, -2 leaves a knob
@@ -503,6 +511,30 @@ def submit_kway(graph: Graph, nparts: int, tpwgts=None, ubvec=None, options: Opt
     if t <= 0:
         _raise_for(int(t), "submit_kway")
     return KwayRequest(t, (graph, opts, nv, nc, npr, tp, ub), part, obj)
+
+
+@dataclass
+class NDResult:
+    """Nested dissection ordering (src/types.rs:133-137): perm[v] is the new
+    position of vertex v, iperm its inverse."""
+    perm: np.ndarray
+    iperm: np.ndarray
+
+
+def node_nd(graph: Graph, options: Options | None = None) -> NDResult:
+    """Nested dissection ordering (src/partition/nd.rs:16-44) through
+    RMETIS_NodeND: separators from GPU bisections of each subgraph, lighter
+    side first, separator last. The graph's vertex weights (constraint 0) are
+    used; edge weights are not (the reference's C entry has none)."""
+    options = options or Options()
+    n = graph.nvtxs
+    perm = np.zeros(n, np.int32)
+    iperm = np.zeros(n, np.int32)
+    vw = None if graph.vwgt is None else np.ascontiguousarray(graph.vwgt.reshape(n, graph.ncon)[:, 0])
+    rc = _lib.load().RMETIS_NodeND(ctypes.byref(ctypes.c_int32(n)), _p(graph.xadj), _p(graph.adjncy), _p(vw),
+                                   _p(options.c_array()), _p(perm), _p(iperm))
+    _raise_for(rc, "node_nd")
+    return NDResult(perm=perm, iperm=iperm)
 
 
 from .graphio import format_metis_graph, parse_metis_graph, read_metis_graph, write_metis_graph  # noqa: E402

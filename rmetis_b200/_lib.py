@@ -19,11 +19,13 @@ SIGNATURES = {
     "RMETIS_SetDefaultOptions": [I32P],
     "RMETIS_PartGraphKway": [I32P, I32P, I32P, I32P, I32P, I32P, I32P, I32P, F32P, F32P, I32P, I32P, I32P],
     "RMETIS_PartGraphRecursive": [I32P, I32P, I32P, I32P, I32P, I32P, I32P, I32P, F32P, F32P, I32P, I32P, I32P],
+    "RMETIS_NodeND": [I32P, I32P, I32P, I32P, I32P, I32P, I32P],
     "RMETIS_GPU_PartGraphKwayDevice": [I32P, I32P, VP, VP, VP, VP, I32P, F32P, F32P, I32P, I32P, VP],
     "RMETIS_GPU_SetStream": [VP],
     "RMETIS_GPU_SetTuning": [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int],
     "RMETIS_GPU_SetPoolTuning": [ctypes.c_int, ctypes.c_int],
     "RMETIS_GPU_SetRefineMode": [ctypes.c_int],
+    "RMETIS_GPU_SetKernelShapes": [ctypes.c_int, ctypes.c_int],
     "RMETIS_GPU_SetProfiling": [ctypes.c_int],
     "RMETIS_GPU_GetProfile": [I64P, F64P, F64P, ctypes.c_int],
     "RMETIS_GPU_PartGraphKwayTrace": [I32P, I32P, I32P, I32P, I32P, I32P, I32P, F32P, F32P, I32P, I32P, I32P,

@@ -1,29 +1,41 @@
-"""Autotuner for the engine's launch-shape knobs.
+"""Autotuner for the engine's launch-shape, kernel-shape and refinement knobs.
 
-Two knobs decide how the engine launches the small levels of a hierarchy, and
-neither changes a result (the same kernel bodies run either way, tested
-bit-identical in tests/test_gpu_fused.py and tests/test_gpu_tail.py):
+Result-neutral knobs (the same kernel bodies run either way; tested
+bit-identical in tests/test_gpu_fused.py, tests/test_gpu_tail.py and the
+contraction parity tests):
 
 * ``fused_max_n``: a level of at most this many vertices (and at most 4 times
   as many adjacency entries) is refined by one single-block launch instead of
   a sequence of grid-wide kernels per pass;
 * ``tail_max_n``: from a level of at most this many vertices (and at most 64
   times as many adjacency entries) on, every remaining coarsening level runs
-  in one single-block launch.
+  in one single-block launch;
+* ``contract_thread_max`` (16 or 32): the degree bucket of contraction, the
+  longest merged-row bound one thread merges in registers; longer rows go to
+  a warp each (thread-vs-warp per coarse vertex);
+* ``gain_block`` (128, 256, 512): the block size of the gain-table kernel.
 
 A single-block launch saves launches and host round trips but runs on one SM.
 In a lone call the rest of the device idles meanwhile; jobs that share the
 device (the graphs of a batch, served requests) fill it. The best sizes
-therefore depend on the device and on the concurrency, and the two modes are
-tuned separately: ``plain`` (single calls, ``set_tuning``) and ``pool``
-(batch graphs and submitted requests, ``set_pool_tuning``).
+therefore depend on the device and on the concurrency, and the launch shapes
+are tuned separately for ``plain`` (single calls, ``set_tuning``) and
+``pool`` (batch graphs and submitted requests, ``set_pool_tuning``); the
+kernel shapes are device-wide (``set_kernel_shapes``) and tuned in plain
+mode.
 
-For each candidate setting the tuner runs a workload, checks that every
-result (objval and part vector) equals the first candidate's -- a difference
-means a knob is not neutral and raises ``TuningMismatch`` -- and keeps the
-best of ``repeats`` wall-clock times. The fastest candidate wins; a table
-maps the device name to the winner of each mode, and ``apply()`` sets them
-for the current device when the table has an entry for it.
+One knob changes results: ``exact_max_n``, the largest level whose greedy
+cut passes decide sequentially (larger levels decide by parallel admission,
+``set_refine_mode``). It is tuned for speed under a quality gate: a setting
+is eligible when its summed cut over the plain workload is within
+``QUALITY_TOL`` of the summed cut with sequential passes everywhere.
+
+For each result-neutral candidate the tuner runs a workload, checks that
+every result (objval and part vector) equals the first candidate's -- a
+difference means a knob is not neutral and raises ``TuningMismatch`` -- and
+keeps the best of ``repeats`` wall-clock times. The fastest candidate wins; a
+table maps the device name to the winner of each mode, and ``apply()`` sets
+them for the current device when the table has an entry for it.
 
     python -m rmetis_b200.autotune --mode both --out rmetis_b200/tuning.json
 """
@@ -45,6 +57,11 @@ DEFAULT_TABLE = os.path.join(HERE, "tuning.json")
 FUSED_CANDIDATES = (0, 1024, 2048, 4096, 8192)
 TAIL_CANDIDATES = (0, 1024, 4096, 16384)
 DEFAULTS = {"fused_max_n": 4096, "tail_max_n": 4096}
+SHAPE_CANDIDATES = {"contract_thread_max": (16, 32), "gain_block": (128, 256, 512)}
+SHAPE_DEFAULTS = {"contract_thread_max": 32, "gain_block": 256}
+EXACT_CANDIDATES = (4096, 8192, 16384, 32768, 65536)
+EXACT_DEFAULT = 16384
+QUALITY_TOL = 0.005
 
 
 class TuningMismatch(RuntimeError):
@@ -67,6 +84,40 @@ def candidates(fused=FUSED_CANDIDATES, tail=TAIL_CANDIDATES):
         if s != out[0]:
             out.append(s)
     return out
+
+
+def shape_candidates():
+    """Every kernel-shape pair, the engine defaults first."""
+    out = [dict(SHAPE_DEFAULTS)]
+    for c, b in itertools.product(SHAPE_CANDIDATES["contract_thread_max"], SHAPE_CANDIDATES["gain_block"]):
+        s = {"contract_thread_max": int(c), "gain_block": int(b)}
+        if s != out[0]:
+            out.append(s)
+    return out
+
+
+def tune_quality(run, values, repeats: int = 3, tol: float = QUALITY_TOL, log=None):
+    """The result-changing knob: run(value) for the reference value -1 (every
+    pass sequential) and each candidate; a candidate whose summed objval is
+    within `tol` of the reference's is eligible. Returns (eligible trials
+    fastest first, all trials with their cut ratios)."""
+    ref = sum(int(r.objval) for r in run(-1))
+    trials, eligible = [], []
+    for v in values:
+        out = run(v)  # warm-up; the cut of this setting
+        cut = sum(int(r.objval) for r in out)
+        times = []
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            run(v)
+            times.append(time.perf_counter() - t0)
+        tr = Trial({"exact_max_n": int(v), "cut_ratio": round(cut / max(1, ref), 5)}, min(times), times)
+        trials.append(tr)
+        if cut <= (1.0 + tol) * ref:
+            eligible.append(tr)
+        if log:
+            log(f"  exact_max_n={v}: {tr.seconds * 1e3:.2f} ms, cut {cut} ({cut / max(1, ref):.4f} of sequential)")
+    return sorted(eligible, key=lambda t: t.seconds), trials
 
 
 def digest(results) -> list:
@@ -149,8 +200,21 @@ def plain_runner(graphs, options=None):
     o = options or rmb.Options(rtype=rmb.RType.Greedy, seed=7)
 
     def run(s):
-        rmb.set_tuning(fused_max_n=s["fused_max_n"], tail_max_n=s["tail_max_n"])
+        if "fused_max_n" in s:
+            rmb.set_tuning(fused_max_n=s["fused_max_n"], tail_max_n=s["tail_max_n"])
+        if "contract_thread_max" in s:
+            rmb.set_kernel_shapes(s["contract_thread_max"], s["gain_block"])
         return [rmb.part_graph_kway(g, k, options=o) for g, k in graphs]
+    return run
+
+
+def exact_runner(graphs, options=None):
+    import rmetis_b200 as rmb
+    inner = plain_runner(graphs, options)
+
+    def run(v):
+        rmb.set_refine_mode(v)
+        return inner({})
     return run
 
 
@@ -209,13 +273,22 @@ def apply(path: str = DEFAULT_TABLE, device: str | None = None, setters=None) ->
         return {}
     if setters is None:
         import rmetis_b200 as rmb
-        setters = {"plain": rmb.set_tuning, "pool": rmb.set_pool_tuning}
+        setters = {"plain": rmb.set_tuning, "pool": rmb.set_pool_tuning, "shapes": rmb.set_kernel_shapes,
+                   "refine": rmb.set_refine_mode}
     applied = {}
-    for mode, fn in setters.items():
-        if mode in entry:
+    for mode in ("plain", "pool"):
+        if mode in entry and mode in setters:
             s = entry[mode]["setting"]
-            fn(fused_max_n=int(s["fused_max_n"]), tail_max_n=int(s["tail_max_n"]))
-            applied[mode] = dict(s)
+            setters[mode](fused_max_n=int(s["fused_max_n"]), tail_max_n=int(s["tail_max_n"]))
+            applied[mode] = {"fused_max_n": int(s["fused_max_n"]), "tail_max_n": int(s["tail_max_n"])}
+    if "shapes" in entry and "shapes" in setters:
+        s = entry["shapes"]["setting"]
+        setters["shapes"](int(s["contract_thread_max"]), int(s["gain_block"]))
+        applied["shapes"] = {"contract_thread_max": int(s["contract_thread_max"]), "gain_block": int(s["gain_block"])}
+    if "refine" in entry and "refine" in setters:
+        v = int(entry["refine"]["setting"]["exact_max_n"])
+        setters["refine"](v)
+        applied["refine"] = {"exact_max_n": v}
     return applied
 
 
@@ -239,6 +312,23 @@ def main(argv=None):
                    note="sum over: 64x64 grid k=8, weighted 64^3 grid k=64, RGG n=20000 ncon=2 k=16"
                         + ("" if args.small else ", weighted 128^3 grid k=64") + "; host-buffer calls")
         print(f"plain winner {trials[0].setting} {trials[0].seconds * 1e3:.2f} ms", flush=True)
+        rmb.set_tuning(**trials[0].setting)
+        shapes = shape_candidates()
+        print(f"kernel shapes ({len(shapes)} settings)", flush=True)
+        st = tune(plain_runner(wl), shapes, args.repeats, log=print)
+        save_entry(args.out, dev, "shapes", st, note="plain workload, launch shapes of the plain winner")
+        rmb.set_kernel_shapes(**st[0].setting)
+        print(f"shapes winner {st[0].setting} {st[0].seconds * 1e3:.2f} ms", flush=True)
+        elig, all_trials = tune_quality(exact_runner(wl), EXACT_CANDIDATES, args.repeats, log=print)
+        best = elig if elig else [t for t in all_trials if t.setting["exact_max_n"] == max(EXACT_CANDIDATES)]
+        rest = [t for t in sorted(all_trials, key=lambda t: t.seconds) if t is not best[0]]
+        save_entry(args.out, dev, "refine", [best[0]] + rest,
+                   note=f"fastest exact_max_n whose summed cut is within {QUALITY_TOL:.1%} of sequential passes "
+                        "everywhere (cut_ratio)")
+        rmb.set_refine_mode(EXACT_DEFAULT)
+        rmb.set_kernel_shapes(**SHAPE_DEFAULTS)
+        rmb.set_tuning(**DEFAULTS)
+        print(f"refine winner {best[0].setting} {best[0].seconds * 1e3:.2f} ms", flush=True)
     if args.mode in ("pool", "both"):
         print(f"pool ({len(settings)} settings, {args.graphs} graphs) on {dev}", flush=True)
         graphs, ks = pool_workload(args.graphs)

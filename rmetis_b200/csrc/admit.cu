@@ -484,7 +484,7 @@ bool admit_supported(int k, int ncon) {
 int admit_cut_pass(const DGraph& g, int k, int32_t nmax, const int32_t* nm_dev, const idx_t* movers,
                    const idx_t* ncand, const idx_t* wfrom, const idx_t* cand_p, const idx_t* cand_g, idx_t* part,
                    long long* pw, const long long* feas, int32_t* nmoves, int32_t* rounds_out,
-                   const AdmitScratch& s, cudaStream_t st) {
+                   const AdmitScratch& s, cudaStream_t st, bool apply) {
   const int ph = profiler().begin(kProfAdmit, st);
   PickArgs P;
   P.nm_dev = nm_dev;
@@ -526,8 +526,10 @@ int admit_cut_pass(const DGraph& g, int k, int32_t nmax, const int32_t* nm_dev, 
   allow_dyn_smem((const void*)k_admit, kAdmitMaxSmem);
   k_admit<<<1, kAdmitThreads, kAdmitMaxSmem, st>>>(A);
   RMB_LAUNCH_CHECK();
-  k_admit_apply<<<blocks, 256, 0, st>>>(nm_dev, movers, s.tgt, s.rank, s.cut, part);
-  RMB_LAUNCH_CHECK();
+  if (apply) {
+    k_admit_apply<<<blocks, 256, 0, st>>>(nm_dev, movers, s.tgt, s.rank, s.cut, part);
+    RMB_LAUNCH_CHECK();
+  }
   profiler().end(ph, st, 0.0);
   return ph;
 }

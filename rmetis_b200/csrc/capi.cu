@@ -1,5 +1,6 @@
 // extern "C" boundary: the reference's C ABI (src/ffi/c_api.rs) plus the GPU
 // extensions declared in include/rmetis.h.
+#include <future>
 #include <algorithm>
 #include <chrono>
 #include <cstdlib>
@@ -42,6 +43,8 @@ struct Tuning {
   int fused_max_n = 4096;
   int tail_max_n = 4096;
   int exact_max_n = 16384;
+  int contract_thread_max = 32;
+  int gain_block = 256;
 };
 Tuning& tuning() {
   static Tuning t;
@@ -56,6 +59,8 @@ void apply_tuning(KwayOptions& o) {
   o.fused_max_n = tuning().fused_max_n;
   o.tail_max_n = tuning().tail_max_n;
   o.exact_max_n = tuning().exact_max_n;
+  o.contract_thread_max = tuning().contract_thread_max;
+  o.gain_block = tuning().gain_block;
 }
 
 // Launch-shape knobs of jobs that share the device with other jobs (batch
@@ -290,44 +295,115 @@ void bisect(Engine& E, const HostGraph& g, const std::vector<float>& tp2, const 
   RMB_CUDA(cudaStreamSynchronize(E.stream()));
 }
 
-// rb_recurse (recursive.rs:61-131). The reference draws every bisection's
-// random choices from one generator; here bisection i (in the recursion's
-// order) runs with seed + i (0 stays 0: an entropy seed per bisection).
-void rb_recurse(Engine& E, const HostGraph& g, int32_t nparts, int32_t offset, const std::vector<float>& tp,
-                const real_t* ubvec, const KwayOptions& o, uint64_t& counter, std::vector<idx_t>& part) {
-  if (nparts == 1) {
-    for (int32_t v = 0; v < g.n; ++v) part[v] = offset;
-    return;
+
+// ---- independent bisections at once --------------------------------------
+// The subgraphs of one level of a recursion do not depend on each other:
+// their bisections run concurrently on the device's worker pool (each worker
+// has its own stream and workspace), instead of one after another.
+struct BisectJob {
+  const HostGraph* g = nullptr;
+  std::vector<float> tp2;
+  uint64_t seed = 0;
+  std::vector<idx_t> part;
+};
+
+void bisect_all(std::vector<BisectJob>& jobs, const real_t* ubvec, const KwayOptions& o) {
+  if (jobs.empty()) return;
+  int dev = 0;
+  RMB_CUDA(cudaGetDevice(&dev));
+  WorkerPool& pool = pool_for_device(dev);
+  std::vector<std::future<int>> fut;
+  fut.reserve(jobs.size());
+  for (BisectJob& j : jobs) {
+    BisectJob* jp = &j;
+    fut.push_back(pool.submit(footprint_bytes(j.g->n, j.g->xadj[j.g->n], 2, j.g->ncon), [jp, ubvec, &o](Engine& W) {
+      bisect(W, *jp->g, jp->tp2, ubvec, o, jp->seed, jp->part);
+      return 1;
+    }));
   }
-  if (g.n <= nparts) {
-    for (int32_t v = 0; v < g.n; ++v) part[v] = offset + std::min(v, nparts - 1);
-    return;
+  int rc = 1;
+  for (auto& f : fut) {
+    const int r = f.get();
+    if (r != 1 && rc == 1) rc = r;
   }
-  const int32_t k1 = nparts / 2, k2 = nparts - k1, nc = g.ncon;
-  std::vector<float> lw(nc, 0.0f), rw(nc, 0.0f);
-  for (int c = 0; c < nc; ++c) {
-    for (int32_t i = c; i < k1 * nc; i += nc) lw[c] += tp[i];
-    for (int32_t i = k1 * nc + c; i < nparts * nc; i += nc) rw[c] += tp[i];
+  if (rc != 1) throw Error(rc, "a bisection failed");
+}
+
+// rb_recurse (recursive.rs:61-131), one recursion level at a time: a node
+// with nparts parts is bisected with the summed f32 targets of its halves
+// (k1 = nparts / 2), both sides are extracted as subgraphs and become the next
+// level's nodes with their targets divided by constraint 0's sum; a node with
+// one part, or no more vertices than parts, is assigned directly. The
+// bisections of a level run concurrently (bisect_all). The reference draws
+// every bisection from one generator; here the bisection at position h of the
+// recursion tree (root 0, children 2h+1 and 2h+2) runs with seed + h (0 stays
+// 0: an entropy seed per bisection).
+struct RbNode {
+  HostGraph g;
+  std::vector<int32_t> orig;
+  int32_t nparts = 2, offset = 0;
+  std::vector<float> tp;
+  uint64_t heap = 0;
+};
+
+void rb_levels(RbNode root, const real_t* ubvec, const KwayOptions& o, std::vector<idx_t>& part) {
+  std::vector<RbNode> frontier;
+  frontier.push_back(std::move(root));
+  while (!frontier.empty()) {
+    std::vector<RbNode*> split;
+    std::vector<BisectJob> jobs;
+    for (RbNode& nd : frontier) {
+      if (nd.nparts == 1) {
+        for (int32_t v : nd.orig) part[v] = nd.offset;
+        continue;
+      }
+      if (nd.g.n <= nd.nparts) {
+        for (int32_t v = 0; v < nd.g.n; ++v) part[nd.orig[v]] = nd.offset + std::min(v, nd.nparts - 1);
+        continue;
+      }
+      split.push_back(&nd);
+    }
+    jobs.resize(split.size());
+    std::vector<std::vector<float>> lws(split.size()), rws(split.size());
+    for (size_t i = 0; i < split.size(); ++i) {
+      const RbNode& nd = *split[i];
+      const int32_t k1 = nd.nparts / 2, nc = nd.g.ncon;
+      std::vector<float>& lw = lws[i];
+      std::vector<float>& rw = rws[i];
+      lw.assign(nc, 0.0f);
+      rw.assign(nc, 0.0f);
+      for (int c = 0; c < nc; ++c) {
+        for (int32_t t = c; t < k1 * nc; t += nc) lw[c] += nd.tp[t];
+        for (int32_t t = k1 * nc + c; t < nd.nparts * nc; t += nc) rw[c] += nd.tp[t];
+      }
+      const float total = lw[0] + rw[0];
+      for (int c = 0; c < nc; ++c) jobs[i].tp2.push_back(lw[c] / total);
+      for (int c = 0; c < nc; ++c) jobs[i].tp2.push_back(rw[c] / total);
+      jobs[i].g = &nd.g;
+      jobs[i].seed = o.seed == 0 ? 0 : o.seed + nd.heap;
+    }
+    bisect_all(jobs, ubvec, o);
+    std::vector<RbNode> next;
+    for (size_t i = 0; i < split.size(); ++i) {
+      const RbNode& nd = *split[i];
+      const int32_t k1 = nd.nparts / 2, k2 = nd.nparts - k1, nc = nd.g.ncon;
+      for (int side = 0; side < 2; ++side) {
+        RbNode ch;
+        std::vector<int32_t> n2o;
+        ch.g = extract_sub(nd.g, jobs[i].part, side, n2o);
+        ch.orig.resize(n2o.size());
+        for (size_t t = 0; t < n2o.size(); ++t) ch.orig[t] = nd.orig[n2o[t]];
+        ch.nparts = side == 0 ? k1 : k2;
+        ch.offset = side == 0 ? nd.offset : nd.offset + k1;
+        const float div = side == 0 ? lws[i][0] : rws[i][0];
+        for (int32_t t = side == 0 ? 0 : k1 * nc; t < (side == 0 ? k1 * nc : nd.nparts * nc); ++t)
+          ch.tp.push_back(nd.tp[t] / div);
+        ch.heap = 2 * nd.heap + 1 + (uint64_t)side;
+        next.push_back(std::move(ch));
+      }
+    }
+    frontier = std::move(next);
   }
-  const float total = lw[0] + rw[0];
-  std::vector<float> bis;
-  for (int c = 0; c < nc; ++c) bis.push_back(lw[c] / total);
-  for (int c = 0; c < nc; ++c) bis.push_back(rw[c] / total);
-  std::vector<idx_t> bp;
-  const uint64_t seed = o.seed == 0 ? 0 : o.seed + counter;
-  ++counter;
-  bisect(E, g, bis, ubvec, o, seed, bp);
-  std::vector<int32_t> n2o0, n2o1;
-  HostGraph g0 = extract_sub(g, bp, 0, n2o0);
-  HostGraph g1 = extract_sub(g, bp, 1, n2o1);
-  std::vector<float> ltp, rtp;
-  for (int32_t i = 0; i < k1 * nc; ++i) ltp.push_back(tp[i] / lw[0]);
-  for (int32_t i = k1 * nc; i < nparts * nc; ++i) rtp.push_back(tp[i] / rw[0]);
-  std::vector<idx_t> sp0((size_t)g0.n, 0), sp1((size_t)g1.n, 0);
-  rb_recurse(E, g0, k1, 0, ltp, ubvec, o, counter, sp0);
-  rb_recurse(E, g1, k2, 0, rtp, ubvec, o, counter, sp1);
-  for (size_t i = 0; i < n2o0.size(); ++i) part[n2o0[i]] = sp0[i] + offset;
-  for (size_t i = 0; i < n2o1.size(); ++i) part[n2o1[i]] = sp1[i] + offset + k1;
 }
 
 int recursive_host(const idx_t* nvtxs, const idx_t* ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
@@ -377,8 +453,13 @@ int recursive_host(const idx_t* nvtxs, const idx_t* ncon, const idx_t* xadj, con
   if (tpwgts) tp.assign(tpwgts, tpwgts + (size_t)np * nc);
   else tp.assign((size_t)np * nc, 1.0f / (float)np);  // recursive.rs:38-43
   std::vector<idx_t> out((size_t)n, 0);
-  uint64_t counter = 0;
-  rb_recurse(E, g, np, 0, tp, ubvec, o, counter, out);
+  RbNode root;
+  root.g = std::move(g);
+  root.orig.resize(n);
+  for (int32_t v = 0; v < n; ++v) root.orig[v] = v;
+  root.nparts = np;
+  root.tp = std::move(tp);
+  rb_levels(std::move(root), ubvec, o, out);
   // edge_cut (src/graph/mod.rs:123-137): i32 sum over both directions, / 2.
   uint32_t cut = 0;
   for (int32_t v = 0; v < n; ++v)
@@ -386,6 +467,144 @@ int recursive_host(const idx_t* nvtxs, const idx_t* ncon, const idx_t* xadj, con
       if (out[adjncy[j]] != out[v]) cut += (uint32_t)(adjwgt ? adjwgt[j] : 1);
   std::memcpy(part, out.data(), sizeof(idx_t) * (size_t)n);
   if (objval) *objval = (idx_t)cut / 2;
+  return METIS_OK;
+}
+
+// ---- nested dissection (src/partition/nd.rs:16-111, src/separator/mod.rs:10-61)
+// The reference recurses depth first: a graph of more than 100 vertices is
+// bisected by partition_recursive (targets 0.5/0.5, ubvec 1.05, the caller's
+// options, so every bisection starts from options.seed), the boundary of the
+// lighter side (constraint 0, ties to side 0) becomes the separator, and the
+// two sides without it are ordered first (lighter side first), the separator
+// last; a separator of n/2 vertices or more, or a graph of at most 100
+// vertices, is ordered as it stands. Here the recursion tree is built level by
+// level, every bisection of a level at once on the worker pool; the numbering
+// is then assigned in the reference's depth-first order.
+struct NdNode {
+  HostGraph g;
+  std::vector<int32_t> orig;  // original id of each local vertex
+  int left = -1, right = -1;  // children (node indices), -1 if none
+  std::vector<int32_t> sep;   // local ids of the separator, ascending
+  bool leaf = true;
+};
+
+constexpr int32_t kNdThreshold = 100;  // nd.rs:13
+
+void nd_order(std::vector<NdNode>& nodes, const KwayOptions& o) {
+  const real_t ub[1] = {1.05f};  // separator/mod.rs:21
+  std::vector<int> frontier{0};
+  while (!frontier.empty()) {
+    std::vector<int> split;
+    for (int id : frontier)
+      if (nodes[id].g.n > kNdThreshold) split.push_back(id);
+    std::vector<BisectJob> jobs(split.size());
+    for (size_t i = 0; i < split.size(); ++i) {
+      jobs[i].g = &nodes[split[i]].g;
+      jobs[i].tp2 = {0.5f, 0.5f};
+      jobs[i].seed = o.seed;
+    }
+    bisect_all(jobs, ub, o);
+    std::vector<int> next;
+    for (size_t i = 0; i < split.size(); ++i) {
+      const int id = split[i];
+      const HostGraph& g = nodes[id].g;
+      const std::vector<idx_t>& part = jobs[i].part;
+      int32_t pw[2] = {0, 0};  // partition_weights, i32 as the reference sums them
+      for (int32_t v = 0; v < g.n; ++v) pw[part[v]] = (int32_t)((uint32_t)pw[part[v]] + (uint32_t)g.vw(v, 0));
+      const idx_t smaller = pw[0] <= pw[1] ? 0 : 1;
+      std::vector<idx_t> code((size_t)g.n);
+      std::vector<int32_t> sep;
+      for (int32_t v = 0; v < g.n; ++v) {
+        bool cut = false;
+        if (part[v] == smaller)
+          for (idx_t j = g.xadj[v]; j < g.xadj[v + 1] && !cut; ++j) cut = part[g.adj[j]] != part[v];
+        if (cut) sep.push_back(v);
+        code[v] = cut ? 2 : (part[v] == smaller ? 0 : 1);
+      }
+      if ((int64_t)sep.size() >= g.n / 2) continue;  // degenerate separator: ordered as it stands (nd.rs:78-84)
+      nodes[id].leaf = false;
+      nodes[id].sep = std::move(sep);
+      for (idx_t side = 0; side < 2; ++side) {
+        std::vector<int32_t> n2o;
+        HostGraph sub = extract_sub(nodes[id].g, code, side, n2o);
+        if (sub.n == 0) continue;
+        NdNode child;
+        child.g = std::move(sub);
+        child.orig.resize(n2o.size());
+        for (size_t t = 0; t < n2o.size(); ++t) child.orig[t] = nodes[id].orig[n2o[t]];
+        nodes.push_back(std::move(child));  // may move nodes: index, not reference
+        const int cid = (int)nodes.size() - 1;
+        (side == 0 ? nodes[id].left : nodes[id].right) = cid;
+        next.push_back(cid);
+      }
+    }
+    frontier = std::move(next);
+  }
+}
+
+int nodend_host(const idx_t* nvtxs, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
+                const idx_t* options, idx_t* perm, idx_t* iperm) {
+  // Pointer and size checks (src/ffi/c_api.rs:95-99).
+  if (!nvtxs || !xadj || !adjncy || !perm || !iperm) return METIS_ERROR_INPUT;
+  const int32_t n = *nvtxs;
+  if (n <= 0) return METIS_ERROR_INPUT;
+  if (xadj[0] != 0 || xadj[n] < 0) return METIS_ERROR_INPUT;
+  const int64_t ne = xadj[n];
+  KwayOptions o = parse_options(options);
+  apply_tuning(o);
+  Engine& E = engine_for_current_device();
+  {
+    // Graph::new (validate_csr) on the device: ncon 1, vwgt, no edge weights.
+    std::lock_guard<std::mutex> lk(E.mu);
+    Arena::Mark mk = E.arena().mark();
+    struct Rewind {
+      Engine& E;
+      Arena::Mark m;
+      ~Rewind() { E.arena().reset_to(m); }
+    } rw{E, mk};
+    DGraph g;
+    g.n = n;
+    g.m = ne;
+    g.ncon = 1;
+    g.xadj = upload(E, xadj, (size_t)n + 1);
+    g.adjncy = upload(E, adjncy, (size_t)ne);
+    g.vwgt = upload(E, vwgt, (size_t)n);
+    if (validate_device(g, E.arena(), E.stream(), E.host_scratch()) != 0)
+      throw Error(METIS_ERROR_INPUT, "graph failed validation");
+  }
+  std::vector<NdNode> nodes(1);
+  HostGraph& g = nodes[0].g;
+  g.n = n;
+  g.ncon = 1;
+  g.xadj.assign(xadj, xadj + n + 1);
+  g.adj.assign(adjncy, adjncy + ne);
+  g.has_vw = vwgt != nullptr;
+  if (vwgt) g.vwgt.assign(vwgt, vwgt + n);
+  nodes[0].orig.resize(n);
+  for (int32_t v = 0; v < n; ++v) nodes[0].orig[v] = v;
+  nd_order(nodes, o);
+  // Depth-first numbering: left subtree, right subtree, then the separator
+  // (nd.rs:88-110); a leaf in its own vertex order (nd.rs:57-63).
+  int32_t counter = 0;
+  std::vector<std::pair<int, int>> stack{{0, 0}};  // (node, stage)
+  while (!stack.empty()) {
+    auto& top = stack.back();
+    const NdNode& nd = nodes[top.first];
+    if (nd.leaf) {
+      for (int32_t v : nd.orig) perm[v] = counter++;
+      stack.pop_back();
+    } else if (top.second == 0) {
+      top.second = 1;
+      if (nd.left >= 0) stack.push_back({nd.left, 0});
+    } else if (top.second == 1) {
+      top.second = 2;
+      if (nd.right >= 0) stack.push_back({nd.right, 0});
+    } else {
+      for (int32_t v : nd.sep) perm[nd.orig[v]] = counter++;
+      stack.pop_back();
+    }
+  }
+  for (int32_t v = 0; v < n; ++v) iperm[perm[v]] = v;
   return METIS_OK;
 }
 
@@ -432,6 +651,11 @@ int RMETIS_PartGraphRecursive(const idx_t* nvtxs, const idx_t* ncon, const idx_t
   return guarded([&] {
     return recursive_host(nvtxs, ncon, xadj, adjncy, vwgt, adjwgt, nparts, tpwgts, ubvec, options, objval, part);
   });
+}
+
+int RMETIS_NodeND(const idx_t* nvtxs, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt, const idx_t* options,
+                  idx_t* perm, idx_t* iperm) {
+  return guarded([&] { return nodend_host(nvtxs, xadj, adjncy, vwgt, options, perm, iperm); });
 }
 
 int RMETIS_GPU_PartGraphKwayDevice(const idx_t* nvtxs, const idx_t* ncon, const idx_t* d_xadj,
@@ -488,6 +712,14 @@ int RMETIS_GPU_SetTuning(int grow_trials, int match_rounds, int summed_unit_weig
 int RMETIS_GPU_SetRefineMode(int exact_max_n) {
   if (exact_max_n < -1) return METIS_ERROR_INPUT;
   tuning().exact_max_n = exact_max_n == -1 ? INT32_MAX : exact_max_n;
+  return METIS_OK;
+}
+
+int RMETIS_GPU_SetKernelShapes(int contract_thread_max, int gain_block) {
+  if (contract_thread_max != -1 && contract_thread_max != 16 && contract_thread_max != 32) return METIS_ERROR_INPUT;
+  if (gain_block != -1 && gain_block != 128 && gain_block != 256 && gain_block != 512) return METIS_ERROR_INPUT;
+  if (contract_thread_max != -1) tuning().contract_thread_max = contract_thread_max;
+  if (gain_block != -1) tuning().gain_block = gain_block;
   return METIS_OK;
 }
 
@@ -750,7 +982,8 @@ int RMETIS_GPU_BuildCoarseGraph(idx_t n, idx_t ncon, const idx_t* xadj, const id
     HostCall h;
     DGraph g = dgraph(h, n, ncon, xadj, adjncy, vwgt, adjwgt);
     idx_t* d_match = upload(h.E, match, (size_t)n);
-    CoarseResult r = contract(g, d_match, vwgt ? 1 : 0, h.E.arena(), h.st(), h.E.host_scratch());
+    CoarseResult r = contract(g, d_match, vwgt ? 1 : 0, h.E.arena(), h.st(), h.E.host_scratch(),
+                              tuning().contract_thread_max);
     *cn = r.g.n;
     download(h.E, cmap, r.cmap, (size_t)n);
     download(h.E, cxadj, r.xadj, (size_t)r.g.n + 1);
@@ -892,7 +1125,8 @@ static int refine_entry(bool fm, idx_t n, idx_t ncon, const idx_t* xadj, const i
     rp.over_thr = d_over;
     rp.collect_stats = stats != nullptr;
     rp.fused_max_n = tuning().fused_max_n;
-    if (!fm) rp.exact_max_n = tuning().exact_max_n;
+    rp.exact_max_n = tuning().exact_max_n;
+    rp.gain_block = tuning().gain_block;
     {
       std::vector<long long> tot(ncon, 0);
       for (int64_t v = 0; v < n; ++v)

@@ -308,17 +308,16 @@ __device__ __forceinline__ void coarse_vwgt_body(int32_t cn, int32_t ncon, const
   }
 }
 
-// Merge of one coarse row in registers (bound <= kContractThreadMax). The
+// Merge of one coarse row in registers (bound <= T). The
 // row of the first member is scanned before the second, each in CSR order,
 // and a neighbour is appended at its first appearance (mod.rs:323-341).
 // Longer rows are listed in hlist for the warp merge.
-template <bool HAS_W>
+template <bool HAS_W, int T>
 __device__ __forceinline__ void contract_thread_body(const idx_t* xadj, const idx_t* adj, const idx_t* adjwgt,
                                                      const idx_t* cmap, int32_t cn, const idx_t* mem0,
                                                      const idx_t* mem1, const idx_t* ub, const idx_t* ub_off,
                                                      idx_t* tmp_adj, idx_t* tmp_w, idx_t* cdeg, idx_t* hlist,
                                                      int32_t* hcount, Lanes L) {
-  constexpr int T = kContractThreadMax;
   RMB_FOR(c, cn, L) {
     if (ub[c] > T) {
       hlist[atomicAdd(hcount, 1)] = (idx_t)c;
@@ -493,14 +492,14 @@ __global__ void k_coarse_vwgt(int32_t cn, int32_t ncon, const idx_t* __restrict_
   coarse_vwgt_body(cn, ncon, mem0, mem1, vwgt, cvwgt, grid_lanes());
 }
 
-template <bool HAS_W>
+template <bool HAS_W, int T>
 __global__ void k_contract_thread(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
                                   const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ cmap, int32_t cn,
                                   const idx_t* __restrict__ mem0, const idx_t* __restrict__ mem1,
                                   const idx_t* __restrict__ ub, const idx_t* __restrict__ ub_off,
                                   idx_t* __restrict__ tmp_adj, idx_t* __restrict__ tmp_w, idx_t* __restrict__ cdeg,
                                   idx_t* __restrict__ hlist, int32_t* __restrict__ hcount) {
-  contract_thread_body<HAS_W>(xadj, adj, adjwgt, cmap, cn, mem0, mem1, ub, ub_off, tmp_adj, tmp_w, cdeg, hlist,
+  contract_thread_body<HAS_W, T>(xadj, adj, adjwgt, cmap, cn, mem0, mem1, ub, ub_off, tmp_adj, tmp_w, cdeg, hlist,
                               hcount, grid_lanes());
 }
 
@@ -551,7 +550,7 @@ int32_t heavy_list(const DGraph& g, idx_t* out, Arena& arena, cudaStream_t st, i
 }
 
 CoarseResult contract(const DGraph& g, const idx_t* match, int coarse_vwgt, Arena& arena, cudaStream_t st,
-                      int32_t* h_scratch) {
+                      int32_t* h_scratch, int thread_max) {
   CoarseResult r;
   const int32_t n = g.n;
   // The coarse level is allocated first at upper-bound sizes (cn <= n,
@@ -584,12 +583,17 @@ CoarseResult contract(const DGraph& g, const idx_t* match, int coarse_vwgt, Aren
   // members, bounds, offsets (20 B per coarse vertex), member row offsets,
   // adjncy + cmap gathers (+ adjwgt), merged rows written (8 B per entry).
   const int ph = profiler().begin(kProfContract, st);
-  if (g.adjwgt)
-    k_contract_thread<true><<<grid_for(cn, 128), 128, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, cmap, cn, mem0, mem1,
-                                                                ub, ub_off, tmp_adj, tmp_w, cdeg, hlist, counts + 1);
-  else
-    k_contract_thread<false><<<grid_for(cn, 128), 128, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, cmap, cn, mem0, mem1,
-                                                                 ub, ub_off, tmp_adj, tmp_w, cdeg, hlist, counts + 1);
+#define RMB_CONTRACT_THREAD(HW, TT)                                                                           \
+  k_contract_thread<HW, TT><<<grid_for(cn, 128), 128, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, cmap, cn, mem0, mem1, ub, \
+                                                               ub_off, tmp_adj, tmp_w, cdeg, hlist, counts + 1)
+  if (thread_max >= kContractThreadMaxGrid) {
+    if (g.adjwgt) RMB_CONTRACT_THREAD(true, kContractThreadMaxGrid);
+    else RMB_CONTRACT_THREAD(false, kContractThreadMaxGrid);
+  } else {
+    if (g.adjwgt) RMB_CONTRACT_THREAD(true, kContractThreadMax);
+    else RMB_CONTRACT_THREAD(false, kContractThreadMax);
+  }
+#undef RMB_CONTRACT_THREAD
   RMB_LAUNCH_CHECK();
   profiler().end(ph, st, 20.0 * cn + 8.0 * n + (g.adjwgt ? 12.0 : 8.0) * (double)g.m + 8.0 * (double)g.m);
   RMB_CUDA(cudaMemcpyAsync(h_scratch + 1, counts + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
@@ -790,10 +794,10 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_coarsen_tail(TailArgs a) {
       break;
     }
     if (w)
-      contract_thread_body<true>(cur.xadj, cur.adjncy, cur.adjwgt, cmap, cn, mem0, mem1, ub, ub_off, tmp_adj, tmp_w,
+      contract_thread_body<true, kContractThreadMax>(cur.xadj, cur.adjncy, cur.adjwgt, cmap, cn, mem0, mem1, ub, ub_off, tmp_adj, tmp_w,
                                  cdeg, hlist, cnt + 2, L);
     else
-      contract_thread_body<false>(cur.xadj, cur.adjncy, cur.adjwgt, cmap, cn, mem0, mem1, ub, ub_off, tmp_adj,
+      contract_thread_body<false, kContractThreadMax>(cur.xadj, cur.adjncy, cur.adjwgt, cmap, cn, mem0, mem1, ub, ub_off, tmp_adj,
                                   tmp_w, cdeg, hlist, cnt + 2, L);
     __syncthreads();
     const int32_t nlong = cnt[2];

@@ -308,7 +308,7 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
       // Coarse vertex weights: the reference gives a coarse graph vwgt only
       // when the fine graph has it (graph/mod.rs:300).
       const bool coarse_vw = has_vw.back() || o.summed_unit_weights;
-      CoarseResult cr = contract(cur, match, coarse_vw ? 1 : 0, arena_, st, h_scratch_);
+      CoarseResult cr = contract(cur, match, coarse_vw ? 1 : 0, arena_, st, h_scratch_, o.contract_thread_max);
       // The matching is scratch once contracted; keep the coarse level.
       (void)mm;
       const float ratio = (float)cr.g.n / (float)cur.n;
@@ -440,6 +440,7 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
     rp.fused_max_n = o.fused_max_n;
     // A traced run replays bit for bit in the oracle: exact walks everywhere.
     rp.exact_max_n = trace ? INT32_MAX : o.exact_max_n;
+    rp.gain_block = o.gain_block;
     rp.collect_stats = trace != nullptr;
     {
       RefineStats rs = refine_level(o.rtype, cg, part, rp, heavy_lists[L], heavy_counts[L]);

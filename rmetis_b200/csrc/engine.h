@@ -35,6 +35,8 @@ struct KwayOptions {
   int fused_max_n = 4096;       // levels up to this size (and 4x its edges) refine in one launch
   int tail_max_n = 4096;        // from a level of at most this size, coarsening runs in one launch
   int exact_max_n = 16384;      // larger levels decide cut passes by parallel admission
+  int contract_thread_max = 32; // coarse rows with a longer bound are merged by a warp (16 or 32)
+  int gain_block = 256;         // threads per block of the gain-table kernel
 };
 
 // Per-kernel-family device time, measured with CUDA events on the engine's

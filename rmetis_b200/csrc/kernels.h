@@ -27,6 +27,9 @@ struct DGraph {
 constexpr int kHeavyDegree = 64;
 // Coarse vertices whose merged row bound exceeds this use the warp merge.
 constexpr int kContractThreadMax = 16;
+// The same bound in the grid-wide contraction kernel, whose threads have more
+// registers to spare than those of the 1024-thread coarse-tail block.
+constexpr int kContractThreadMaxGrid = 32;
 // Movers per block in the refinement decision kernel.
 constexpr int kDecideBlock = 256;
 
@@ -84,7 +87,7 @@ struct CoarseResult {
 // coarse_vwgt: 0 = coarse graph has no vwgt (reference rule when the fine
 // graph has none), 1 = sum (materialising 1 for a unit fine graph).
 CoarseResult contract(const DGraph& g, const idx_t* match, int coarse_vwgt, Arena& arena,
-                      cudaStream_t st, int32_t* h_scratch);
+                      cudaStream_t st, int32_t* h_scratch, int thread_max = kContractThreadMaxGrid);
 
 // Degree > kHeavyDegree vertex list of a level (ascending ids).
 int32_t heavy_list(const DGraph& g, idx_t* out, Arena& arena, cudaStream_t st, int32_t* h_scratch);
@@ -143,6 +146,9 @@ struct RefineParams {
   // Cut passes of levels with more vertices than this decide by parallel
   // admission (admit.cu) instead of the exact sequential walk.
   int32_t exact_max_n = INT32_MAX;
+  // Threads per block of the gain-table kernel (128, 256 or 512; the same
+  // table whatever the size).
+  int gain_block = 256;
 };
 
 // True when the totals and thresholds allow 32-bit slacks in the walk.
@@ -205,12 +211,14 @@ struct AdmitScratch {
 size_t admit_smem_bytes(int k, int ncon);
 bool admit_supported(int k, int ncon);
 // Returns the profiler handle of the pass. nmax bounds the movers (grid
-// size); nmoves gets the moves applied, rounds_out (optional) the admission
-// rounds (negative: the bound was hit).
+// size); nmoves gets the moves admitted, rounds_out (optional) the admission
+// rounds (negative: the bound was hit). With apply = false the part vector is
+// left to the caller: mover j moves to s.tgt[j] when s.tgt[j] >= 0 and
+// s.rank[j] < s.cut[s.tgt[j]].
 int admit_cut_pass(const DGraph& g, int k, int32_t nmax, const int32_t* nm_dev, const idx_t* movers,
                    const idx_t* ncand, const idx_t* wfrom, const idx_t* cand_p, const idx_t* cand_g, idx_t* part,
                    long long* pw, const long long* feas, int32_t* nmoves, int32_t* rounds_out,
-                   const AdmitScratch& s, cudaStream_t st);
+                   const AdmitScratch& s, cudaStream_t st, bool apply = true);
 
 // Opts a kernel in to `bytes` of dynamic shared memory on the current device
 // (once per kernel and device; safe from several host threads).

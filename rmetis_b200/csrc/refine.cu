@@ -1236,18 +1236,18 @@ template <int MODE>
 static int launch_gain(const DGraph& g, const idx_t* part, int k, const long long* pw0, const long long* over_thr,
                        idx_t* mover, idx_t* ncand, idx_t* wfrom, idx_t* cand_p, idx_t* cand_g, const idx_t* heavy,
                        int32_t nheavy, int32_t* ghist, cudaStream_t st, const int32_t* stop = nullptr,
-                       const idx_t* only = nullptr) {
-  const int blocks = grid_for(g.n, 256);
+                       const idx_t* only = nullptr, int block = 256) {
+  const int blocks = grid_for(g.n, block, 148 * 32 * 256 / block);
   // Algorithmic bytes of a full pass: xadj, part (own + neighbour gathers),
   // adjncy, adjwgt, mover flag.
   // (A launch limited to the vertices of `only` counts only its flag scan.)
   const double bytes = only ? 4.0 * g.n : 12.0 * g.n + (g.adjwgt ? 12.0 : 8.0) * (double)g.m;
   const int ph = MODE == kCut ? profiler().begin(kProfGain, st) : -1;
   if (g.adjwgt)
-    k_gain<true, MODE><<<blocks, 256, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, g.n, g.ncon, part, k, pw0, over_thr,
+    k_gain<true, MODE><<<blocks, block, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, g.n, g.ncon, part, k, pw0, over_thr,
                                                 mover, ncand, wfrom, cand_p, cand_g, stop, only);
   else
-    k_gain<false, MODE><<<blocks, 256, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, g.n, g.ncon, part, k, pw0, over_thr,
+    k_gain<false, MODE><<<blocks, block, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, g.n, g.ncon, part, k, pw0, over_thr,
                                                  mover, ncand, wfrom, cand_p, cand_g, stop, only);
   RMB_LAUNCH_CHECK();
   profiler().end(ph, st, bytes);
@@ -1570,7 +1570,7 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
       launch_gain<kRepair>(g, part, k, pw, rp.over_thr, mover, ncand, wfrom, cand_p, cand_g, heavy, nheavy, ghist, st);
     else
       gain_handles.push_back(launch_gain<kCut>(g, part, k, pw, rp.over_thr, mover, ncand, wfrom, cand_p, cand_g,
-                                               heavy, nheavy, ghist, st, stop));
+                                               heavy, nheavy, ghist, st, stop, nullptr, rp.gain_block));
     compact_flags(mover, g.n, movers, nm_dev, arena, st);
     if (mode == kRepair)
       walk_handles.push_back(launch_walk<kRepair>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r,
@@ -1745,6 +1745,33 @@ __global__ void k_fm_after(const int32_t* __restrict__ nm_dev, const idx_t* __re
   }
 }
 
+// k_fm_after for a round decided by admission, with the moves applied here:
+// an admitted mover moves and is locked, and frees its dropped unselected
+// neighbours; a mover that was not admitted is dropped.
+__global__ void k_fm_apply_after(const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
+                                 const int32_t* __restrict__ tgt, const int32_t* __restrict__ rank,
+                                 const int32_t* __restrict__ cut, const idx_t* __restrict__ xadj,
+                                 const idx_t* __restrict__ adj, idx_t* __restrict__ part, const idx_t* __restrict__ sel,
+                                 int32_t* __restrict__ state, idx_t* __restrict__ changed) {
+  const int32_t nm = *nm_dev;
+  RMB_GRID_STRIDE(i, nm) {
+    const int32_t v = movers[i];
+    const int32_t t = tgt[i];
+    changed[v] = 1;
+    if (t >= 0 && rank[i] < cut[t]) {
+      part[v] = t;
+      state[v] = kFmLocked;
+      for (int32_t j = xadj[v]; j < xadj[v + 1]; ++j) {
+        const int32_t u = adj[j];
+        changed[u] = 1;
+        if (!sel[u] && state[u] == kFmDropped) state[u] = kFmFree;
+      }
+    } else {
+      state[v] = kFmDropped;
+    }
+  }
+}
+
 // active_next = changed and their neighbours (zero on entry). Also clears the
 // flags the round just used (changed_cur, active_cur) for the round after next.
 __global__ void k_fm_spread(int32_t n, const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
@@ -1797,6 +1824,24 @@ RefineStats fm_refine(const DGraph& g, idx_t* part, const RefineParams& rp, cons
   r.np = arena.alloc<int32_t>((size_t)g.n);
   int32_t* ghist = nullptr;
   if (nheavy > 0 && k > kGainHist) ghist = arena.alloc<int32_t>((size_t)k * 256 * 4);
+  // The moves of a round on a large level are decided by parallel admission
+  // (admit.cu) instead of the sequential walk: every selected vertex is a
+  // local maximum whose move alone is feasible or not, and a part admits the
+  // longest prefix of its selected in-moves that fits its limit given the
+  // moves out of it.
+  const bool admit = g.n > rp.exact_max_n && admit_supported(k, g.ncon);
+  AdmitScratch as;
+  if (admit) {
+    as.tgt = arena.alloc<int32_t>((size_t)g.n);
+    as.src = arena.alloc<int32_t>((size_t)g.n);
+    as.w = arena.alloc<int32_t>((size_t)g.n * g.ncon);
+    as.rank = arena.alloc<int32_t>((size_t)g.n);
+    as.pref = arena.alloc<long long>((size_t)g.n * g.ncon);
+    as.gsrc = arena.alloc<int32_t>((size_t)g.n);
+    as.out = arena.alloc<long long>((size_t)K);
+    as.cut = arena.alloc<int32_t>((size_t)k);
+    RMB_CUDA(cudaMemsetAsync(as.out, 0, sizeof(long long) * (size_t)K, st));
+  }
   RMB_CUDA(cudaMemsetAsync(long_flag, 0, sizeof(int32_t), st));
   RMB_CUDA(cudaMemsetAsync(in_max, 0, sizeof(long long) * (size_t)K, st));
   RMB_CUDA(cudaMemsetAsync(out_max, 0, sizeof(long long) * (size_t)K, st));
@@ -1824,14 +1869,21 @@ RefineStats fm_refine(const DGraph& g, idx_t* part, const RefineParams& rp, cons
         idx_t* const* cur = flags[rounds & 1];
         idx_t* const* nxt = flags[(rounds + 1) & 1];
         launch_gain<kCut>(g, part, k, nullptr, nullptr, mover, ncand, wfrom, cand_p, cand_g, heavy, nheavy, ghist,
-                          st, stop, rounds > 0 ? cur[0] : nullptr);
+                          st, stop, rounds > 0 ? cur[0] : nullptr, rp.gain_block);
         k_fm_select<<<nb, 256, 0, st>>>(g.n, g.xadj, g.adjncy, part, mover, ncand, cand_g, state,
                                         rounds > 0 ? cur[1] : nullptr, sel);
         RMB_LAUNCH_CHECK();
         compact_flags(sel, g.n, movers, nm_dev, arena, st);
-        launch_walk<kCut>(g.n, nm_dev, movers, g, part, k, sel, zero, cand_p, cand_g, r, pw, rp.feas_max,
-                          rp.over_thr, in_max, out_max, nm_dev + 1, rp.small_weights, long_flag, st);
-        k_fm_after<<<nb, 256, 0, st>>>(nm_dev, movers, g.xadj, g.adjncy, part, cand_p, sel, state, nxt[0]);
+        if (admit) {
+          admit_cut_pass(g, k, g.n, nm_dev, movers, sel, zero, cand_p, cand_g, part, pw, rp.feas_max, nm_dev + 1,
+                         nullptr, as, st, /*apply=*/false);
+          k_fm_apply_after<<<grid_for(g.n, 256, 148 * 4), 256, 0, st>>>(nm_dev, movers, as.tgt, as.rank, as.cut,
+                                                                        g.xadj, g.adjncy, part, sel, state, nxt[0]);
+        } else {
+          launch_walk<kCut>(g.n, nm_dev, movers, g, part, k, sel, zero, cand_p, cand_g, r, pw, rp.feas_max,
+                            rp.over_thr, in_max, out_max, nm_dev + 1, rp.small_weights, long_flag, st);
+          k_fm_after<<<nb, 256, 0, st>>>(nm_dev, movers, g.xadj, g.adjncy, part, cand_p, sel, state, nxt[0]);
+        }
         RMB_LAUNCH_CHECK();
         k_fm_spread<<<nb, 256, 0, st>>>(g.n, g.xadj, g.adjncy, nxt[0], nxt[1], cur[0], cur[1]);
         RMB_LAUNCH_CHECK();

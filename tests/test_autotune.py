@@ -84,11 +84,52 @@ def test_table_round_trip_and_apply(tmp_path):
 def test_committed_table_is_well_formed():
     t = A.load_table()
     for dev, entry in t.items():
-        assert set(entry) <= {"plain", "pool"}
-        for mode in entry.values():
+        assert set(entry) <= {"plain", "pool", "shapes", "refine"}
+        for name, mode in entry.items():
             s = mode["setting"]
-            assert set(s) == {"fused_max_n", "tail_max_n"}
-            assert all(isinstance(v, int) and v >= 0 for v in s.values())
+            if name in ("plain", "pool"):
+                assert set(s) == {"fused_max_n", "tail_max_n"}
+                assert all(isinstance(v, int) and v >= 0 for v in s.values())
+            elif name == "shapes":
+                assert s["contract_thread_max"] in (16, 32) and s["gain_block"] in (128, 256, 512)
+            else:
+                assert s["exact_max_n"] in A.EXACT_CANDIDATES
+                assert s["cut_ratio"] <= 1.0 + A.QUALITY_TOL or s["exact_max_n"] == max(A.EXACT_CANDIDATES)
+
+
+def test_shape_candidates_start_with_the_defaults():
+    c = A.shape_candidates()
+    assert c[0] == A.SHAPE_DEFAULTS
+    assert len(c) == 6 and len({tuple(sorted(x.items())) for x in c}) == 6
+
+
+def test_quality_gated_refine_mode(monkeypatch):
+    """The result-changing knob: the fastest setting whose summed cut stays
+    within the tolerance of sequential passes everywhere wins."""
+    cut = {-1: 1000, 4096: 1030, 8192: 1004, 16384: 1001}
+    cost = {-1: 0.9, 4096: 0.1, 8192: 0.2, 16384: 0.3}
+    clock = [0.0]
+    monkeypatch.setattr(A.time, "perf_counter", lambda: clock[0])
+
+    def run(v):
+        clock[0] += cost[v]
+        return [_res(cut[v], [0])]
+
+    elig, trials = A.tune_quality(run, (4096, 8192, 16384), repeats=2, tol=0.005)
+    assert [t.setting["exact_max_n"] for t in elig] == [8192, 16384]
+    assert {t.setting["exact_max_n"]: t.setting["cut_ratio"] for t in trials}[4096] == 1.03
+
+
+def test_apply_sets_shapes_and_refine_mode(tmp_path):
+    path = str(tmp_path / "t.json")
+    A.save_entry(path, "Dev", "shapes", [A.Trial({"contract_thread_max": 16, "gain_block": 512}, 0.1)])
+    A.save_entry(path, "Dev", "refine", [A.Trial({"exact_max_n": 8192, "cut_ratio": 1.001}, 0.1)])
+    got = {}
+    setters = {"shapes": lambda c, b: got.__setitem__("shapes", (c, b)),
+               "refine": lambda v: got.__setitem__("refine", v)}
+    applied = A.apply(path, device="Dev", setters=setters)
+    assert got == {"shapes": (16, 512), "refine": 8192}
+    assert applied == {"shapes": {"contract_thread_max": 16, "gain_block": 512}, "refine": {"exact_max_n": 8192}}
 
 
 @pytest.mark.gpu

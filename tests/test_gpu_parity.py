@@ -82,8 +82,12 @@ def _check_contraction(rmb, oracle, x, a, v, w, m, ncon=1):
 
 @pytest.mark.parametrize("name", list(GRAPHS))
 @pytest.mark.parametrize("source", ["shem", "rm", "gpu"])
-def test_contraction_bit_exact(rmb, oracle, name, source):
+@pytest.mark.parametrize("thread_max", [16, 32])
+def test_contraction_bit_exact(rmb, oracle, name, source, thread_max):
+    """Rows merged by one thread (bound up to thread_max) and by a warp give
+    the same coarse graph."""
     from rmetis_b200 import functions as F
+    rmb.set_kernel_shapes(contract_thread_max=thread_max)
     x, a, v, w = load(name)
     n = len(x) - 1
     if source == "shem":
@@ -92,7 +96,10 @@ def test_contraction_bit_exact(rmb, oracle, name, source):
         m = oracle.random_matching(x, a, oracle.SmallRng(12))
     else:
         m = F.match(rmb.Graph(n, 1, x, a, adjwgt=w), mode=1, seed=13)
-    _check_contraction(rmb, oracle, x, a, v, w, m)
+    try:
+        _check_contraction(rmb, oracle, x, a, v, w, m)
+    finally:
+        rmb.set_kernel_shapes(contract_thread_max=32)
 
 
 def test_contraction_multiconstraint(rmb, oracle):
