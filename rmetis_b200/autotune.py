@@ -61,7 +61,7 @@ SHAPE_CANDIDATES = {"contract_thread_max": (16, 32), "gain_block": (128, 256, 51
 SHAPE_DEFAULTS = {"contract_thread_max": 32, "gain_block": 256}
 EXACT_CANDIDATES = (4096, 8192, 16384, 32768, 65536)
 EXACT_DEFAULT = 16384
-QUALITY_TOL = 0.005
+QUALITY_TOL = 0.02
 
 
 class TuningMismatch(RuntimeError):
@@ -129,8 +129,12 @@ def digest(results) -> list:
 def tune(run, settings, repeats: int = 3, log=None):
     """Run `run(setting) -> results` `repeats` times per setting (plus one
     untimed warm-up), check every result against the first setting's, and
-    return the trials sorted fastest first."""
+    return the trials sorted fastest first. A runner that records the time of
+    each item of a run (`run.item_times`, a list) is scored by the sum of its
+    items' times relative to the first setting's, so that a small graph
+    counts as much as a large one; otherwise by the run's wall time."""
     ref = None
+    base = None
     trials = []
     for s in settings:
         first = digest(run(s))  # warm-up, and the results to compare
@@ -140,14 +144,22 @@ def tune(run, settings, repeats: int = 3, log=None):
             bad = next(i for i, (a, b) in enumerate(zip(first, ref)) if a != b) if len(first) == len(ref) else -1
             raise TuningMismatch(f"setting {s} changed result {bad}: {first[bad] if bad >= 0 else len(first)} "
                                  f"vs {ref[bad] if bad >= 0 else len(ref)}")
-        times = []
+        times, items = [], None
         for _ in range(repeats):
             t0 = time.perf_counter()
             out = run(s)
             times.append(time.perf_counter() - t0)
+            it = getattr(run, "item_times", None)
+            if it:
+                items = list(it) if items is None else [min(a, b) for a, b in zip(items, it)]
             if digest(out) != ref:
                 raise TuningMismatch(f"setting {s} is not reproducible")
-        tr = Trial(dict(s), min(times), times)
+        score = min(times)
+        if items:
+            if base is None:
+                base = items
+            score = sum(a / b for a, b in zip(items, base) if b > 0) / len(items) * sum(base)
+        tr = Trial(dict(s), score, times)
         trials.append(tr)
         if log:
             log(f"  {s}: {tr.seconds * 1e3:.2f} ms (best of {repeats})")
@@ -204,7 +216,13 @@ def plain_runner(graphs, options=None):
             rmb.set_tuning(fused_max_n=s["fused_max_n"], tail_max_n=s["tail_max_n"])
         if "contract_thread_max" in s:
             rmb.set_kernel_shapes(s["contract_thread_max"], s["gain_block"])
-        return [rmb.part_graph_kway(g, k, options=o) for g, k in graphs]
+        out, run.item_times = [], []
+        for g, k in graphs:
+            t0 = time.perf_counter()
+            out.append(rmb.part_graph_kway(g, k, options=o))
+            run.item_times.append(time.perf_counter() - t0)
+        return out
+    run.item_times = []
     return run
 
 
@@ -320,7 +338,7 @@ def main(argv=None):
         rmb.set_kernel_shapes(**st[0].setting)
         print(f"shapes winner {st[0].setting} {st[0].seconds * 1e3:.2f} ms", flush=True)
         elig, all_trials = tune_quality(exact_runner(wl), EXACT_CANDIDATES, args.repeats, log=print)
-        best = elig if elig else [t for t in all_trials if t.setting["exact_max_n"] == max(EXACT_CANDIDATES)]
+        best = elig if elig else [t for t in all_trials if t.setting["exact_max_n"] == EXACT_DEFAULT]
         rest = [t for t in sorted(all_trials, key=lambda t: t.seconds) if t is not best[0]]
         save_entry(args.out, dev, "refine", [best[0]] + rest,
                    note=f"fastest exact_max_n whose summed cut is within {QUALITY_TOL:.1%} of sequential passes "

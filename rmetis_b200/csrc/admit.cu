@@ -132,13 +132,24 @@ __global__ void k_admit_pick(PickArgs A) {
 // The admitted moves of a pass, applied to the part vector: mover j moves to
 // its target when its rank in the target's in-list is below the part's
 // admitted prefix.
+// With `touched`, every moved vertex and its neighbours are flagged there:
+// the only vertices whose gain table the move changes.
 __global__ void k_admit_apply(const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
                               const int32_t* __restrict__ tgt, const int32_t* __restrict__ rank,
-                              const int32_t* __restrict__ cut, idx_t* __restrict__ part) {
+                              const int32_t* __restrict__ cut, idx_t* __restrict__ part,
+                              const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                              idx_t* __restrict__ touched) {
   const int32_t nm = *nm_dev;
   RMB_GRID_STRIDE(j, nm) {
     const int32_t t = tgt[j];
-    if (t >= 0 && rank[j] < cut[t]) part[movers[j]] = t;
+    if (t >= 0 && rank[j] < cut[t]) {
+      const int32_t v = movers[j];
+      part[v] = t;
+      if (touched) {
+        touched[v] = 1;
+        for (int32_t e = xadj[v]; e < xadj[v + 1]; ++e) touched[adj[e]] = 1;
+      }
+    }
   }
 }
 
@@ -484,7 +495,7 @@ bool admit_supported(int k, int ncon) {
 int admit_cut_pass(const DGraph& g, int k, int32_t nmax, const int32_t* nm_dev, const idx_t* movers,
                    const idx_t* ncand, const idx_t* wfrom, const idx_t* cand_p, const idx_t* cand_g, idx_t* part,
                    long long* pw, const long long* feas, int32_t* nmoves, int32_t* rounds_out,
-                   const AdmitScratch& s, cudaStream_t st, bool apply) {
+                   const AdmitScratch& s, cudaStream_t st, bool apply, idx_t* touched) {
   const int ph = profiler().begin(kProfAdmit, st);
   PickArgs P;
   P.nm_dev = nm_dev;
@@ -527,7 +538,7 @@ int admit_cut_pass(const DGraph& g, int k, int32_t nmax, const int32_t* nm_dev, 
   k_admit<<<1, kAdmitThreads, kAdmitMaxSmem, st>>>(A);
   RMB_LAUNCH_CHECK();
   if (apply) {
-    k_admit_apply<<<blocks, 256, 0, st>>>(nm_dev, movers, s.tgt, s.rank, s.cut, part);
+    k_admit_apply<<<blocks, 256, 0, st>>>(nm_dev, movers, s.tgt, s.rank, s.cut, part, g.xadj, g.adjncy, touched);
     RMB_LAUNCH_CHECK();
   }
   profiler().end(ph, st, 0.0);

@@ -4,6 +4,9 @@
 #include <cmath>
 #include <cstring>
 #include <random>
+#include <sstream>
+
+#include <nvtx3/nvToolsExt.h>
 
 #include "engine.h"
 #include "hostrng.h"
@@ -242,8 +245,18 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
   Arena::Mark att_mark = arena_.mark();
   unsigned long long* d_cut = arena_.alloc<unsigned long long>(1);
   KwayTrace local;
+  const bool json = trace_json_path() != nullptr;
+  struct LevelRec {
+    int32_t n;
+    int64_t m;
+    int64_t passes = 0, moves = 0;
+    cudaEvent_t a = nullptr, b = nullptr;
+  };
+  std::vector<LevelRec> recs;
+  nvtxRangePushA("rmetis attempt");
   {
     // ---- coarsening (coarsen/mod.rs:36-71) ----
+    nvtxRangePushA("coarsen");
     std::vector<DGraph> levels{g0};
     std::vector<idx_t*> cmaps;
     std::vector<idx_t*> heavy_lists;
@@ -322,7 +335,10 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
       has_vw.push_back(coarse_vw);
       if ((size_t)cr.g.n <= limit || ratio > 0.95f) break;
     }
+    nvtxRangePop();  // coarsen
     const int L = (int)levels.size() - 1;  // number of coarse levels
+    if (checks_enabled())
+      for (int l = 0; l < L; ++l) check_contraction(levels[l], levels[l + 1], cmaps[l], arena_, st, h_scratch_);
     // heavy list of the coarsest level (the loop computed lists for 0..L-1)
     if ((int)heavy_lists.size() < (int)levels.size()) {
       idx_t* hl = arena_.alloc<idx_t>((size_t)levels.back().n);
@@ -362,6 +378,7 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
     long long* d_grow = d_thr + 3 * K * (size_t)L + 2 * K;
 
     // ---- initial partition of the coarsest graph (initial/mod.rs:11-22) ----
+    nvtxRangePushA("initial partition");
     const DGraph& cg = levels.back();
     idx_t* part = arena_.alloc<idx_t>((size_t)cg.n);
     if (o.iptype == 1) {
@@ -426,10 +443,29 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
     // ---- refinement at the coarsest level and on the way up (kway.rs:72-92) ----
     // refine_level (kway.rs:145-162): Greedy, or FM through refine_kway
     // (src/refine/mod.rs:26-38).
+    nvtxRangePop();  // initial partition
     auto refine_level = [&](int rtype, const DGraph& lg, idx_t* lpart, const RefineParams& lrp, const idx_t* hl,
                             int32_t nh) {
-      return rtype == 1 ? greedy_refine(lg, lpart, lrp, hl, nh, arena_, st, h_scratch_)
-                        : fm_refine(lg, lpart, lrp, hl, nh, arena_, st, h_scratch_);
+      nvtxRangePushA(rtype == 1 ? "refine level (greedy)" : "refine level (fm)");
+      LevelRec rec;
+      rec.n = lg.n;
+      rec.m = lg.m;
+      if (json) {
+        RMB_CUDA(cudaEventCreate(&rec.a));
+        RMB_CUDA(cudaEventCreate(&rec.b));
+        RMB_CUDA(cudaEventRecord(rec.a, st));
+      }
+      RefineStats rs = rtype == 1 ? greedy_refine(lg, lpart, lrp, hl, nh, arena_, st, h_scratch_)
+                                  : fm_refine(lg, lpart, lrp, hl, nh, arena_, st, h_scratch_);
+      if (json) {
+        RMB_CUDA(cudaEventRecord(rec.b, st));
+        rec.passes = rs.passes;
+        rec.moves = rs.moves;
+        recs.push_back(rec);
+      }
+      if (checks_enabled()) check_refined(lg, lpart, k, arena_, st, h_scratch_);
+      nvtxRangePop();
+      return rs;
     };
     RefineParams rp;
     rp.k = k;
@@ -441,7 +477,7 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
     // A traced run replays bit for bit in the oracle: exact walks everywhere.
     rp.exact_max_n = trace ? INT32_MAX : o.exact_max_n;
     rp.gain_block = o.gain_block;
-    rp.collect_stats = trace != nullptr;
+    rp.collect_stats = trace != nullptr || json;
     {
       RefineStats rs = refine_level(o.rtype, cg, part, rp, heavy_lists[L], heavy_counts[L]);
       local.refine_passes += rs.passes;
@@ -471,7 +507,27 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
     std::memcpy(&cut_raw, h_scratch_ + 32, sizeof(cut_raw));
     *objval = (int32_t)(uint32_t)cut_raw / 2;
     if (trace) *trace = std::move(local);
+    if (json) {
+      // One line per attempt: every refined level, coarsest first.
+      std::ostringstream os;
+      os << "{\"n\": " << g0.n << ", \"m\": " << g0.m << ", \"k\": " << k << ", \"ncon\": " << ncon
+         << ", \"seed\": " << seed64 << ", \"rtype\": \"" << (o.rtype == 1 ? "greedy" : "fm")
+         << "\", \"cut\": " << *objval << ", \"levels\": [";
+      for (size_t i = 0; i < recs.size(); ++i) {
+        float ms = 0.f;
+        RMB_CUDA(cudaEventElapsedTime(&ms, recs[i].a, recs[i].b));
+        const double bytes = (double)recs[i].passes * (12.0 * recs[i].n + 12.0 * (double)recs[i].m);
+        os << (i ? ", " : "") << "{\"n\": " << recs[i].n << ", \"m\": " << recs[i].m << ", \"passes\": "
+           << recs[i].passes << ", \"moves\": " << recs[i].moves << ", \"refine_ms\": " << ms
+           << ", \"gain_gbps\": " << (ms > 0 ? bytes / (ms * 1e-3) / 1e9 : 0.0) << "}";
+        cudaEventDestroy(recs[i].a);
+        cudaEventDestroy(recs[i].b);
+      }
+      os << "]}";
+      trace_json_write(os.str());
+    }
   }
+  nvtxRangePop();  // attempt
   arena_.reset_to(att_mark);
 }
 

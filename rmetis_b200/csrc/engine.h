@@ -9,6 +9,7 @@
 #include <future>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -157,6 +158,17 @@ class WorkerPool {
 // The pool of a device, created on first use: RMETIS_B200_WORKERS threads
 // (default 8) and a budget of RMETIS_B200_POOL_BYTES (default 150 GB).
 WorkerPool& pool_for_device(int device);
+
+// Debug invariant checks (checks.cu; on when RMETIS_B200_CHECKS is set): a
+// violation throws Error(-4) naming the invariant.
+bool checks_enabled();
+void check_contraction(const DGraph& fine, const DGraph& coarse, const idx_t* cmap, Arena& arena, cudaStream_t st,
+                       int32_t* h_scratch);
+void check_refined(const DGraph& g, const idx_t* part, int k, Arena& arena, cudaStream_t st, int32_t* h_scratch);
+// Per-level trace: one JSON line per attempt appended to the file named by
+// RMETIS_B200_TRACE_JSON (null: tracing off).
+const char* trace_json_path();
+void trace_json_write(const std::string& line);
 
 // Host-side threshold form of the reference's f64 tests:
 //   feasible   (pw + vw) as f64 <= t * ub   <=>  pw + vw <= feas

@@ -214,11 +214,12 @@ bool admit_supported(int k, int ncon);
 // size); nmoves gets the moves admitted, rounds_out (optional) the admission
 // rounds (negative: the bound was hit). With apply = false the part vector is
 // left to the caller: mover j moves to s.tgt[j] when s.tgt[j] >= 0 and
-// s.rank[j] < s.cut[s.tgt[j]].
+// s.rank[j] < s.cut[s.tgt[j]]. With `touched` (n flags), the moved vertices
+// and their neighbours are flagged there.
 int admit_cut_pass(const DGraph& g, int k, int32_t nmax, const int32_t* nm_dev, const idx_t* movers,
                    const idx_t* ncand, const idx_t* wfrom, const idx_t* cand_p, const idx_t* cand_g, idx_t* part,
                    long long* pw, const long long* feas, int32_t* nmoves, int32_t* rounds_out,
-                   const AdmitScratch& s, cudaStream_t st, bool apply = true);
+                   const AdmitScratch& s, cudaStream_t st, bool apply = true, idx_t* touched = nullptr);
 
 // Opts a kernel in to `bytes` of dynamic shared memory on the current device
 // (once per kernel and device; safe from several host threads).

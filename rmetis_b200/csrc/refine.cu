@@ -54,11 +54,12 @@ __device__ void gain_body(Lanes L, const idx_t* __restrict__ xadj, const idx_t* 
                           int32_t k, const long long* __restrict__ pw0, const long long* __restrict__ over_thr,
                           idx_t* __restrict__ mover, idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom,
                           idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g,
-                          const idx_t* __restrict__ only = nullptr) {
+                          const idx_t* __restrict__ only = nullptr, bool clear_only = false) {
   RMB_FOR(v, n, L) {
     if (only && !only[v]) continue;  // entries of vertices outside `only` stay as they are
     const int32_t s = xadj[v], e = xadj[v + 1];
     if (e - s > kHeavyDegree) continue;  // warp path
+    if (clear_only) const_cast<idx_t*>(only)[v] = 0;  // consumed: the flag set is empty again after the pass
     const int32_t pv = part[v];
     if (MODE == kRepair) {
       bool over = false;
@@ -173,7 +174,7 @@ __global__ void k_gain(const idx_t* __restrict__ xadj, const idx_t* __restrict__
                        int32_t k, const long long* __restrict__ pw0, const long long* __restrict__ over_thr,
                        idx_t* __restrict__ mover, idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom,
                        idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g, const int32_t* __restrict__ stop,
-                       const idx_t* __restrict__ only) {
+                       const idx_t* __restrict__ only, bool clear_only) {
   // stop: moves of the previous cut pass. None means this pass would find the
   // same movers and make no move either (the reference stops there): no movers.
   if (stop && *stop == 0) {
@@ -181,7 +182,7 @@ __global__ void k_gain(const idx_t* __restrict__ xadj, const idx_t* __restrict__
     return;
   }
   gain_body<HAS_W, MODE>(grid_lanes(), xadj, adj, adjwgt, n, ncon, part, k, pw0, over_thr, mover, ncand, wfrom,
-                         cand_p, cand_g, only);
+                         cand_p, cand_g, only, clear_only);
 }
 
 constexpr int kGainHist = 2048;  // dense per-warp part histogram in shared memory
@@ -200,12 +201,15 @@ __device__ void gain_heavy_body(int32_t gw, int32_t nw, int32_t* hist, const idx
                                 const idx_t* __restrict__ part, int32_t k, const long long* __restrict__ pw0,
                                 const long long* __restrict__ over_thr, idx_t* __restrict__ mover,
                                 idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom, idx_t* __restrict__ cand_p,
-                                idx_t* __restrict__ cand_g, const idx_t* __restrict__ only = nullptr) {
+                                idx_t* __restrict__ cand_g, const idx_t* __restrict__ only = nullptr,
+                                bool clear_only = false) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   for (int32_t hi = gw; hi < nheavy; hi += nw) {
     const int32_t v = heavy[hi];
     if (only && !only[v]) continue;  // warp-uniform: every lane reads the same flag
+    __syncwarp();
+    if (clear_only && lane == 0) const_cast<idx_t*>(only)[v] = 0;
     const int32_t s = xadj[v], e = xadj[v + 1];
     const int32_t pv = part[v];
     if (MODE == kRepair) {
@@ -271,7 +275,8 @@ __global__ void k_gain_heavy(const idx_t* __restrict__ xadj, const idx_t* __rest
                              const long long* __restrict__ pw0, const long long* __restrict__ over_thr,
                              idx_t* __restrict__ mover, idx_t* __restrict__ ncand, idx_t* __restrict__ wfrom,
                              idx_t* __restrict__ cand_p, idx_t* __restrict__ cand_g, int32_t* __restrict__ ghist,
-                             const int32_t* __restrict__ stop, const idx_t* __restrict__ only) {
+                             const int32_t* __restrict__ stop, const idx_t* __restrict__ only,
+                             bool clear_only) {
   if (stop && *stop == 0) return;  // k_gain has cleared every mover flag
   __shared__ int32_t sh_all[4][kGainHist];
   const int wib = threadIdx.x >> 5;
@@ -279,7 +284,7 @@ __global__ void k_gain_heavy(const idx_t* __restrict__ xadj, const idx_t* __rest
   const int32_t nw = gridDim.x * (blockDim.x >> 5);
   int32_t* hist = (k <= kGainHist) ? sh_all[wib] : ghist + (int64_t)gw * k;
   gain_heavy_body<HAS_W, MODE>(gw, nw, hist, xadj, adj, adjwgt, heavy, nheavy, ncon, part, k, pw0, over_thr, mover,
-                               ncand, wfrom, cand_p, cand_g, only);
+                               ncand, wfrom, cand_p, cand_g, only, clear_only);
 }
 
 
@@ -1236,7 +1241,7 @@ template <int MODE>
 static int launch_gain(const DGraph& g, const idx_t* part, int k, const long long* pw0, const long long* over_thr,
                        idx_t* mover, idx_t* ncand, idx_t* wfrom, idx_t* cand_p, idx_t* cand_g, const idx_t* heavy,
                        int32_t nheavy, int32_t* ghist, cudaStream_t st, const int32_t* stop = nullptr,
-                       const idx_t* only = nullptr, int block = 256) {
+                       const idx_t* only = nullptr, int block = 256, bool clear_only = false) {
   const int blocks = grid_for(g.n, block, 148 * 32 * 256 / block);
   // Algorithmic bytes of a full pass: xadj, part (own + neighbour gathers),
   // adjncy, adjwgt, mover flag.
@@ -1245,10 +1250,10 @@ static int launch_gain(const DGraph& g, const idx_t* part, int k, const long lon
   const int ph = MODE == kCut ? profiler().begin(kProfGain, st) : -1;
   if (g.adjwgt)
     k_gain<true, MODE><<<blocks, block, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, g.n, g.ncon, part, k, pw0, over_thr,
-                                                mover, ncand, wfrom, cand_p, cand_g, stop, only);
+                                                mover, ncand, wfrom, cand_p, cand_g, stop, only, clear_only);
   else
     k_gain<false, MODE><<<blocks, block, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, g.n, g.ncon, part, k, pw0, over_thr,
-                                                 mover, ncand, wfrom, cand_p, cand_g, stop, only);
+                                                 mover, ncand, wfrom, cand_p, cand_g, stop, only, clear_only);
   RMB_LAUNCH_CHECK();
   profiler().end(ph, st, bytes);
   if (nheavy > 0) {
@@ -1256,11 +1261,11 @@ static int launch_gain(const DGraph& g, const idx_t* part, int k, const long lon
     if (g.adjwgt)
       k_gain_heavy<true, MODE><<<hb, 128, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, heavy, nheavy, g.ncon, part, k, pw0,
                                                     over_thr, mover, ncand, wfrom, cand_p, cand_g, ghist, stop,
-                                                    only);
+                                                    only, clear_only);
     else
       k_gain_heavy<false, MODE><<<hb, 128, 0, st>>>(g.xadj, g.adjncy, g.adjwgt, heavy, nheavy, g.ncon, part, k, pw0,
                                                      over_thr, mover, ncand, wfrom, cand_p, cand_g, ghist, stop,
-                                                     only);
+                                                     only, clear_only);
     RMB_LAUNCH_CHECK();
   }
   return ph;
@@ -1507,6 +1512,7 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
   const bool admit = !fused && g.n > rp.exact_max_n && admit_supported(k, g.ncon);
   AdmitScratch as;
   int32_t* rounds = nullptr;
+  idx_t* touched[2] = {nullptr, nullptr};
   if (admit) {
     as.tgt = arena.alloc<int32_t>((size_t)g.n);
     as.src = arena.alloc<int32_t>((size_t)g.n);
@@ -1518,6 +1524,14 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
     as.cut = arena.alloc<int32_t>((size_t)k);
     RMB_CUDA(cudaMemsetAsync(as.out, 0, sizeof(long long) * (size_t)K, st));
     rounds = arena.alloc<int32_t>((size_t)rp.niter + 1);
+    // Incremental gain tables: after the first cut pass, a pass recomputes
+    // only the vertices the previous pass moved and their neighbours (the
+    // other entries are unchanged); each pass's moves flag the next pass's
+    // set, alternating between two flag arrays.
+    for (int b = 0; b < 2; ++b) {
+      touched[b] = arena.alloc<idx_t>((size_t)g.n);
+      RMB_CUDA(cudaMemsetAsync(touched[b], 0, sizeof(idx_t) * (size_t)g.n, st));
+    }
   }
   std::vector<int> walk_handles, gain_handles;
   if (fused) {
@@ -1570,7 +1584,9 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
       launch_gain<kRepair>(g, part, k, pw, rp.over_thr, mover, ncand, wfrom, cand_p, cand_g, heavy, nheavy, ghist, st);
     else
       gain_handles.push_back(launch_gain<kCut>(g, part, k, pw, rp.over_thr, mover, ncand, wfrom, cand_p, cand_g,
-                                               heavy, nheavy, ghist, st, stop, nullptr, rp.gain_block));
+                                               heavy, nheavy, ghist, st, stop,
+                                               admit && pass >= 2 ? touched[(pass - 1) & 1] : nullptr,
+                                               rp.gain_block, admit && pass >= 2));
     compact_flags(mover, g.n, movers, nm_dev, arena, st);
     if (mode == kRepair)
       walk_handles.push_back(launch_walk<kRepair>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r,
@@ -1578,7 +1594,8 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
                                                   rp.small_weights, long_flag, st));
     else if (admit)
       walk_handles.push_back(admit_cut_pass(g, k, g.n, nm_dev, movers, ncand, wfrom, cand_p, cand_g, part, pw,
-                                            rp.feas_max, nm_dev + 1, rounds + pass, as, st));
+                                            rp.feas_max, nm_dev + 1, rounds + pass, as, st, true,
+                                            pass + 1 <= rp.niter ? touched[pass & 1] : nullptr));
     else
       walk_handles.push_back(launch_walk<kCut>(g.n, nm_dev, movers, g, part, k, ncand, wfrom, cand_p, cand_g, r, pw,
                                                rp.feas_max, rp.over_thr, in_max, out_max, nm_dev + 1,

@@ -94,7 +94,20 @@ def test_committed_table_is_well_formed():
                 assert s["contract_thread_max"] in (16, 32) and s["gain_block"] in (128, 256, 512)
             else:
                 assert s["exact_max_n"] in A.EXACT_CANDIDATES
-                assert s["cut_ratio"] <= 1.0 + A.QUALITY_TOL or s["exact_max_n"] == max(A.EXACT_CANDIDATES)
+                assert s["cut_ratio"] <= 1.0 + A.QUALITY_TOL or s["exact_max_n"] == A.EXACT_DEFAULT
+
+
+def test_tune_scores_items_relative_to_the_first_setting():
+    """With per-item times, a setting that halves a small item's time beats
+    one that saves the same absolute time on a large item."""
+    items = {"a": [1.0, 0.010], "b": [0.99, 0.005], "c": [0.985, 0.010]}
+
+    def run(s):
+        run.item_times = list(items[s["name"]])
+        return [_res(1, [0])]
+    run.item_times = []
+    trials = A.tune(run, [{"name": "a"}, {"name": "b"}, {"name": "c"}], repeats=1)
+    assert [t.setting["name"] for t in trials] == ["b", "c", "a"]
 
 
 def test_shape_candidates_start_with_the_defaults():
