@@ -94,10 +94,10 @@ RMETIS_API int RMETIS_PartGraphKway(const idx_t *nvtxs, const idx_t *ncon, const
  * subgraph extraction follow the reference on the host; each bisection is a
  * 2-way multilevel partition on the GPU (coarsening to 40 vertices, grow
  * trials, refinement), and the bisections of one recursion level run
- * concurrently on the device's worker pool. Differences: rtype Fm refines a
- * bisection with the k-way FM rule (positive-gain moves) rather than the
- * reference's 2-way FM (src/refine/fm.rs, which also makes negative moves and
- * rolls back), and the bisection at position h of the recursion tree (root 0,
+ * concurrently on the device's worker pool. With rtype Fm every bisection is
+ * refined by the reference's 2-way FM rule (src/refine/fm.rs: negative moves
+ * and a rollback to the lowest cut) in parallel rounds (RMETIS_GPU_Fm2Refine).
+ * Differences: the order of those moves, and the bisection at position h of the recursion tree (root 0,
  * children 2h+1, 2h+2) runs with seed + h where the reference draws all
  * bisections from one generator; partitions match the reference's in quality,
  * not bit for bit. Graphs with more than 8 constraints return
@@ -119,7 +119,7 @@ RMETIS_API int RMETIS_PartGraphRecursive(const idx_t *nvtxs, const idx_t *ncon, 
  * reference does. Each bisection is a 2-way multilevel partition on the GPU;
  * the bisections of one recursion level run concurrently on the device's
  * worker pool. The bisections differ from the reference's (parallel matching,
- * the k-way refinement rules for rtype Fm), so orderings match it in quality
+ * the 2-way FM moves in parallel rounds for rtype Fm), so orderings match it in quality
  * (separator sizes, fill), not bit for bit. */
 RMETIS_API int RMETIS_NodeND(const idx_t *nvtxs, const idx_t *xadj, const idx_t *adjncy, const idx_t *vwgt,
                              const idx_t *options, idx_t *perm, idx_t *iperm);
@@ -304,6 +304,22 @@ RMETIS_API int RMETIS_GPU_GreedyRefine(idx_t n, idx_t ncon, const idx_t *xadj, c
 RMETIS_API int RMETIS_GPU_FmRefine(idx_t n, idx_t ncon, const idx_t *xadj, const idx_t *adjncy, const idx_t *vwgt,
                                    const idx_t *adjwgt, idx_t *part, idx_t nparts, const double *targets,
                                    const double *ubvec, idx_t niter, idx_t *cut, int64_t *stats);
+
+/* fm_refine (src/refine/fm.rs:12-127) of a bisection: the refinement that
+ * RMETIS_PartGraphRecursive applies to every bisection with rtype Fm
+ * (refine_2way, src/partition/recursive.rs:184-186). A pass moves free
+ * boundary vertices to the other side, negative gains included, each move
+ * feasible ((pw+vw) as f64 <= target*ub), moved vertices locked for the pass,
+ * then undoes the moves after the lowest cut of the pass; passes repeat while
+ * one improves (at most niter). Here a pass moves rounds of non-adjacent
+ * local-maximum vertices and rolls back to the best round, so results match
+ * the reference in quality, not bit for bit. targets: [2][ncon]; stats
+ * (optional, 4 entries): passes, moves kept, rounds, selected movers. The cut
+ * never rises; each side ends at most at max(its start weight,
+ * floor(target*ub)). */
+RMETIS_API int RMETIS_GPU_Fm2Refine(idx_t n, idx_t ncon, const idx_t *xadj, const idx_t *adjncy, const idx_t *vwgt,
+                                    const idx_t *adjwgt, idx_t *part, const double *targets, const double *ubvec,
+                                    idx_t niter, idx_t *cut, int64_t *stats);
 
 /* Edge cut and partition weights of a device-resident graph without any
  * allocation, for callers that cannot allocate device memory at the point of

@@ -43,6 +43,8 @@ SIGNATURES = {
                                 F64P, ctypes.c_int32, I32P, I64P],
     "RMETIS_GPU_FmRefine": [ctypes.c_int32, ctypes.c_int32, I32P, I32P, I32P, I32P, I32P, ctypes.c_int32, F64P,
                             F64P, ctypes.c_int32, I32P, I64P],
+    "RMETIS_GPU_Fm2Refine": [ctypes.c_int32, ctypes.c_int32, I32P, I32P, I32P, I32P, I32P, F64P, F64P,
+                             ctypes.c_int32, I32P, I64P],
     "RMETIS_GPU_EdgeCutWeightsNoAlloc": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, VP, VP, VP, VP, VP,
                                          ctypes.c_int32, VP, VP, VP],
     "RMETIS_GPU_PartGraphKwayBatch": [ctypes.c_int32, ctypes.c_int32, I64P, I64P, I32P, I32P, I32P, I32P, I32P,

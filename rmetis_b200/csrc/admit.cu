@@ -71,6 +71,7 @@ struct PickArgs {
   int32_t* src;
   int32_t* w;      // [nm][ncon]
   long long* out;  // [k][ncon], zero on entry: weight of the picks out of each part
+  int any_gain;    // 1: the first feasible candidate is picked whatever its gain (2-way FM rounds)
 };
 
 __global__ void k_admit_pick(PickArgs A) {
@@ -97,7 +98,7 @@ __global__ void k_admit_pick(PickArgs A) {
       // Candidates are sorted by (gain desc, part asc); parts outside the
       // list have gain ig <= 0 and never qualify.
       for (int32_t i = 0; i < ne; ++i) {
-        if (A.cand_g[s + i] <= 0) break;
+        if (A.cand_g[s + i] <= 0 && !A.any_gain) break;
         const int32_t p = A.cand_p[s + i];
         if (feasible(p)) {
           t = p;
@@ -495,7 +496,7 @@ bool admit_supported(int k, int ncon) {
 int admit_cut_pass(const DGraph& g, int k, int32_t nmax, const int32_t* nm_dev, const idx_t* movers,
                    const idx_t* ncand, const idx_t* wfrom, const idx_t* cand_p, const idx_t* cand_g, idx_t* part,
                    long long* pw, const long long* feas, int32_t* nmoves, int32_t* rounds_out,
-                   const AdmitScratch& s, cudaStream_t st, bool apply, idx_t* touched) {
+                   const AdmitScratch& s, cudaStream_t st, bool apply, idx_t* touched, bool any_gain) {
   const int ph = profiler().begin(kProfAdmit, st);
   PickArgs P;
   P.nm_dev = nm_dev;
@@ -515,6 +516,7 @@ int admit_cut_pass(const DGraph& g, int k, int32_t nmax, const int32_t* nm_dev, 
   P.src = s.src;
   P.w = s.w;
   P.out = s.out;
+  P.any_gain = any_gain ? 1 : 0;
   const int blocks = grid_for(nmax, 256, 148 * 4);
   k_admit_pick<<<blocks, 256, 0, st>>>(P);
   RMB_LAUNCH_CHECK();

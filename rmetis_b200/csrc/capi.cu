@@ -289,6 +289,7 @@ void bisect(Engine& E, const HostGraph& g, const std::vector<float>& tp2, const 
   ob.seed = seed;
   ob.ncuts = 1;
   ob.parallel_attempts = 0;
+  ob.bisect_fm2 = 1;  // refine_2way (recursive.rs:184-186): the 2-way FM of fm.rs for rtype Fm
   int32_t obj = 0;
   E.partition_kway(dg, 2, tp2.data(), ubvec, ob, d_part, &obj, nullptr);
   download(E, part.data(), d_part, (size_t)g.n);
@@ -1096,8 +1097,9 @@ int RMETIS_GPU_GrowPartition(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t
   });
 }
 
-// The refinement of a host graph and partition by greedy_refine or fm_refine.
-static int refine_entry(bool fm, idx_t n, idx_t ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
+// The refinement of a host graph and partition by greedy_refine (fm 0),
+// fm_refine (fm 1) or the 2-way fm2_refine (fm 2).
+static int refine_entry(int fm, idx_t n, idx_t ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
                         const idx_t* adjwgt, idx_t* part, idx_t nparts, const double* targets, const double* ubvec,
                         idx_t niter, idx_t* cut, int64_t* stats) {
   return guarded([&] {
@@ -1133,8 +1135,9 @@ static int refine_entry(bool fm, idx_t n, idx_t ncon, const idx_t* xadj, const i
         for (int c = 0; c < ncon; ++c) tot[c] += vwgt ? vwgt[v * ncon + c] : 1;
       rp.small_weights = weights_fit_int32(tot.data(), ncon, feas.data(), over.data(), K);
     }
-    RefineStats rs = fm ? fm_refine(g, d_part, rp, d_heavy, nh, h.E.arena(), h.st(), h.E.host_scratch())
-                        : greedy_refine(g, d_part, rp, d_heavy, nh, h.E.arena(), h.st(), h.E.host_scratch());
+    RefineStats rs = fm == 2   ? fm2_refine(g, d_part, rp, h.E.arena(), h.st(), h.E.host_scratch())
+                     : fm == 1 ? fm_refine(g, d_part, rp, d_heavy, nh, h.E.arena(), h.st(), h.E.host_scratch())
+                               : greedy_refine(g, d_part, rp, d_heavy, nh, h.E.arena(), h.st(), h.E.host_scratch());
     unsigned long long* acc = h.E.arena().alloc<unsigned long long>(1);
     cut_and_weights(g, d_part, nparts, acc, nullptr, h.st());
     download(h.E, part, d_part, (size_t)n);
@@ -1156,13 +1159,19 @@ static int refine_entry(bool fm, idx_t n, idx_t ncon, const idx_t* xadj, const i
 int RMETIS_GPU_GreedyRefine(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
                             const idx_t* adjwgt, idx_t* part, idx_t nparts, const double* targets,
                             const double* ubvec, idx_t niter, idx_t* cut, int64_t* stats) {
-  return refine_entry(false, n, ncon, xadj, adjncy, vwgt, adjwgt, part, nparts, targets, ubvec, niter, cut, stats);
+  return refine_entry(0, n, ncon, xadj, adjncy, vwgt, adjwgt, part, nparts, targets, ubvec, niter, cut, stats);
 }
 
 int RMETIS_GPU_FmRefine(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
                         const idx_t* adjwgt, idx_t* part, idx_t nparts, const double* targets, const double* ubvec,
                         idx_t niter, idx_t* cut, int64_t* stats) {
-  return refine_entry(true, n, ncon, xadj, adjncy, vwgt, adjwgt, part, nparts, targets, ubvec, niter, cut, stats);
+  return refine_entry(1, n, ncon, xadj, adjncy, vwgt, adjwgt, part, nparts, targets, ubvec, niter, cut, stats);
+}
+
+int RMETIS_GPU_Fm2Refine(idx_t n, idx_t ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
+                         const idx_t* adjwgt, idx_t* part, const double* targets, const double* ubvec, idx_t niter,
+                         idx_t* cut, int64_t* stats) {
+  return refine_entry(2, n, ncon, xadj, adjncy, vwgt, adjwgt, part, 2, targets, ubvec, niter, cut, stats);
 }
 
 }  // extern "C"

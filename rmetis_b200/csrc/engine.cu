@@ -456,7 +456,8 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
         RMB_CUDA(cudaEventRecord(rec.a, st));
       }
       RefineStats rs = rtype == 1 ? greedy_refine(lg, lpart, lrp, hl, nh, arena_, st, h_scratch_)
-                                  : fm_refine(lg, lpart, lrp, hl, nh, arena_, st, h_scratch_);
+                       : (k == 2 && o.bisect_fm2) ? fm2_refine(lg, lpart, lrp, arena_, st, h_scratch_)
+                                                   : fm_refine(lg, lpart, lrp, hl, nh, arena_, st, h_scratch_);
       if (json) {
         RMB_CUDA(cudaEventRecord(rec.b, st));
         rec.passes = rs.passes;

@@ -184,6 +184,14 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
 RefineStats fm_refine(const DGraph& g, idx_t* part, const RefineParams& rp, const idx_t* heavy, int32_t nheavy,
                       Arena& arena, cudaStream_t st, int32_t* h_scratch);
 
+// fm_refine (src/refine/fm.rs:12-127) of a bisection (k = 2): passes of
+// moves of free boundary vertices, negative gains included, then a rollback
+// to the lowest cut of the pass; in rounds of non-adjacent local-maximum
+// moves admitted by the parallel admission. Stats: passes, moves kept,
+// rounds, selected movers.
+RefineStats fm2_refine(const DGraph& g, idx_t* part, const RefineParams& rp, Arena& arena, cudaStream_t st,
+                       int32_t* h_scratch);
+
 // Gain table of one pass (boundary_vertices + compute_move_gain,
 // src/graph/mod.rs:164-171, src/refine/greedy.rs:197-218): per vertex the
 // boundary flag, w_from and the explicit candidate list sorted by
@@ -219,7 +227,8 @@ bool admit_supported(int k, int ncon);
 int admit_cut_pass(const DGraph& g, int k, int32_t nmax, const int32_t* nm_dev, const idx_t* movers,
                    const idx_t* ncand, const idx_t* wfrom, const idx_t* cand_p, const idx_t* cand_g, idx_t* part,
                    long long* pw, const long long* feas, int32_t* nmoves, int32_t* rounds_out,
-                   const AdmitScratch& s, cudaStream_t st, bool apply = true, idx_t* touched = nullptr);
+                   const AdmitScratch& s, cudaStream_t st, bool apply = true, idx_t* touched = nullptr,
+                   bool any_gain = false);
 
 // Opts a kernel in to `bytes` of dynamic shared memory on the current device
 // (once per kernel and device; safe from several host threads).

@@ -68,6 +68,21 @@ def greedy_refine(graph: Graph, part, nparts: int, targets, ubvec, niter: int = 
     return part, int(cut.value), stats
 
 
+def fm2_refine(graph: Graph, part, targets, ubvec, niter: int = 10):
+    """2-way fm_refine (src/refine/fm.rs:12-28) of a bisection on the GPU.
+    Returns (refined part, edge cut, stats[passes, moves kept, rounds, movers])."""
+    part = np.array(part, dtype=np.int32)
+    t = np.ascontiguousarray(targets, dtype=np.float64)
+    ub = np.ascontiguousarray(ubvec, dtype=np.float64)
+    cut = ctypes.c_int32(0)
+    stats = np.zeros(4, np.int64)
+    rc = _lib.load().RMETIS_GPU_Fm2Refine(graph.nvtxs, graph.ncon, _p(graph.xadj), _p(graph.adjncy),
+                                          _p(graph.vwgt), _p(graph.adjwgt), _p(part), _p(t, F64P), _p(ub, F64P),
+                                          niter, ctypes.byref(cut), _p(stats, I64P))
+    _raise_for(rc, "fm2_refine")
+    return part, int(cut.value), stats
+
+
 def fm_refine(graph: Graph, part, nparts: int, targets, ubvec, niter: int = 10):
     """fm_kway_refine (src/refine/fm_kway.rs:12-31) on the GPU. Returns
     (refined part, edge cut, stats[passes, moves, rounds with movers, movers])."""
