@@ -188,15 +188,26 @@ RMETIS_API int RMETIS_GPU_SetPoolTuning(int fused_max_n, int tail_max_n);
  * CSR entries; its xadj (n_g+1 local offsets) starts at xadj[vtx_off[g]+g],
  * its adjncy/adjwgt (local vertex ids) at edge_off[g], its vwgt at
  * vtx_off[g]*ncon, its part at part[vtx_off[g]]. nparts[g] per graph; ncon,
- * ubvec and options are shared. The batch is uploaded once and the graphs are
- * partitioned concurrently on the device's worker pool; each result equals
- * the one of a separate RMETIS_PartGraphKway call. status[g] gets each graph's
- * return code; the call returns METIS_OK or the first failing code. */
+ * ubvec and options are shared. The batch is uploaded once. With Greedy
+ * refinement (options[METIS_OPTION_RTYPE] = 1), ncuts 1, a grown initial
+ * partition, ncon <= 2 and nparts[g] <= 256, the graphs go through the
+ * pipeline together: each step (validation, coarsening, grow trials, the
+ * refinement of one level per graph, the cut) is one launch over the batch,
+ * one thread block per graph; the other graphs are partitioned concurrently
+ * on the device's worker pool. Either way each result equals the one of a
+ * separate RMETIS_PartGraphKway call. status[g] gets each graph's return code;
+ * the call returns METIS_OK or the first failing code. */
 RMETIS_API int RMETIS_GPU_PartGraphKwayBatch(idx_t ngraphs, idx_t ncon, const int64_t *vtx_off,
                                              const int64_t *edge_off, const idx_t *xadj, const idx_t *adjncy,
                                              const idx_t *vwgt, const idx_t *adjwgt, const idx_t *nparts,
                                              const real_t *ubvec, const idx_t *options, idx_t *objval,
                                              idx_t *part, idx_t *status);
+
+/* 1 (default): eligible graphs of RMETIS_GPU_PartGraphKwayBatch run through
+ * the batched launches; 0: every graph runs on the worker pool (no
+ * counterpart in the reference; results are the same either way). Other
+ * values return METIS_ERROR_INPUT. */
+RMETIS_API int RMETIS_GPU_SetBatchMode(int mode);
 
 /* Asynchronous requests for a serving loop (no counterpart in the reference).
  * Same arguments as RMETIS_PartGraphKway without vsize; returns a ticket > 0,

@@ -417,9 +417,19 @@ def set_pool_tuning(fused_max_n: int = -2, tail_max_n: int = -2):
     _raise_for(_lib.load().RMETIS_GPU_SetPoolTuning(fused_max_n, tail_max_n), "set_pool_tuning")
 
 
+def set_batch_mode(mode: int = 1):
+    """1 (default): eligible graphs of part_graph_kway_batch (Greedy, ncuts 1,
+    grown initial partitions, ncon <= 2, nparts <= 256) go through the
+    batched launches, one step of the pipeline for all graphs at a time; 0:
+    every graph runs on the worker pool. Results are the same either way."""
+    _raise_for(_lib.load().RMETIS_GPU_SetBatchMode(mode), "set_batch_mode")
+
+
 def part_graph_kway_batch(graphs, nparts, ubvec=None, options: Options | None = None):
-    """Partition many graphs in one call: the batch is uploaded once and the
-    graphs run concurrently on the device's worker pool. Returns one
+    """Partition many graphs in one call: the batch is uploaded once; eligible
+    graphs go through the pipeline together (one launch per step, one block
+    per graph, see set_batch_mode), the others run concurrently on the
+    device's worker pool. Returns one
     PartitionResult per graph, each equal to part_graph_kway's for that graph.
     `nparts` is an int or one value per graph; all graphs share ncon and
     either all have vertex (edge) weights or none has."""

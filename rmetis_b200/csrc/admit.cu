@@ -34,6 +34,8 @@
 // checkers that replay a pass bit for bit.
 #include "kernels.h"
 #include "prof.h"
+#include "scan.cuh"
+#include "gain.cuh"
 
 namespace rmb {
 
@@ -74,10 +76,10 @@ struct PickArgs {
   int any_gain;    // 1: the first feasible candidate is picked whatever its gain (2-way FM rounds)
 };
 
-__global__ void k_admit_pick(PickArgs A) {
+__device__ void pick_body(const PickArgs& A, Lanes L) {
   const int32_t nm = *A.nm_dev;
   const int32_t ncon = A.ncon;
-  RMB_GRID_STRIDE(j, nm) {
+  RMB_FOR(j, nm, L) {
     const int32_t v = A.movers[j];
     const int32_t pv = A.part[v];
     const int32_t s = A.xadj[v];
@@ -130,18 +132,20 @@ __global__ void k_admit_pick(PickArgs A) {
   }
 }
 
+__global__ void k_admit_pick(PickArgs A) { pick_body(A, grid_lanes()); }
+
 // The admitted moves of a pass, applied to the part vector: mover j moves to
 // its target when its rank in the target's in-list is below the part's
 // admitted prefix.
 // With `touched`, every moved vertex and its neighbours are flagged there:
 // the only vertices whose gain table the move changes.
-__global__ void k_admit_apply(const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
-                              const int32_t* __restrict__ tgt, const int32_t* __restrict__ rank,
-                              const int32_t* __restrict__ cut, idx_t* __restrict__ part,
-                              const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
-                              idx_t* __restrict__ touched) {
+__device__ void apply_body(Lanes L, const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
+                           const int32_t* __restrict__ tgt, const int32_t* __restrict__ rank,
+                           const int32_t* __restrict__ cut, idx_t* __restrict__ part,
+                           const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                           idx_t* __restrict__ touched) {
   const int32_t nm = *nm_dev;
-  RMB_GRID_STRIDE(j, nm) {
+  RMB_FOR(j, nm, L) {
     const int32_t t = tgt[j];
     if (t >= 0 && rank[j] < cut[t]) {
       const int32_t v = movers[j];
@@ -152,6 +156,14 @@ __global__ void k_admit_apply(const int32_t* __restrict__ nm_dev, const idx_t* _
       }
     }
   }
+}
+
+__global__ void k_admit_apply(const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
+                              const int32_t* __restrict__ tgt, const int32_t* __restrict__ rank,
+                              const int32_t* __restrict__ cut, idx_t* __restrict__ part,
+                              const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                              idx_t* __restrict__ touched) {
+  apply_body(grid_lanes(), nm_dev, movers, tgt, rank, cut, part, xadj, adj, touched);
 }
 
 // ---------------------------------------------------------------------------
@@ -241,8 +253,9 @@ __device__ int32_t fit_prefix(const long long* pref, int32_t ncon, int32_t off_p
   return good;
 }
 
-__global__ void __launch_bounds__(kAdmitThreads, 1) k_admit(AdmitArgs A) {
-  extern __shared__ __align__(16) unsigned char smem[];
+// The admission of one pass by a block of kAdmitThreads threads; smem:
+// kAdmitMaxSmem bytes of dynamic shared memory.
+__device__ void admit_body(const AdmitArgs& A, unsigned char* smem) {
   const AdmitSmem L(A.k, A.ncon);
   long long* pw_s = reinterpret_cast<long long*>(smem + L.pw);
   long long* feas_s = reinterpret_cast<long long*>(smem + L.feas);
@@ -485,6 +498,82 @@ __global__ void __launch_bounds__(kAdmitThreads, 1) k_admit(AdmitArgs A) {
   }
 }
 
+__global__ void __launch_bounds__(kAdmitThreads, 1) k_admit(AdmitArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  admit_body(A, smem);
+}
+
+// The cut passes of admission levels of a batch: block b refines the level
+// of jobs[b] (its part vector and part weights left by k_batch_level's repair
+// pass). Each pass as greedy_refine runs it with admit_cut_pass: gain table
+// (the first pass everywhere, later ones for the vertices the last pass
+// moved and their neighbours), mover list in ascending id, picks, admission,
+// moves; a pass without a move ends the level (greedy.rs:184-186).
+template <bool HAS_W>
+__global__ void __launch_bounds__(kAdmitThreads, 1) k_batch_admit(const LevelJob* __restrict__ jobs) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int32_t sw[32];
+  const LevelJob& J = jobs[blockIdx.x];
+  const Lanes L = block_lanes();
+  const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int pass = 1; pass <= J.niter; ++pass) {
+    if (pass >= 2 && J.counters[2 * (pass - 1) + 1] == 0) break;
+    idx_t* only = pass >= 2 ? J.touched[(pass - 1) & 1] : nullptr;
+    int32_t* nm_dev = J.counters + 2 * pass;
+    gain_body<HAS_W, kCut>(L, J.xadj, J.adjncy, J.adjwgt, J.n, J.ncon, J.part, J.k, J.pw, J.over, J.mover, J.ncand,
+                           J.wfrom, J.cand_p, J.cand_g, only, only != nullptr);
+    if (J.nheavy > 0)
+      gain_heavy_body<HAS_W, kCut>(warp, nwarps, J.ghist + (int64_t)warp * J.k, J.xadj, J.adjncy, J.adjwgt,
+                                   J.heavy, J.nheavy, J.ncon, J.part, J.k, J.pw, J.over, J.mover, J.ncand, J.wfrom,
+                                   J.cand_p, J.cand_g, only, only != nullptr);
+    __syncthreads();
+    block_scan_n<int32_t>(LoadNonZero{J.mover}, StoreCompact{J.mover, J.movers}, J.n, nm_dev, sw);
+    __syncthreads();
+    PickArgs P;
+    P.nm_dev = nm_dev;
+    P.movers = J.movers;
+    P.xadj = J.xadj;
+    P.ncand = J.ncand;
+    P.wfrom = J.wfrom;
+    P.cand_p = J.cand_p;
+    P.cand_g = J.cand_g;
+    P.vwgt = J.vwgt;
+    P.part = J.part;
+    P.pw = J.pw;
+    P.feas = J.feas;
+    P.ncon = J.ncon;
+    P.k = J.k;
+    P.tgt = J.a_tgt;
+    P.src = J.a_src;
+    P.w = J.a_w;
+    P.out = J.a_out;
+    P.any_gain = 0;
+    pick_body(P, L);
+    __syncthreads();
+    AdmitArgs A;
+    A.nm_dev = nm_dev;
+    A.ncon = J.ncon;
+    A.k = J.k;
+    A.pw = J.pw;
+    A.feas = J.feas;
+    A.nmoves = nm_dev + 1;
+    A.rounds_out = nullptr;
+    A.tgt = J.a_tgt;
+    A.src = J.a_src;
+    A.w = J.a_w;
+    A.rank = J.a_rank;
+    A.out_g = J.a_out;
+    A.cut_g = J.a_cut;
+    A.pref_g = J.a_pref;
+    A.src_g = J.a_gsrc;
+    admit_body(A, smem);
+    __syncthreads();
+    apply_body(L, nm_dev, J.movers, J.a_tgt, J.a_rank, J.a_cut, J.part, J.xadj, J.adjncy,
+               pass + 1 <= J.niter ? J.touched[pass & 1] : nullptr);
+    __syncthreads();
+  }
+}
+
 }  // namespace
 
 size_t admit_smem_bytes(int k, int ncon) { return AdmitSmem(k, ncon).total; }
@@ -545,6 +634,16 @@ int admit_cut_pass(const DGraph& g, int k, int32_t nmax, const int32_t* nm_dev, 
   }
   profiler().end(ph, st, 0.0);
   return ph;
+}
+
+void batch_admit_launch(const LevelJob* d_jobs, int njobs, bool has_w, cudaStream_t st) {
+  if (njobs <= 0) return;
+  const int ph = profiler().begin(kProfAdmit, st);
+  auto kern = has_w ? k_batch_admit<true> : k_batch_admit<false>;
+  allow_dyn_smem((const void*)kern, kAdmitMaxSmem);
+  kern<<<njobs, kAdmitThreads, kAdmitMaxSmem, st>>>(d_jobs);
+  RMB_LAUNCH_CHECK();
+  profiler().end(ph, st, 0.0);
 }
 
 }  // namespace rmb

@@ -46,6 +46,11 @@ struct Tuning {
   int contract_thread_max = 32;
   int gain_block = 256;
 };
+// 1: batches run through the batched kernels (RMETIS_GPU_SetBatchMode).
+int& batch_mode() {
+  static int m = 1;
+  return m;
+}
 Tuning& tuning() {
   static Tuning t;
   return t;
@@ -724,6 +729,12 @@ int RMETIS_GPU_SetKernelShapes(int contract_thread_max, int gain_block) {
   return METIS_OK;
 }
 
+int RMETIS_GPU_SetBatchMode(int mode) {
+  if (mode < 0 || mode > 1) return METIS_ERROR_INPUT;
+  batch_mode() = mode;
+  return METIS_OK;
+}
+
 int RMETIS_GPU_SetPoolTuning(int fused_max_n, int tail_max_n) {
   if (fused_max_n >= -1) pool_tuning().fused_max_n = fused_max_n;
   if (tail_max_n >= -1) pool_tuning().tail_max_n = tail_max_n;
@@ -785,19 +796,59 @@ int RMETIS_GPU_PartGraphKwayBatch(idx_t ngraphs, idx_t ncon, const int64_t* vtx_
     idx_t* d_vwgt = upload(E, vwgt, (size_t)ntot * ncon);
     idx_t* d_adjwgt = upload(E, adjwgt, (size_t)mtot);
     idx_t* d_part = E.arena().alloc<idx_t>((size_t)ntot);
+    std::vector<int> done(ngraphs, 0);
+    std::vector<int32_t> objs(ngraphs, 0);
+    if (batch_mode() == 1) {
+      // Eligible graphs through the batched kernels (one launch per step for
+      // all of them); the rest, and any graph they could not finish, alone.
+      std::vector<BatchItem> items;
+      std::vector<idx_t> which;
+      for (idx_t g = 0; g < ngraphs; ++g) {
+        const int64_t v0 = vtx_off[g], e0 = edge_off[g];
+        const int32_t n = (int32_t)(vtx_off[g + 1] - v0);
+        if (!batch_eligible(o, n, nparts[g], ncon)) continue;
+        BatchItem it;
+        it.g.n = n;
+        it.g.m = edge_off[g + 1] - e0;
+        it.g.ncon = ncon;
+        it.g.xadj = d_xadj + v0 + g;
+        it.g.adjncy = d_adj + e0;
+        it.g.adjwgt = d_adjwgt ? d_adjwgt + e0 : nullptr;
+        it.g.vwgt = d_vwgt ? d_vwgt + v0 * ncon : nullptr;
+        it.k = nparts[g];
+        it.part_out = d_part + v0;
+        items.push_back(it);
+        which.push_back(g);
+      }
+      if (!items.empty()) {
+        try {
+          E.partition_kway_batch(items, ubvec, o);
+        } catch (const Error& e) {
+          if (e.code != METIS_ERROR_MEMORY) throw;
+          for (BatchItem& it : items) it.status = 0;  // out of device memory: every graph alone
+        }
+        for (size_t i = 0; i < items.size(); ++i) {
+          if (items[i].status == 0) continue;
+          const idx_t g = which[i];
+          done[g] = 1;
+          status[g] = items[i].status;
+          objval[g] = items[i].objval;
+        }
+      }
+    }
     RMB_CUDA(cudaStreamSynchronize(E.stream()));
     int dev = 0;
     RMB_CUDA(cudaGetDevice(&dev));
     WorkerPool& pool = pool_for_device(dev);
-    std::vector<std::future<int>> fut;
-    std::vector<int32_t> objs(ngraphs, 0);
+    std::vector<std::future<int>> fut(ngraphs);
     for (idx_t g = 0; g < ngraphs; ++g) {
+      if (done[g]) continue;
       const int64_t v0 = vtx_off[g], e0 = edge_off[g];
       const int32_t n = (int32_t)(vtx_off[g + 1] - v0);
       const int64_t m = edge_off[g + 1] - e0;
       const int32_t k = nparts[g];
       int32_t* obj_g = &objs[g];
-      fut.push_back(pool.submit(footprint_bytes(n, m, std::max(k, 2), ncon), [=](Engine& W) {
+      fut[g] = pool.submit(footprint_bytes(n, m, std::max(k, 2), ncon), [=](Engine& W) {
         DGraph gr;
         gr.n = n;
         gr.m = m;
@@ -809,12 +860,14 @@ int RMETIS_GPU_PartGraphKwayBatch(idx_t ngraphs, idx_t ncon, const int64_t* vtx_
         if (k < 2 || k > n) return (int)METIS_ERROR_INPUT;
         if (validate_device(gr, W.arena(), W.stream(), W.host_scratch()) != 0) return (int)METIS_ERROR_INPUT;
         return W.partition_kway(gr, k, nullptr, ubvec, o, d_part + v0, obj_g, nullptr);
-      }));
+      });
     }
     int rc = METIS_OK;
     for (idx_t g = 0; g < ngraphs; ++g) {
-      status[g] = fut[g].get();
-      objval[g] = objs[g];
+      if (!done[g]) {
+        status[g] = fut[g].get();
+        objval[g] = objs[g];
+      }
       if (status[g] != METIS_OK && rc == METIS_OK) rc = status[g];
     }
     download(E, part, d_part, (size_t)ntot);

@@ -650,18 +650,10 @@ CoarseResult contract(const DGraph& g, const idx_t* match, int coarse_vwgt, Aren
 // ---------------------------------------------------------------------------
 constexpr int kTailThreads = 1024;
 
-struct TailArgs {
-  DGraph g;
-  int has_vw, summed_unit, mode, lvl0, k, rounds;
-  uint64_t seed64;
-  long long limit;
-  char* ws;
-  long long ws_bytes;
-};
 
 __device__ __forceinline__ long long tail_round(long long b) { return (b + 255) & ~255LL; }
 
-__global__ void __launch_bounds__(kTailThreads, 1) k_coarsen_tail(TailArgs a) {
+__device__ void tail_body(const TailArgs& a) {
   __shared__ idx_t sw[32];
   __shared__ int32_t lanew_all[kTailThreads / 32][32];
   __shared__ int32_t xs_all[kTailThreads / 32][33];
@@ -875,6 +867,37 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_coarsen_tail(TailArgs a) {
     out->ncoarse = nc;
     out->finished = finished;
   }
+}
+
+__global__ void __launch_bounds__(kTailThreads, 1) k_coarsen_tail(TailArgs a) { tail_body(a); }
+
+// The coarsening of a batch of graphs: block b coarsens graph order[b]
+// (largest first, so the longest jobs start first); a graph flagged in bad
+// (failed validation) gets an empty level table.
+__global__ void __launch_bounds__(kTailThreads, 1) k_batch_coarsen(const TailArgs* __restrict__ args,
+                                                                   const int32_t* __restrict__ order,
+                                                                   const int32_t* __restrict__ bad) {
+  const int32_t gi = order[blockIdx.x];
+  const TailArgs a = args[gi];
+  if (bad[gi]) {
+    if (threadIdx.x == 0) {
+      TailOut* out = reinterpret_cast<TailOut*>(a.ws);
+      out->levels = 0;
+      out->ncoarse = 0;
+      out->finished = 0;
+    }
+    return;
+  }
+  tail_body(a);
+}
+
+void coarsen_tail_batch(const TailArgs* d_args, const int32_t* d_order, const int32_t* d_bad, int ngraphs,
+                        cudaStream_t st) {
+  if (ngraphs <= 0) return;
+  const int ph = profiler().begin(kProfTail, st);
+  k_batch_coarsen<<<ngraphs, kTailThreads, 0, st>>>(d_args, d_order, d_bad);
+  RMB_LAUNCH_CHECK();
+  profiler().end(ph, st, 0.0);
 }
 
 int64_t tail_workspace_bytes(const DGraph& g, int rounds) {

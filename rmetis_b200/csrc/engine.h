@@ -59,6 +59,21 @@ struct KwayTrace {
   int64_t refine_passes = 0, refine_moves = 0, decide_rounds = 0;
 };
 
+// One graph of a batched call: a device-resident graph, its part count and
+// its output (part_out on the device); objval and status are filled in.
+struct BatchItem {
+  DGraph g;
+  int k = 2;
+  idx_t* part_out = nullptr;
+  int32_t objval = 0;
+  int status = 0;
+};
+
+// Whether the batched kernels can run a graph with these options: Greedy
+// refinement, one attempt, grown initial partitions, ncon <= 2,
+// 2 <= k <= min(n, 256).
+bool batch_eligible(const KwayOptions& o, int32_t n, int k, int ncon);
+
 class Engine {
  public:
   // A worker engine (one per pool thread) never hands work to the pool.
@@ -77,6 +92,14 @@ class Engine {
   void run_attempt(const DGraph& g, int k, const float* tpwgts, const std::vector<double>& ub,
                    const std::vector<int32_t>& total0, const KwayOptions& o, uint64_t seed64, idx_t* part_out,
                    int32_t* objval, KwayTrace* trace);
+
+  // Every graph of a batch through the pipeline in a handful of launches,
+  // one block per graph and step (batch.cu). Each item's result equals the
+  // single call partition_kway(item.g, item.k, nullptr, ubvec, o, ...).
+  // Items must be eligible (batch_eligible); an item the batched kernels could
+  // not finish (a coarsening deeper than the level table) is left with
+  // status 0 for the caller to run alone. status: 1 done, -2 invalid graph.
+  void partition_kway_batch(std::vector<BatchItem>& items, const float* ubvec, const KwayOptions& o);
 
   void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
   cudaStream_t stream() const { return stream_; }

@@ -24,17 +24,12 @@ namespace rmb {
 // during its own turn, so the parts that may grow in a round are known at the
 // round's start.
 template <bool HAS_VW>
-__global__ void __launch_bounds__(32) k_grow(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
-                                             const idx_t* __restrict__ adjwgt, const idx_t* __restrict__ vwgt,
-                                             int32_t n, int32_t ncon, int32_t k, const idx_t* __restrict__ seeds,
-                                             const long long* __restrict__ grow_tgt, idx_t* __restrict__ parts,
-                                             unsigned char* __restrict__ gscratch, size_t scratch_bytes,
-                                             int use_smem) {
-  extern __shared__ __align__(16) unsigned char smem[];
+__device__ void grow_body(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                          const idx_t* __restrict__ vwgt, int32_t n, int32_t ncon, int32_t k,
+                          const idx_t* __restrict__ sd, const long long* __restrict__ grow_tgt,
+                          idx_t* __restrict__ out, unsigned char* base) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  const int trial = blockIdx.x;
-  unsigned char* base = use_smem ? smem : gscratch + (size_t)trial * scratch_bytes;
   long long* pw = reinterpret_cast<long long*>(base);
   idx_t* part = reinterpret_cast<idx_t*>(pw + (size_t)k * ncon);
   idx_t* next = part + n;
@@ -42,8 +37,6 @@ __global__ void __launch_bounds__(32) k_grow(const idx_t* __restrict__ xadj, con
   idx_t* tail = head + k;
   unsigned* needy = reinterpret_cast<unsigned*>(tail + k);
   const int32_t nwords = (k + 31) >> 5;
-  const idx_t* sd = seeds + (int64_t)trial * k;
-  idx_t* out = parts + (int64_t)trial * n;
 
   for (int32_t v = lane; v < n; v += 32) part[v] = -1;
   __syncwarp();
@@ -242,14 +235,70 @@ __global__ void __launch_bounds__(32) k_grow(const idx_t* __restrict__ xadj, con
   // Write the partition out; the trial cuts are computed edge-parallel for
   // all trials at once afterwards (trial_cuts).
   for (int32_t v = lane; v < n; v += 32) out[v] = part[v];
+  __syncwarp();
+}
+
+template <bool HAS_VW>
+__global__ void __launch_bounds__(32) k_grow(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                                             const idx_t* __restrict__ vwgt, int32_t n, int32_t ncon, int32_t k,
+                                             const idx_t* __restrict__ seeds,
+                                             const long long* __restrict__ grow_tgt, idx_t* __restrict__ parts,
+                                             unsigned char* __restrict__ gscratch, size_t scratch_bytes,
+                                             int use_smem) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int trial = blockIdx.x;
+  unsigned char* base = use_smem ? smem : gscratch + (size_t)trial * scratch_bytes;
+  grow_body<HAS_VW>(xadj, adj, vwgt, n, ncon, k, seeds + (int64_t)trial * k, grow_tgt, parts + (int64_t)trial * n,
+                    base);
+}
+
+// The grow trials of a batch of coarsest graphs: block b runs trial
+// b - first_block of job block_job[b] and then sums its directed edge cut
+// (the quantity trial_cuts computes) into the job's cuts.
+__global__ void __launch_bounds__(32) k_batch_grow(const GrowJob* __restrict__ jobs,
+                                                   const int32_t* __restrict__ block_job) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const GrowJob& J = jobs[block_job[blockIdx.x]];
+  const int trial = blockIdx.x - J.first_block;
+  unsigned char* base = J.use_smem ? smem : J.scratch + (size_t)trial * (size_t)J.scratch_bytes;
+  idx_t* out = J.parts + (int64_t)trial * J.n;
+  if (J.vwgt)
+    grow_body<true>(J.xadj, J.adjncy, J.vwgt, J.n, J.ncon, J.k, J.seeds + (int64_t)trial * J.k, J.grow_tgt, out,
+                    base);
+  else
+    grow_body<false>(J.xadj, J.adjncy, J.vwgt, J.n, J.ncon, J.k, J.seeds + (int64_t)trial * J.k, J.grow_tgt, out,
+                     base);
+  const int lane = threadIdx.x & 31;
+  unsigned long long acc = 0;
+  for (int32_t v = lane; v < J.n; v += 32) {
+    const int32_t pv = out[v];
+    for (int32_t j = J.xadj[v]; j < J.xadj[v + 1]; ++j)
+      if (out[J.adjncy[j]] != pv) acc += (unsigned long long)(long long)(J.adjwgt ? J.adjwgt[j] : 1);
+  }
+  acc = warp_sum(acc);
+  if (lane == 0) J.cuts[trial] = (long long)acc;
+}
+
+void grow_trials_batch(const GrowJob* d_jobs, const int32_t* d_block_job, int nblocks, size_t dyn_smem,
+                       cudaStream_t st) {
+  if (nblocks <= 0) return;
+  RMB_CUDA(cudaFuncSetAttribute(k_batch_grow, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
+  const int ph = profiler().begin(kProfGrow, st);
+  k_batch_grow<<<nblocks, 32, dyn_smem, st>>>(d_jobs, d_block_job);
+  RMB_LAUNCH_CHECK();
+  profiler().end(ph, st, 0.0);
+}
+
+size_t grow_scratch_bytes(int32_t n, int k, int ncon) {
+  const size_t bytes = sizeof(long long) * (size_t)k * ncon + sizeof(idx_t) * (2 * (size_t)n + 2 * (size_t)k) +
+                       sizeof(unsigned) * (((size_t)k + 31) / 32) + 16;
+  return (bytes + 255) & ~(size_t)255;
 }
 
 void grow_trials(const DGraph& g, int k, int ntrials, const idx_t* seeds, const long long* grow_tgt, idx_t* parts,
                  long long* cuts, Arena& arena, cudaStream_t st) {
   Arena::Mark mk = arena.mark();
-  const size_t bytes = sizeof(long long) * (size_t)k * g.ncon + sizeof(idx_t) * (2 * (size_t)g.n + 2 * (size_t)k) +
-                       sizeof(unsigned) * (((size_t)k + 31) / 32) + 16;
-  const size_t bytes_al = (bytes + 255) & ~(size_t)255;
+  const size_t bytes_al = grow_scratch_bytes(g.n, k, g.ncon);
   const size_t kSmemLimit = 200 * 1024;
   const int use_smem = bytes_al <= kSmemLimit ? 1 : 0;
   unsigned char* scratch = use_smem ? nullptr : arena.alloc<unsigned char>(bytes_al * (size_t)ntrials);
@@ -257,8 +306,8 @@ void grow_trials(const DGraph& g, int k, int ntrials, const idx_t* seeds, const 
   auto kern = g.vwgt ? k_grow<true> : k_grow<false>;
   RMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimit));
   const int ph = profiler().begin(kProfGrow, st);
-  kern<<<ntrials, 32, dyn, st>>>(g.xadj, g.adjncy, g.adjwgt, g.vwgt, g.n, g.ncon, k, seeds, grow_tgt, parts, scratch,
-                                 bytes_al, use_smem);
+  kern<<<ntrials, 32, dyn, st>>>(g.xadj, g.adjncy, g.vwgt, g.n, g.ncon, k, seeds, grow_tgt, parts, scratch, bytes_al,
+                                 use_smem);
   RMB_LAUNCH_CHECK();
   trial_cuts(g, parts, ntrials, cuts, st);
   profiler().end(ph, st, (double)ntrials * (16.0 * g.n + 8.0 * (double)g.m));

@@ -110,6 +110,26 @@ struct TailOut {
   int32_t coarse_vw[kTailMaxLevels];
 };
 
+// Arguments of one graph's coarsening in a single block (coarsen_tail and
+// the batched form).
+struct TailArgs {
+  DGraph g;
+  int has_vw, summed_unit, mode, lvl0, k, rounds;
+  uint64_t seed64;
+  long long limit;
+  char* ws;           // workspace of tail_workspace_bytes(g, rounds), 256-byte aligned; TailOut at its start
+  long long ws_bytes;
+};
+
+// Workspace bytes of one graph's single-block coarsening.
+int64_t tail_workspace_bytes(const DGraph& g, int rounds);
+
+// Every graph of a batch coarsened in one launch, one block per graph
+// (d_args[order[b]] for block b); graphs with d_bad set are skipped. Each
+// graph's level table is the TailOut at the start of its workspace.
+void coarsen_tail_batch(const TailArgs* d_args, const int32_t* d_order, const int32_t* d_bad, int ngraphs,
+                        cudaStream_t st);
+
 // The coarsening loop of coarsen/mod.rs:36-71 from level lvl0 (graph g) on,
 // in one single-block launch: per level the heavy list, match_parallel (same
 // seeds, rounds and progress checks) and contract, then the stop rule (cn < k
@@ -128,6 +148,44 @@ void coarsen_tail(const DGraph& g, int has_vw, int summed_unit, int mode, uint64
 // [ntrials] edge cut of each grown partition.
 void grow_trials(const DGraph& g, int k, int ntrials, const idx_t* seeds, const long long* grow_tgt,
                  idx_t* parts, long long* cuts, Arena& arena, cudaStream_t st);
+
+// One coarsest graph's grow trials in the batched launch.
+struct GrowJob {
+  const idx_t* xadj;
+  const idx_t* adjncy;
+  const idx_t* adjwgt;
+  const idx_t* vwgt;
+  int32_t n, ncon, k, trials;
+  const idx_t* seeds;         // [trials][k]
+  const long long* grow_tgt;  // [k][ncon]
+  idx_t* parts;               // [trials][n]
+  long long* cuts;            // [trials] directed edge cut of each trial
+  unsigned char* scratch;     // [trials][scratch_bytes] when use_smem is 0
+  long long scratch_bytes;
+  int32_t use_smem;
+  int32_t first_block;        // the job's trials are blocks first_block ..
+};
+
+// Bytes of one grow trial's state (shared memory or global scratch).
+size_t grow_scratch_bytes(int32_t n, int k, int ncon);
+
+// Every grow trial of a batch in one launch (block b: job d_block_job[b]);
+// dyn_smem covers the jobs with use_smem set.
+void grow_trials_batch(const GrowJob* d_jobs, const int32_t* d_block_job, int nblocks, size_t dyn_smem,
+                       cudaStream_t st);
+
+// ---- batch.cu ------------------------------------------------------------
+// One graph's validation in the batched launch (the checks of validate_device)
+// and the total weight per constraint (64-bit sums).
+struct ValJob {
+  const idx_t* xadj;
+  const idx_t* adjncy;
+  const idx_t* vwgt;
+  int32_t n, ncon;
+  int32_t* degcheck;  // [n], zero on entry
+  int32_t* flag;      // validate_device's bits, zero on entry
+  long long* total;   // [ncon]
+};
 
 // ---- refine.cu -----------------------------------------------------------
 struct RefineParams {
@@ -199,6 +257,76 @@ RefineStats fm2_refine(const DGraph& g, idx_t* part, const RefineParams& rp, Are
 void gain_table(const DGraph& g, const idx_t* part, int k, idx_t* boundary, idx_t* ncand,
                 idx_t* wfrom, idx_t* cand_p, idx_t* cand_g, const idx_t* heavy, int32_t nheavy,
                 cudaStream_t st);
+
+// One graph's level in a step of the batched refinement (k_batch_level and,
+// for an admission level, k_batch_admit). Scratch arrays are the graph's own,
+// sized for its finest level.
+struct LevelJob {
+  const idx_t* xadj;
+  const idx_t* adjncy;
+  const idx_t* adjwgt;
+  const idx_t* vwgt;
+  int32_t n, ncon, k, niter;
+  // start partition: the best grow trial (trial_parts set) or the projection
+  // part[v] = cpart[cmap[v]] of the coarser level's
+  const idx_t* trial_parts;
+  const long long* trial_cuts;
+  int32_t trials;
+  int32_t admit;  // 1: cut passes by parallel admission (k_batch_admit), 0: exact walk
+  const idx_t* cmap;
+  const idx_t* cpart;
+  idx_t* part;
+  const long long* feas;
+  const long long* over;
+  const idx_t* heavy;
+  int32_t nheavy;
+  int32_t pad;
+  long long* pw;
+  long long* in_max;
+  long long* out_max;
+  idx_t* mover;
+  idx_t* ncand;
+  idx_t* wfrom;
+  idx_t* cand_p;
+  idx_t* cand_g;
+  idx_t* movers;
+  int32_t* rec_pv;
+  int32_t* rec_ne;
+  int32_t* rec_wf;
+  int32_t* rec_coff;
+  int32_t* rec_known;
+  int32_t* rec_cp;
+  int32_t* rec_cg;
+  int32_t* rec_vw;
+  int32_t* rec_np;
+  int32_t* ghist;     // [32][k]
+  int32_t* counters;  // [2 * (niter + 1)]
+  int32_t* long_flag;
+  int32_t* a_tgt;
+  int32_t* a_src;
+  int32_t* a_w;
+  int32_t* a_rank;
+  int32_t* a_gsrc;
+  int32_t* a_cut;
+  long long* a_pref;
+  long long* a_out;   // [k][ncon], zero on entry
+  idx_t* touched[2];
+};
+
+// Inline candidate slots of a mover record (the walk's record layout).
+constexpr int kRecInline = 4;
+
+// A step of the batched refinement over njobs levels of one kind (edge
+// weights, 32-bit slacks, the k bucket of k, ncon 1 or 2): projection or
+// best trial, part weights, repair pass and, unless the job's admit is set,
+// the cut passes with the exact walk; one block (512 threads) per job.
+void batch_level_launch(const LevelJob* d_jobs, int njobs, bool has_w, bool small_weights, int k, int ncon,
+                        cudaStream_t st);
+
+// The cut passes of admission levels, one block (1024 threads) per job:
+// gain table (after the first pass only where the last pass moved), picks,
+// admission fixed point and moves, as admit_cut_pass does with grid kernels.
+void batch_admit_launch(const LevelJob* d_jobs, int njobs, bool has_w, cudaStream_t st);
 
 // ---- admit.cu -----------------------------------------------------------
 // Parallel admission of one greedy cut pass (src/refine/greedy.rs:126-190 in
