@@ -190,11 +190,11 @@ RMETIS_API int RMETIS_GPU_SetPoolTuning(int fused_max_n, int tail_max_n);
  * vtx_off[g]*ncon, its part at part[vtx_off[g]]. nparts[g] per graph; ncon,
  * ubvec and options are shared. The batch is uploaded once. With Greedy
  * refinement (options[METIS_OPTION_RTYPE] = 1), ncuts 1, a grown initial
- * partition, ncon <= 2 and nparts[g] <= 256, the graphs go through the
- * pipeline together: each step (validation, coarsening, grow trials, the
- * refinement of one level per graph, the cut) is one launch over the batch,
- * one thread block per graph; the other graphs are partitioned concurrently
- * on the device's worker pool. Either way each result equals the one of a
+ * partition, ncon <= 2 and nparts[g] <= 256, graphs of up to 131072
+ * vertices (RMETIS_GPU_SetBatchMode) go through the pipeline together: each
+ * step (validation, coarsening, grow trials, the refinement of one level per
+ * graph, the cut) is one launch over them, one thread block per graph; the
+ * other graphs are partitioned concurrently on the device's worker pool. Either way each result equals the one of a
  * separate RMETIS_PartGraphKway call. status[g] gets each graph's return code;
  * the call returns METIS_OK or the first failing code. */
 RMETIS_API int RMETIS_GPU_PartGraphKwayBatch(idx_t ngraphs, idx_t ncon, const int64_t *vtx_off,
@@ -203,11 +203,15 @@ RMETIS_API int RMETIS_GPU_PartGraphKwayBatch(idx_t ngraphs, idx_t ncon, const in
                                              const real_t *ubvec, const idx_t *options, idx_t *objval,
                                              idx_t *part, idx_t *status);
 
-/* 1 (default): eligible graphs of RMETIS_GPU_PartGraphKwayBatch run through
- * the batched launches; 0: every graph runs on the worker pool (no
- * counterpart in the reference; results are the same either way). Other
- * values return METIS_ERROR_INPUT. */
-RMETIS_API int RMETIS_GPU_SetBatchMode(int mode);
+/* How RMETIS_GPU_PartGraphKwayBatch runs its graphs (no counterpart in the
+ * reference; results are the same either way). mode 1 (default): eligible
+ * graphs with at most max_n vertices (default 131072) go through the batched
+ * launches, while the others run on the worker pool at the same time (a
+ * large graph's levels take one thread block each in the batched launches,
+ * so it finishes sooner on the pool's grid-wide kernels); mode 0: every graph
+ * on the worker pool. -1 leaves a value unchanged; other negative values, or
+ * a mode above 1, return METIS_ERROR_INPUT. */
+RMETIS_API int RMETIS_GPU_SetBatchMode(int mode, int max_n);
 
 /* Asynchronous requests for a serving loop (no counterpart in the reference).
  * Same arguments as RMETIS_PartGraphKway without vsize; returns a ticket > 0,

@@ -417,12 +417,15 @@ def set_pool_tuning(fused_max_n: int = -2, tail_max_n: int = -2):
     _raise_for(_lib.load().RMETIS_GPU_SetPoolTuning(fused_max_n, tail_max_n), "set_pool_tuning")
 
 
-def set_batch_mode(mode: int = 1):
-    """1 (default): eligible graphs of part_graph_kway_batch (Greedy, ncuts 1,
-    grown initial partitions, ncon <= 2, nparts <= 256) go through the
-    batched launches, one step of the pipeline for all graphs at a time; 0:
-    every graph runs on the worker pool. Results are the same either way."""
-    _raise_for(_lib.load().RMETIS_GPU_SetBatchMode(mode), "set_batch_mode")
+def set_batch_mode(mode: int = -1, max_n: int = -1):
+    """How part_graph_kway_batch runs its graphs. mode 1 (default): eligible
+    graphs (Greedy, ncuts 1, grown initial partitions, ncon <= 2,
+    nparts <= 256) of at most max_n vertices (default 131072) go through the
+    batched launches, one step of the pipeline for all of them at a time,
+    while the others run on the worker pool at the same time; mode 0: every
+    graph on the worker pool. -1 leaves a value unchanged. Results are the
+    same either way."""
+    _raise_for(_lib.load().RMETIS_GPU_SetBatchMode(mode, max_n), "set_batch_mode")
 
 
 def part_graph_kway_batch(graphs, nparts, ubvec=None, options: Options | None = None):

@@ -599,11 +599,33 @@ void Engine::partition_kway_batch(std::vector<BatchItem>& items, const float* ub
     nvtxRangePop();
     nvtxRangePushA("batch refine");
     const LevelJob* d_jobs = reinterpret_cast<const LevelJob*>(d_s3 + o_jobs);
-    for (const Group& gr : groups) {
+    const bool verbose = std::getenv("RMETIS_B200_VERBOSE") != nullptr;
+    std::vector<cudaEvent_t> ev;
+    if (verbose) {
+      ev.resize(groups.size() + 1);
+      for (auto& e : ev) RMB_CUDA(cudaEventCreate(&e));
+      RMB_CUDA(cudaEventRecord(ev[0], st));
+    }
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+      const Group& gr = groups[gi];
       if (gr.kind == 0)
         batch_level_launch(d_jobs + gr.first, (int)gr.count, gr.has_w, gr.small, gr.kmax, ncon, st);
       else
         batch_admit_launch(d_jobs + gr.first, (int)gr.count, gr.has_w, st);
+      if (verbose) RMB_CUDA(cudaEventRecord(ev[gi + 1], st));
+    }
+    if (verbose) {
+      RMB_CUDA(cudaEventSynchronize(ev.back()));
+      for (size_t gi = 0; gi < groups.size(); ++gi) {
+        float ms = 0.f;
+        RMB_CUDA(cudaEventElapsedTime(&ms, ev[gi], ev[gi + 1]));
+        const Group& gr = groups[gi];
+        int32_t nmax = 0;
+        for (size_t j = gr.first; j < gr.first + gr.count; ++j) nmax = std::max(nmax, jobs[j].n);
+        std::fprintf(stderr, "rmetis_b200: batch step %d %s: %zu levels (largest %d vertices), %.2f ms\n", gr.step,
+                     gr.kind == 0 ? "level" : "admission", gr.count, nmax, ms);
+      }
+      for (auto& e : ev) cudaEventDestroy(e);
     }
     nvtxRangePop();
     k_batch_cut<<<(int)cj.size(), 512, 0, st>>>(reinterpret_cast<const CutJob*>(d_s3 + o_cj));

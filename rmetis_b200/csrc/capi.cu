@@ -5,6 +5,7 @@
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -49,6 +50,12 @@ struct Tuning {
 // 1: batches run through the batched kernels (RMETIS_GPU_SetBatchMode).
 int& batch_mode() {
   static int m = 1;
+  return m;
+}
+// Graphs of a batch with more vertices than this run on the worker pool,
+// alongside the batched launches of the others.
+int& batch_max_n() {
+  static int m = 131072;
   return m;
 }
 Tuning& tuning() {
@@ -729,9 +736,10 @@ int RMETIS_GPU_SetKernelShapes(int contract_thread_max, int gain_block) {
   return METIS_OK;
 }
 
-int RMETIS_GPU_SetBatchMode(int mode) {
-  if (mode < 0 || mode > 1) return METIS_ERROR_INPUT;
-  batch_mode() = mode;
+int RMETIS_GPU_SetBatchMode(int mode, int max_n) {
+  if (mode < -1 || mode > 1 || max_n < -1) return METIS_ERROR_INPUT;
+  if (mode >= 0) batch_mode() = mode;
+  if (max_n >= 0) batch_max_n() = max_n;
   return METIS_OK;
 }
 
@@ -798,56 +806,28 @@ int RMETIS_GPU_PartGraphKwayBatch(idx_t ngraphs, idx_t ncon, const int64_t* vtx_
     idx_t* d_part = E.arena().alloc<idx_t>((size_t)ntot);
     std::vector<int> done(ngraphs, 0);
     std::vector<int32_t> objs(ngraphs, 0);
-    if (batch_mode() == 1) {
-      // Eligible graphs through the batched kernels (one launch per step for
-      // all of them); the rest, and any graph they could not finish, alone.
-      std::vector<BatchItem> items;
-      std::vector<idx_t> which;
+    // Graphs for the batched kernels: eligible and at most batch_max_n
+    // vertices (a large graph's levels take one block each there, so it runs
+    // faster on the pool's grid-wide kernels).
+    std::vector<char> batched(ngraphs, 0);
+    if (batch_mode() == 1)
       for (idx_t g = 0; g < ngraphs; ++g) {
-        const int64_t v0 = vtx_off[g], e0 = edge_off[g];
-        const int32_t n = (int32_t)(vtx_off[g + 1] - v0);
-        if (!batch_eligible(o, n, nparts[g], ncon)) continue;
-        BatchItem it;
-        it.g.n = n;
-        it.g.m = edge_off[g + 1] - e0;
-        it.g.ncon = ncon;
-        it.g.xadj = d_xadj + v0 + g;
-        it.g.adjncy = d_adj + e0;
-        it.g.adjwgt = d_adjwgt ? d_adjwgt + e0 : nullptr;
-        it.g.vwgt = d_vwgt ? d_vwgt + v0 * ncon : nullptr;
-        it.k = nparts[g];
-        it.part_out = d_part + v0;
-        items.push_back(it);
-        which.push_back(g);
+        const int32_t n = (int32_t)(vtx_off[g + 1] - vtx_off[g]);
+        batched[g] = batch_eligible(o, n, nparts[g], ncon) && n <= batch_max_n();
       }
-      if (!items.empty()) {
-        try {
-          E.partition_kway_batch(items, ubvec, o);
-        } catch (const Error& e) {
-          if (e.code != METIS_ERROR_MEMORY) throw;
-          for (BatchItem& it : items) it.status = 0;  // out of device memory: every graph alone
-        }
-        for (size_t i = 0; i < items.size(); ++i) {
-          if (items[i].status == 0) continue;
-          const idx_t g = which[i];
-          done[g] = 1;
-          status[g] = items[i].status;
-          objval[g] = items[i].objval;
-        }
-      }
-    }
-    RMB_CUDA(cudaStreamSynchronize(E.stream()));
+    RMB_CUDA(cudaStreamSynchronize(E.stream()));  // the upload is complete before other streams read it
     int dev = 0;
     RMB_CUDA(cudaGetDevice(&dev));
     WorkerPool& pool = pool_for_device(dev);
     std::vector<std::future<int>> fut(ngraphs);
-    for (idx_t g = 0; g < ngraphs; ++g) {
-      if (done[g]) continue;
+    std::vector<char> submitted(ngraphs, 0);
+    auto submit = [&](idx_t g) {
       const int64_t v0 = vtx_off[g], e0 = edge_off[g];
       const int32_t n = (int32_t)(vtx_off[g + 1] - v0);
       const int64_t m = edge_off[g + 1] - e0;
       const int32_t k = nparts[g];
       int32_t* obj_g = &objs[g];
+      submitted[g] = 1;
       fut[g] = pool.submit(footprint_bytes(n, m, std::max(k, 2), ncon), [=](Engine& W) {
         DGraph gr;
         gr.n = n;
@@ -861,6 +841,64 @@ int RMETIS_GPU_PartGraphKwayBatch(idx_t ngraphs, idx_t ncon, const int64_t* vtx_
         if (validate_device(gr, W.arena(), W.stream(), W.host_scratch()) != 0) return (int)METIS_ERROR_INPUT;
         return W.partition_kway(gr, k, nullptr, ubvec, o, d_part + v0, obj_g, nullptr);
       });
+    };
+    // The pool's graphs first, largest first: they run on the workers'
+    // streams while the batched launches run on this engine's stream.
+    {
+      std::vector<idx_t> rest;
+      for (idx_t g = 0; g < ngraphs; ++g)
+        if (!batched[g]) rest.push_back(g);
+      std::stable_sort(rest.begin(), rest.end(), [&](idx_t x, idx_t y) {
+        return edge_off[x + 1] - edge_off[x] > edge_off[y + 1] - edge_off[y];
+      });
+      for (idx_t g : rest) submit(g);
+    }
+    std::vector<BatchItem> items;
+    std::vector<idx_t> which;
+    for (idx_t g = 0; g < ngraphs; ++g) {
+      if (!batched[g]) continue;
+      const int64_t v0 = vtx_off[g], e0 = edge_off[g];
+      BatchItem it;
+      it.g.n = (int32_t)(vtx_off[g + 1] - v0);
+      it.g.m = edge_off[g + 1] - e0;
+      it.g.ncon = ncon;
+      it.g.xadj = d_xadj + v0 + g;
+      it.g.adjncy = d_adj + e0;
+      it.g.adjwgt = d_adjwgt ? d_adjwgt + e0 : nullptr;
+      it.g.vwgt = d_vwgt ? d_vwgt + v0 * ncon : nullptr;
+      it.k = nparts[g];
+      it.part_out = d_part + v0;
+      items.push_back(it);
+      which.push_back(g);
+    }
+    if (!items.empty()) {
+      std::exception_ptr err;
+      try {
+        E.partition_kway_batch(items, ubvec, o);
+      } catch (const Error& e) {
+        if (e.code == METIS_ERROR_MEMORY) {
+          for (BatchItem& it : items) it.status = 0;  // out of device memory: every graph alone
+        } else {
+          err = std::current_exception();
+        }
+      } catch (...) {
+        err = std::current_exception();
+      }
+      if (err) {  // the pool's jobs read this call's buffers: let them finish first
+        for (idx_t g = 0; g < ngraphs; ++g)
+          if (submitted[g]) fut[g].wait();
+        std::rethrow_exception(err);
+      }
+      for (size_t i = 0; i < items.size(); ++i) {
+        const idx_t g = which[i];
+        if (items[i].status == 0) {
+          submit(g);  // the batched kernels could not finish it: alone
+          continue;
+        }
+        done[g] = 1;
+        status[g] = items[i].status;
+        objval[g] = items[i].objval;
+      }
     }
     int rc = METIS_OK;
     for (idx_t g = 0; g < ngraphs; ++g) {

@@ -33,21 +33,25 @@ def graph_of(rmb, x, a, v=None, w=None, ncon=1):
 @pytest.fixture
 def batch_mode(rmb):
     yield
-    rmb.set_batch_mode(1)
+    rmb.set_batch_mode(1, 131072)
 
 
 def _check(rmb, graphs, ks, opts):
-    rmb.set_batch_mode(1)
+    """Batched launches for every eligible graph; every graph on the pool;
+    and graphs above 5,000 vertices on the pool while the batched launches
+    run the others."""
+    rmb.set_batch_mode(1, 1 << 30)
     batch = rmb.part_graph_kway_batch(graphs, ks, options=opts)
     rmb.set_batch_mode(0)
     pool = rmb.part_graph_kway_batch(graphs, ks, options=opts)
-    rmb.set_batch_mode(1)
-    for i, (g, k, r, q) in enumerate(zip(graphs, ks, batch, pool)):
+    rmb.set_batch_mode(1, 5000)
+    mixed = rmb.part_graph_kway_batch(graphs, ks, options=opts)
+    rmb.set_batch_mode(1, 131072)
+    for i, (g, k, r, q, x) in enumerate(zip(graphs, ks, batch, pool, mixed)):
         solo = rmb.part_graph_kway(g, k, options=opts)
-        assert r.objval == solo.objval, (i, k, r.objval, solo.objval)
-        np.testing.assert_array_equal(r.part, solo.part)
-        assert q.objval == solo.objval
-        np.testing.assert_array_equal(q.part, solo.part)
+        for res in (r, q, x):
+            assert res.objval == solo.objval, (i, k, res.objval, solo.objval)
+            np.testing.assert_array_equal(res.part, solo.part)
     return batch
 
 
