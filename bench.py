@@ -540,7 +540,7 @@ def run_rgg_batch(args):
     h_plain = torch.empty(int(vtx_off[-1]), dtype=torch.int32).pin_memory()
     same = True
     t0 = time.perf_counter()
-    for i in range(G_):
+    for i in range(0 if args.no_plain else G_):
         v0, e0 = int(vtx_off[i]), int(edge_off[i])
         nv.value = int(vtx_off[i + 1] - v0)
         npr.value = ks[i]
@@ -552,7 +552,7 @@ def run_rgg_batch(args):
             raise RuntimeError(f"RMETIS_PartGraphKway returned {rc}")
         same = same and obj.value == int(res_obj[i])
     pt = time.perf_counter() - t0
-    same = same and bool((h_plain.numpy() == res_part).all())
+    same = same and bool((h_plain.numpy() == res_part).all()) if not args.no_plain else None
     b = float(np.mean(bt))
     line = {
         "metric": "k-way graphs/s (batched uneven graphs)", "value": args.graphs / b, "unit": "graphs/s",
@@ -566,8 +566,8 @@ def run_rgg_batch(args):
                              "host buffers (one upload, all graphs, results back on the host)",
                    "l2": "inputs larger than L2"},
         "edges_per_s": m_tot / b,
-        "plain_gpu": {"s": pt, "graphs_per_s": args.graphs / pt, "same_result": same},
-        "speedup_vs_plain_gpu": pt / b,
+        "plain_gpu": None if args.no_plain else {"s": pt, "graphs_per_s": args.graphs / pt, "same_result": same},
+        "speedup_vs_plain_gpu": None if args.no_plain else pt / b,
         "e2e": {"value": args.graphs / b, "unit": "graphs/s", "ms_per_step": b * 1e3,
                 "h2d_bytes_per_step": int(4 * (sum(len(s[0]) + len(s[1]) + len(s[2]) + len(s[3]) for s in specs))),
                 "d2h_bytes_per_step": int(4 * n_tot + 8 * args.graphs)},
@@ -723,6 +723,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="rgg_batch: skip the one-graph-at-a-time leg (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     RTYPE.update(code=0 if args.rtype == "fm" else 1, name=args.rtype)
