@@ -203,6 +203,13 @@ RMETIS_API int RMETIS_GPU_PartGraphKwayBatch(idx_t ngraphs, idx_t ncon, const in
                                              const real_t *ubvec, const idx_t *options, idx_t *objval,
                                              idx_t *part, idx_t *status);
 
+/* FM levels (rtype Fm) of at most max_n vertices (default 4096) run all their
+ * passes and rounds in one single-block launch instead of about ten launches
+ * per round (no counterpart in the reference); 0 = never, -1 leaves it
+ * unchanged, other negative values return METIS_ERROR_INPUT. Never changes a
+ * result. */
+RMETIS_API int RMETIS_GPU_SetFmFusedMax(int max_n);
+
 /* How RMETIS_GPU_PartGraphKwayBatch runs its graphs (no counterpart in the
  * reference; results are the same either way). mode 1 (default): eligible
  * graphs with at most max_n vertices (default 131072) go through the batched

@@ -417,6 +417,12 @@ def set_pool_tuning(fused_max_n: int = -2, tail_max_n: int = -2):
     _raise_for(_lib.load().RMETIS_GPU_SetPoolTuning(fused_max_n, tail_max_n), "set_pool_tuning")
 
 
+def set_fm_fused_max(max_n: int = -1):
+    """FM levels of at most max_n vertices (default 4096) run all their passes
+    and rounds in one single-block launch; 0 = never. Never changes a result."""
+    _raise_for(_lib.load().RMETIS_GPU_SetFmFusedMax(max_n), "set_fm_fused_max")
+
+
 def set_batch_mode(mode: int = -1, max_n: int = -1):
     """How part_graph_kway_batch runs its graphs. mode 1 (default): eligible
     graphs (Greedy, ncuts 1, grown initial partitions, ncon <= 2,

@@ -46,6 +46,7 @@ struct Tuning {
   int exact_max_n = 16384;
   int contract_thread_max = 32;
   int gain_block = 256;
+  int fm_fused_max_n = 4096;
 };
 // 1: batches run through the batched kernels (RMETIS_GPU_SetBatchMode).
 int& batch_mode() {
@@ -73,6 +74,7 @@ void apply_tuning(KwayOptions& o) {
   o.exact_max_n = tuning().exact_max_n;
   o.contract_thread_max = tuning().contract_thread_max;
   o.gain_block = tuning().gain_block;
+  o.fm_fused_max_n = tuning().fm_fused_max_n;
 }
 
 // Launch-shape knobs of jobs that share the device with other jobs (batch
@@ -736,6 +738,12 @@ int RMETIS_GPU_SetKernelShapes(int contract_thread_max, int gain_block) {
   return METIS_OK;
 }
 
+int RMETIS_GPU_SetFmFusedMax(int max_n) {
+  if (max_n < -1) return METIS_ERROR_INPUT;
+  if (max_n >= 0) tuning().fm_fused_max_n = max_n;
+  return METIS_OK;
+}
+
 int RMETIS_GPU_SetBatchMode(int mode, int max_n) {
   if (mode < -1 || mode > 1 || max_n < -1) return METIS_ERROR_INPUT;
   if (mode >= 0) batch_mode() = mode;
@@ -1218,6 +1226,7 @@ static int refine_entry(int fm, idx_t n, idx_t ncon, const idx_t* xadj, const id
     rp.over_thr = d_over;
     rp.collect_stats = stats != nullptr;
     rp.fused_max_n = tuning().fused_max_n;
+    rp.fm_fused_max_n = tuning().fm_fused_max_n;
     rp.exact_max_n = tuning().exact_max_n;
     rp.gain_block = tuning().gain_block;
     {

@@ -201,6 +201,10 @@ struct RefineParams {
   // entries (and k <= 256, ncon <= 2) run all their passes in one
   // single-block launch (k_refine_level); 0 = never.
   int32_t fused_max_n = 0;
+  // FM levels with at most this many vertices (k <= 256, ncon <= 2, exact
+  // walk) run all their passes and rounds in one single-block launch
+  // (k_fm_level); 0 = never.
+  int32_t fm_fused_max_n = 0;
   // Cut passes of levels with more vertices than this decide by parallel
   // admission (admit.cu) instead of the exact sequential walk.
   int32_t exact_max_n = INT32_MAX;

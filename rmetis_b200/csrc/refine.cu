@@ -1589,12 +1589,12 @@ __device__ __forceinline__ int32_t fm_gain_of(int32_t v, const idx_t* __restrict
 // active (rounds after the first of a pass): only vertices within two hops
 // of the last round's changes can change their selection; the others were
 // not selected then and are not now.
-__global__ void k_fm_select(int32_t n, const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
-                            const idx_t* __restrict__ part, const idx_t* __restrict__ mover,
-                            const idx_t* __restrict__ ncand, const idx_t* __restrict__ cand_g,
-                            const int32_t* __restrict__ state, const idx_t* __restrict__ active,
-                            idx_t* __restrict__ sel) {
-  RMB_GRID_STRIDE(v, n) {
+__device__ void fm_select_body(Lanes L, int32_t n, const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                               const idx_t* __restrict__ part, const idx_t* __restrict__ mover,
+                               const idx_t* __restrict__ ncand, const idx_t* __restrict__ cand_g,
+                               const int32_t* __restrict__ state, const idx_t* __restrict__ active,
+                               idx_t* __restrict__ sel) {
+  RMB_FOR(v, n, L) {
     if (active && !active[v]) {
       sel[v] = 0;
       continue;
@@ -1619,6 +1619,14 @@ __global__ void k_fm_select(int32_t n, const idx_t* __restrict__ xadj, const idx
   }
 }
 
+__global__ void k_fm_select(int32_t n, const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                            const idx_t* __restrict__ part, const idx_t* __restrict__ mover,
+                            const idx_t* __restrict__ ncand, const idx_t* __restrict__ cand_g,
+                            const int32_t* __restrict__ state, const idx_t* __restrict__ active,
+                            idx_t* __restrict__ sel) {
+  fm_select_body(grid_lanes(), n, xadj, adj, part, mover, ncand, cand_g, state, active, sel);
+}
+
 // After the walk: a selected vertex that took its move is locked and frees
 // its dropped neighbours that were not selected this round (the reference
 // re-queues the unlocked neighbours of a moved vertex); a selected vertex
@@ -1627,13 +1635,13 @@ __global__ void k_fm_select(int32_t n, const idx_t* __restrict__ xadj, const idx
 // changed (for the next round; zero on entry): every vertex whose best move
 // may differ now (a moved vertex and its neighbours) or whose state changed
 // (a dropped one).
-__global__ void k_fm_after(const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
-                           const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
-                           const idx_t* __restrict__ part, const idx_t* __restrict__ cand_p,
-                           const idx_t* __restrict__ sel, int32_t* __restrict__ state,
-                           idx_t* __restrict__ changed) {
+__device__ void fm_after_body(Lanes L, const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
+                              const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                              const idx_t* __restrict__ part, const idx_t* __restrict__ cand_p,
+                              const idx_t* __restrict__ sel, int32_t* __restrict__ state,
+                              idx_t* __restrict__ changed) {
   const int32_t nm = *nm_dev;
-  RMB_GRID_STRIDE(i, nm) {
+  RMB_FOR(i, nm, L) {
     const int32_t v = movers[i];
     const int32_t s = xadj[v], e = xadj[v + 1];
     changed[v] = 1;
@@ -1648,6 +1656,14 @@ __global__ void k_fm_after(const int32_t* __restrict__ nm_dev, const idx_t* __re
       state[v] = kFmDropped;
     }
   }
+}
+
+__global__ void k_fm_after(const int32_t* __restrict__ nm_dev, const idx_t* __restrict__ movers,
+                           const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                           const idx_t* __restrict__ part, const idx_t* __restrict__ cand_p,
+                           const idx_t* __restrict__ sel, int32_t* __restrict__ state,
+                           idx_t* __restrict__ changed) {
+  fm_after_body(grid_lanes(), nm_dev, movers, xadj, adj, part, cand_p, sel, state, changed);
 }
 
 // k_fm_after for a round decided by admission, with the moves applied here:
@@ -1679,15 +1695,136 @@ __global__ void k_fm_apply_after(const int32_t* __restrict__ nm_dev, const idx_t
 
 // active_next = changed and their neighbours (zero on entry). Also clears the
 // flags the round just used (changed_cur, active_cur) for the round after next.
-__global__ void k_fm_spread(int32_t n, const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
-                            const idx_t* __restrict__ changed, idx_t* __restrict__ active_next,
-                            idx_t* __restrict__ changed_cur, idx_t* __restrict__ active_cur) {
-  RMB_GRID_STRIDE(v, n) {
+__device__ void fm_spread_body(Lanes L, int32_t n, const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                               const idx_t* __restrict__ changed, idx_t* __restrict__ active_next,
+                               idx_t* __restrict__ changed_cur, idx_t* __restrict__ active_cur) {
+  RMB_FOR(v, n, L) {
     changed_cur[v] = 0;
     active_cur[v] = 0;
     if (!changed[v]) continue;
     active_next[v] = 1;
     for (int32_t j = xadj[v]; j < xadj[v + 1]; ++j) active_next[adj[j]] = 1;
+  }
+}
+
+__global__ void k_fm_spread(int32_t n, const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                            const idx_t* __restrict__ changed, idx_t* __restrict__ active_next,
+                            idx_t* __restrict__ changed_cur, idx_t* __restrict__ active_cur) {
+  fm_spread_body(grid_lanes(), n, xadj, adj, changed, active_next, changed_cur, active_cur);
+}
+
+// A whole FM level in one block (levels of at most fused_max_n vertices): the
+// passes and rounds of fm_refine below, with the same bodies and decisions,
+// the host loop replaced by the block's own loop. Per pass it writes the
+// number of rounds that selected movers, the movers and the moves to
+// pass_stats[3 * pass ..].
+struct FmLevel {
+  LevelRefine P;        // gain tables, walk records and part weights
+  idx_t* sel;
+  idx_t* zero;
+  int32_t* state;
+  idx_t* flags[2][2];   // per round parity: [0] changed, [1] active
+  int32_t* rcount;      // [2 * kFmMaxRounds]: selected movers and moves per round
+  long long* pass_stats;  // [niter][3]
+};
+
+template <bool HAS_W, typename S, int R, int NC>
+__global__ void __launch_bounds__(kFusedThreads) k_fm_level(FmLevel F) {
+  __shared__ WalkShared<S, R, NC> sh;
+  __shared__ int32_t sw[32];
+  extern __shared__ __align__(16) int32_t wdyn[];  // kPoolBytes
+  const LevelRefine& P = F.P;
+  const Lanes L = block_lanes();
+  const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int32_t K = P.k * NC;
+  for (int32_t x = threadIdx.x; x < K; x += blockDim.x) {
+    P.pw[x] = 0;
+    P.in_max[x] = 0;
+    P.out_max[x] = 0;
+  }
+  if (threadIdx.x == 0) *P.long_flag = 0;
+  RMB_FOR(v, P.n, L) F.zero[v] = 0;
+  __syncthreads();
+  RMB_FOR(v, P.n, L) {
+    const int32_t p = P.part[v];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) atomic_add_i64(&P.pw[p * NC + c], P.vwgt ? P.vwgt[v * NC + c] : 1);
+  }
+  __syncthreads();
+  const WalkOut wo{P.movers, P.part, P.in_max, P.out_max, P.k * NC};
+  for (int pass = 0; pass < P.niter; ++pass) {  // fm_kway.rs:23-27
+    RMB_FOR(v, P.n, L) {
+      F.state[v] = kFmFree;
+      F.flags[0][0][v] = 0;
+      F.flags[0][1][v] = 0;
+      F.flags[1][0][v] = 0;
+      F.flags[1][1][v] = 0;
+    }
+    __syncthreads();
+    long long moves = 0, movers = 0, rounds_used = 0;
+    for (int r = 0; r < kFmMaxRounds; ++r) {
+      idx_t* const* cur = F.flags[r & 1];
+      idx_t* const* nxt = F.flags[(r + 1) & 1];
+      int32_t* nm_dev = F.rcount + 2 * r;
+      const idx_t* only = r > 0 ? cur[0] : nullptr;
+      gain_body<HAS_W, kCut>(L, P.xadj, P.adj, P.adjwgt, P.n, NC, P.part, P.k, nullptr, nullptr, P.mover, P.ncand,
+                             P.wfrom, P.cand_p, P.cand_g, only, false);
+      if (P.nheavy > 0)
+        gain_heavy_body<HAS_W, kCut>(warp, nwarps, P.ghist + (int64_t)warp * P.k, P.xadj, P.adj, P.adjwgt, P.heavy,
+                                     P.nheavy, NC, P.part, P.k, nullptr, nullptr, P.mover, P.ncand, P.wfrom,
+                                     P.cand_p, P.cand_g, only, false);
+      __syncthreads();
+      fm_select_body(L, P.n, P.xadj, P.adj, P.part, P.mover, P.ncand, P.cand_g, F.state, r > 0 ? cur[1] : nullptr,
+                     F.sel);
+      __syncthreads();
+      block_scan_n<int32_t>(LoadNonZero{F.sel}, StoreCompact{F.sel, P.movers}, P.n, nm_dev, sw);
+      __syncthreads();
+      const int32_t nm = *nm_dev;
+      if (nm == 0) break;  // nothing selected: the pass is over
+      // The selected moves through the walk, one candidate each (sel is the
+      // candidate count, w_from 0), as launch_walk<kCut> decides them.
+      prep_body<kCut>(L, nm_dev, P.movers, P.part, P.vwgt, NC, P.xadj, F.sel, F.zero, P.cand_p, P.cand_g, P.r,
+                      P.in_max, P.out_max, P.long_flag);
+      __syncthreads();
+      classify_body(L, nm_dev, NC, P.cand_p, P.cand_g, P.r, P.pw, P.feas, P.in_max, P.out_max, P.long_flag);
+      __syncthreads();
+      walk_reg_body<kCut, S, R, NC>(sh, nm_dev, P.r, P.k, P.cand_p, P.cand_g, P.pw, P.feas, P.over, wo, nm_dev + 1,
+                                    P.long_flag, wdyn);
+      __syncthreads();
+      fm_after_body(L, nm_dev, P.movers, P.xadj, P.adj, P.part, P.cand_p, F.sel, F.state, nxt[0]);
+      __syncthreads();
+      fm_spread_body(L, P.n, P.xadj, P.adj, nxt[0], nxt[1], cur[0], cur[1]);
+      __syncthreads();
+      moves += nm_dev[1];
+      movers += nm;
+      rounds_used += 1;
+    }
+    if (threadIdx.x == 0) {
+      F.pass_stats[3 * pass] = rounds_used;
+      F.pass_stats[3 * pass + 1] = movers;
+      F.pass_stats[3 * pass + 2] = moves;
+    }
+    __syncthreads();
+    if (moves == 0) break;  // fm_kway_pass returned false
+  }
+}
+
+template <bool HAS_W, typename S, int NC>
+static void launch_fm_level_r(const FmLevel& F, cudaStream_t st) {
+  const int k = F.P.k;
+  auto kern = k <= 32 ? k_fm_level<HAS_W, S, 1, NC>
+              : k <= 64 ? k_fm_level<HAS_W, S, 2, NC>
+              : k <= 128 ? k_fm_level<HAS_W, S, 4, NC> : k_fm_level<HAS_W, S, 8, NC>;
+  allow_dyn_smem((const void*)kern, kPoolBytes);
+  kern<<<1, kFusedThreads, kPoolBytes, st>>>(F);
+}
+
+template <bool HAS_W>
+static void launch_fm_level(const FmLevel& F, int ncon, bool small_weights, cudaStream_t st) {
+  if (small_weights) {
+    if (ncon == 1) launch_fm_level_r<HAS_W, int32_t, 1>(F, st); else launch_fm_level_r<HAS_W, int32_t, 2>(F, st);
+  } else {
+    if (ncon == 1) launch_fm_level_r<HAS_W, long long, 1>(F, st); else launch_fm_level_r<HAS_W, long long, 2>(F, st);
   }
 }
 
@@ -1746,6 +1883,66 @@ RefineStats fm_refine(const DGraph& g, idx_t* part, const RefineParams& rp, cons
     as.out = arena.alloc<long long>((size_t)K);
     as.cut = arena.alloc<int32_t>((size_t)k);
     RMB_CUDA(cudaMemsetAsync(as.out, 0, sizeof(long long) * (size_t)K, st));
+  }
+  // A small level runs all its passes and rounds in one single-block launch.
+  // (A round of the multi-kernel form costs about ten launches whatever the
+  // level's size, and a round's work is mostly the vertices next to its
+  // moves, so dense levels qualify too.)
+  const bool fused = rp.fm_fused_max_n > 0 && g.n <= rp.fm_fused_max_n && k <= 256 && g.ncon <= 2 && !admit;
+  if (fused) {
+    FmLevel F;
+    F.P.xadj = g.xadj;
+    F.P.adj = g.adjncy;
+    F.P.adjwgt = g.adjwgt;
+    F.P.vwgt = g.vwgt;
+    F.P.n = g.n;
+    F.P.k = k;
+    F.P.niter = rp.niter;
+    F.P.part = part;
+    F.P.pw = pw;
+    F.P.in_max = in_max;
+    F.P.out_max = out_max;
+    F.P.feas = rp.feas_max;
+    F.P.over = rp.over_thr;
+    F.P.mover = mover;
+    F.P.ncand = ncand;
+    F.P.wfrom = wfrom;
+    F.P.cand_p = cand_p;
+    F.P.cand_g = cand_g;
+    F.P.movers = movers;
+    F.P.r = r;
+    F.P.heavy = heavy;
+    F.P.nheavy = nheavy;
+    F.P.ghist = nheavy > 0 ? arena.alloc<int32_t>((size_t)k * (kFusedThreads / 32)) : nullptr;
+    F.P.counters = nullptr;
+    F.P.long_flag = long_flag;
+    F.sel = sel;
+    F.zero = zero;
+    F.state = state;
+    for (int b = 0; b < 2; ++b)
+      for (int f = 0; f < 2; ++f) F.flags[b][f] = flags[b][f];
+    F.rcount = counters;
+    F.pass_stats = arena.alloc<long long>(3 * (size_t)std::max(rp.niter, 1));
+    RMB_CUDA(cudaMemsetAsync(F.pass_stats, 0, sizeof(long long) * 3 * (size_t)std::max(rp.niter, 1), st));
+    const int ph = profiler().begin(kProfLevel, st);
+    if (g.adjwgt) launch_fm_level<true>(F, g.ncon, rp.small_weights, st);
+    else launch_fm_level<false>(F, g.ncon, rp.small_weights, st);
+    RMB_LAUNCH_CHECK();
+    profiler().end(ph, st, 0.0);
+    if (rp.collect_stats) {
+      std::vector<long long> ps(3 * (size_t)std::max(rp.niter, 1));
+      RMB_CUDA(cudaMemcpyAsync(ps.data(), F.pass_stats, sizeof(long long) * ps.size(), cudaMemcpyDeviceToHost, st));
+      RMB_CUDA(cudaStreamSynchronize(st));
+      for (int pass = 0; pass < rp.niter; ++pass) {
+        stats.passes += 1;
+        stats.decide_iters += (int)ps[3 * pass];
+        stats.movers += ps[3 * pass + 1];
+        stats.moves += ps[3 * pass + 2];
+        if (ps[3 * pass + 2] == 0) break;
+      }
+    }
+    arena.reset_to(mk);
+    return stats;
   }
   RMB_CUDA(cudaMemsetAsync(long_flag, 0, sizeof(int32_t), st));
   RMB_CUDA(cudaMemsetAsync(in_max, 0, sizeof(long long) * (size_t)K, st));

@@ -80,3 +80,48 @@ def test_full_partitions_identical_across_paths(rmb):
             rmb.set_tuning(fused_max_n=4096)
         assert multi.objval == fused.objval
         np.testing.assert_array_equal(multi.part, fused.part)
+
+
+@pytest.mark.parametrize("name", list(GRAPHS))
+@pytest.mark.parametrize("k", [2, 9, 48])
+def test_fm_level_paths_identical(rmb, name, k):
+    """The single-block FM level (k_fm_level: every pass and round of
+    fm_kway_refine in one launch) and the multi-kernel rounds decide every
+    round identically: same partition, cut and statistics."""
+    from rmetis_b200 import functions as F
+    x, a, v, w = load(name)
+    n = len(x) - 1
+    rng = np.random.default_rng(500 + k)
+    part = ((np.arange(n) * k) // n).astype(np.int32)
+    flip = rng.random(n) < 0.15
+    part[flip] = rng.integers(0, k, flip.sum())
+    g = rmb.Graph(n, 1, x, a, vwgt=v, adjwgt=w)
+    tot = n if v is None else int(np.asarray(v).sum())
+    t = np.full(k, tot / k, np.float64)
+    out = {}
+    try:
+        for path, fm in (("multi", 0), ("fused", 1 << 30)):
+            rmb.set_fm_fused_max(fm)
+            out[path] = F.fm_refine(g, part, k, t, [1.03], 10)
+    finally:
+        rmb.set_fm_fused_max(4096)
+    assert out["multi"][1] == out["fused"][1]
+    np.testing.assert_array_equal(out["multi"][0], out["fused"][0])
+    np.testing.assert_array_equal(out["multi"][2], out["fused"][2])
+
+
+def test_fm_full_partitions_identical_across_paths(rmb):
+    cases = [(G.grid3d(24, weights_seed=7), 32), (G.grid2d(90, 90) + (None, None), 16),
+             (G.random_graph(6000, 8.0, seed=9), 24)]
+    for (x, a, v, w), k in cases:
+        g = rmb.Graph(len(x) - 1, 1, x, a, vwgt=v, adjwgt=w)
+        o = rmb.Options(rtype=rmb.RType.Fm, seed=4)
+        try:
+            rmb.set_fm_fused_max(0)
+            multi = rmb.part_graph_kway(g, k, options=o)
+            rmb.set_fm_fused_max(1 << 30)
+            fused = rmb.part_graph_kway(g, k, options=o)
+        finally:
+            rmb.set_fm_fused_max(4096)
+        assert multi.objval == fused.objval
+        np.testing.assert_array_equal(multi.part, fused.part)
