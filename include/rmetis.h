@@ -203,6 +203,20 @@ RMETIS_API int RMETIS_GPU_PartGraphKwayBatch(idx_t ngraphs, idx_t ncon, const in
                                              const real_t *ubvec, const idx_t *options, idx_t *objval,
                                              idx_t *part, idx_t *status);
 
+/* 1 (default): the matching rounds of a coarsening level run in one
+ * cooperative launch, with grid-wide barriers between their phases and the
+ * progress checks on the device; 0: one launch per phase and a host check
+ * every other round (no counterpart in the reference). The same matching
+ * either way; other values return METIS_ERROR_INPUT. */
+RMETIS_API int RMETIS_GPU_SetCoopMatching(int on);
+
+/* The edge bound of the single-block levels of RMETIS_GPU_SetTuning's
+ * fused_max_n: a level runs all its passes in one launch when it has at most
+ * fused_max_n vertices and factor * fused_max_n adjacency entries (default
+ * factor 4; no counterpart in the reference). Never changes a result; -1
+ * leaves it unchanged, 0 or other negative values return METIS_ERROR_INPUT. */
+RMETIS_API int RMETIS_GPU_SetFusedEdgeFactor(int factor);
+
 /* FM levels (rtype Fm) of at most max_n vertices (default 4096) run all their
  * passes and rounds in one single-block launch instead of about ten launches
  * per round (no counterpart in the reference); 0 = never, -1 leaves it

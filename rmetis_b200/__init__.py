@@ -417,6 +417,18 @@ def set_pool_tuning(fused_max_n: int = -2, tail_max_n: int = -2):
     _raise_for(_lib.load().RMETIS_GPU_SetPoolTuning(fused_max_n, tail_max_n), "set_pool_tuning")
 
 
+def set_coop_matching(on: int = 1):
+    """1 (default): a level's matching rounds run in one cooperative launch;
+    0: one launch per phase. The same matching either way."""
+    _raise_for(_lib.load().RMETIS_GPU_SetCoopMatching(on), "set_coop_matching")
+
+
+def set_fused_edge_factor(factor: int = -1):
+    """Edge bound of the single-block levels: at most factor * fused_max_n
+    adjacency entries (default 4). Never changes a result."""
+    _raise_for(_lib.load().RMETIS_GPU_SetFusedEdgeFactor(factor), "set_fused_edge_factor")
+
+
 def set_fm_fused_max(max_n: int = -1):
     """FM levels of at most max_n vertices (default 4096) run all their passes
     and rounds in one single-block launch; 0 = never. Never changes a result."""

@@ -48,6 +48,8 @@ SIGNATURES = {
     "RMETIS_GPU_EdgeCutWeightsNoAlloc": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, VP, VP, VP, VP, VP,
                                          ctypes.c_int32, VP, VP, VP],
     "RMETIS_GPU_SetFmFusedMax": [ctypes.c_int32],
+    "RMETIS_GPU_SetFusedEdgeFactor": [ctypes.c_int32],
+    "RMETIS_GPU_SetCoopMatching": [ctypes.c_int32],
     "RMETIS_GPU_SetBatchMode": [ctypes.c_int32, ctypes.c_int32],
     "RMETIS_GPU_PartGraphKwayBatch": [ctypes.c_int32, ctypes.c_int32, I64P, I64P, I32P, I32P, I32P, I32P, I32P,
                                       F32P, I32P, I32P, I32P, I32P],

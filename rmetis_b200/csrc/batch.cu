@@ -348,7 +348,8 @@ void Engine::partition_kway_batch(std::vector<BatchItem>& items, const float* ub
         }
       P.small.push_back(weights_fit_int32(tot.data(), ncon, h, h + K, K));
       const DGraph& lg = P.levels[l];
-      const bool fused = o.fused_max_n > 0 && lg.n <= o.fused_max_n && lg.m <= 4LL * o.fused_max_n;
+      const bool fused = o.fused_max_n > 0 && lg.n <= o.fused_max_n &&
+                         lg.m <= (int64_t)o.fused_edge_factor * o.fused_max_n;
       P.admit.push_back(!fused && lg.n > o.exact_max_n && admit_supported(k, ncon));
     }
     o_thr[b] = s2.put(thr.data(), thr.size());

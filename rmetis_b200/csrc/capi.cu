@@ -47,6 +47,7 @@ struct Tuning {
   int contract_thread_max = 32;
   int gain_block = 256;
   int fm_fused_max_n = 4096;
+  int fused_edge_factor = 4;
 };
 // 1: batches run through the batched kernels (RMETIS_GPU_SetBatchMode).
 int& batch_mode() {
@@ -75,6 +76,7 @@ void apply_tuning(KwayOptions& o) {
   o.contract_thread_max = tuning().contract_thread_max;
   o.gain_block = tuning().gain_block;
   o.fm_fused_max_n = tuning().fm_fused_max_n;
+  o.fused_edge_factor = tuning().fused_edge_factor;
 }
 
 // Launch-shape knobs of jobs that share the device with other jobs (batch
@@ -738,6 +740,18 @@ int RMETIS_GPU_SetKernelShapes(int contract_thread_max, int gain_block) {
   return METIS_OK;
 }
 
+int RMETIS_GPU_SetCoopMatching(int on) {
+  if (on < 0 || on > 1) return METIS_ERROR_INPUT;
+  coop_matching() = on;
+  return METIS_OK;
+}
+
+int RMETIS_GPU_SetFusedEdgeFactor(int factor) {
+  if (factor < -1 || factor == 0) return METIS_ERROR_INPUT;
+  if (factor > 0) tuning().fused_edge_factor = factor;
+  return METIS_OK;
+}
+
 int RMETIS_GPU_SetFmFusedMax(int max_n) {
   if (max_n < -1) return METIS_ERROR_INPUT;
   if (max_n >= 0) tuning().fm_fused_max_n = max_n;
@@ -1227,6 +1241,7 @@ static int refine_entry(int fm, idx_t n, idx_t ncon, const idx_t* xadj, const id
     rp.collect_stats = stats != nullptr;
     rp.fused_max_n = tuning().fused_max_n;
     rp.fm_fused_max_n = tuning().fm_fused_max_n;
+    rp.fused_edge_factor = tuning().fused_edge_factor;
     rp.exact_max_n = tuning().exact_max_n;
     rp.gain_block = tuning().gain_block;
     {

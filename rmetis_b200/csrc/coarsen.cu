@@ -1,9 +1,13 @@
 // Coarsening: parallel matching (locally dominant edges) and contraction.
+#include <cooperative_groups.h>
+
 #include "kernels.h"
 #include "prof.h"
 #include "scan.cuh"
 
 namespace rmb {
+
+namespace cg = cooperative_groups;
 
 // ---------------------------------------------------------------------------
 // Matching
@@ -208,6 +212,90 @@ __global__ void k_match_finalize(int32_t n, idx_t* match) {
   }
 }
 
+// 1 (default): match_parallel runs its rounds in one cooperative launch.
+int& coop_matching() {
+  static int on = 1;
+  return on;
+}
+
+// Every round of match_parallel in one cooperative launch: the phases of a
+// round are separated by grid-wide barriers instead of launches, and the
+// progress checks of the host loop below (every other round, the pairs the
+// last two rounds matched) are made by every thread from the same counters,
+// so the rounds, phases and result are the host loop's. The grid is at most
+// the blocks that fit on the device at once (the launch fails otherwise).
+struct MatchCoop {
+  const idx_t* xadj;
+  const idx_t* adj;
+  const idx_t* adjwgt;
+  const idx_t* heavy;
+  int32_t n, nheavy, mode, rounds;
+  idx_t* match;
+  idx_t* prop;
+  int32_t* stamp;
+  unsigned long long* best;
+  int32_t* newly;  // [rounds + 1], zero on entry
+  uint64_t seed, vseed;
+};
+
+template <bool HAS_W>
+__global__ void __launch_bounds__(256) k_match_coop(MatchCoop a) {
+  cg::grid_group grid = cg::this_grid();
+  const Lanes L = grid_lanes(), W = grid_warps();
+  RMB_FOR(v, a.n, L) a.match[v] = -1;
+  grid.sync();
+  bool handshake = true;
+  int phase_start = 0;
+  for (int r = 0; r < a.rounds; ++r) {
+    if (handshake && a.mode == 1) {
+      propose_body<HAS_W, 1>(a.xadj, a.adj, a.adjwgt, a.n, a.match, a.prop, a.seed, L);
+      propose_heavy_body<HAS_W, 1>(a.xadj, a.adj, a.adjwgt, a.heavy, a.nheavy, a.match, a.prop, a.seed, W);
+    } else {
+      propose_body<false, 0>(a.xadj, a.adj, a.adjwgt, a.n, a.match, a.prop, a.seed, L);
+      propose_heavy_body<false, 0>(a.xadj, a.adj, a.adjwgt, a.heavy, a.nheavy, a.match, a.prop, a.seed, W);
+    }
+    grid.sync();
+    if (handshake) {
+      stamp_body(a.n, a.match, a.prop, a.stamp, r, L);
+      grid.sync();
+      compete_body(a.xadj, a.n, a.match, a.prop, a.stamp, r, a.best, a.vseed, a.mode == 1 ? 1 : 0, L);
+      grid.sync();
+      resolve_body(a.n, a.prop, a.match, a.best, a.newly + r, L);
+    } else {
+      accept_body(a.n, a.prop, a.match, a.newly + r, L);
+    }
+    grid.sync();
+    if (r - phase_start >= 1 && ((r - phase_start) & 1) == 1) {
+      const int64_t last2 = (int64_t)__ldcg(a.newly + r - 1) + __ldcg(a.newly + r);
+      if (last2 * 1000 < (int64_t)a.n) {
+        if (!handshake) break;  // the same decision in every thread
+        handshake = false;
+        phase_start = r + 1;
+      }
+    }
+  }
+  RMB_FOR(v, a.n, L) {
+    if (a.match[v] < 0) a.match[v] = (idx_t)v;
+  }
+}
+
+// Blocks of k_match_coop<HAS_W> that fit on the current device at once.
+template <bool HAS_W>
+static int coop_blocks() {
+  static int blocks[64] = {0};
+  int dev = 0;
+  RMB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return 0;
+  if (blocks[dev] == 0) {
+    int per_sm = 0, sms = 0, coop = 0;
+    RMB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    RMB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    RMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_match_coop<HAS_W>, 256, 0));
+    blocks[dev] = coop ? std::max(per_sm * sms, -1) : -1;
+  }
+  return blocks[dev];
+}
+
 void match_parallel(const DGraph& g, int mode, uint64_t seed, int rounds, idx_t* match, const idx_t* heavy,
                     int32_t nheavy, Arena& arena, cudaStream_t st, int32_t* h_scratch) {
   Arena::Mark mk = arena.mark();
@@ -219,10 +307,43 @@ void match_parallel(const DGraph& g, int mode, uint64_t seed, int rounds, idx_t*
   RMB_CUDA(cudaMemsetAsync(stamp, 0, sizeof(int32_t) * (size_t)g.n, st));
   RMB_CUDA(cudaMemsetAsync(best, 0, sizeof(unsigned long long) * (size_t)g.n, st));
   const int blocks = grid_for(g.n, 256);
-  k_match_init<<<blocks, 256, 0, st>>>(g.n, match);
-  RMB_LAUNCH_CHECK();
   const bool w = g.adjwgt != nullptr;
   const uint64_t vseed = mix64(seed ^ 0x7669736974ULL);
+  if (coop_matching()) {
+    const int cb = w ? coop_blocks<true>() : coop_blocks<false>();
+    if (cb > 0) {
+      MatchCoop a;
+      a.xadj = g.xadj;
+      a.adj = g.adjncy;
+      a.adjwgt = g.adjwgt;
+      a.heavy = heavy;
+      a.n = g.n;
+      a.nheavy = nheavy;
+      a.mode = mode;
+      a.rounds = rounds;
+      a.match = match;
+      a.prop = prop;
+      a.stamp = stamp;
+      a.best = best;
+      a.newly = newly;
+      a.seed = seed;
+      a.vseed = vseed;
+      void* args[] = {&a};
+      const int ph = profiler().begin(kProfPropose, st);
+      const cudaError_t e = cudaLaunchCooperativeKernel(w ? (const void*)k_match_coop<true>
+                                                          : (const void*)k_match_coop<false>,
+                                                        std::min(blocks, cb), 256, args, 0, st);
+      profiler().end(ph, st, 12.0 * g.n + (w && mode == 1 ? 12.0 : 8.0) * (double)g.m);
+      if (e == cudaSuccess) {
+        launch_counter().fetch_add(1);
+        arena.reset_to(mk);
+        return;
+      }
+      cudaGetLastError();  // not launched: the launch-per-phase loop below
+    }
+  }
+  k_match_init<<<blocks, 256, 0, st>>>(g.n, match);
+  RMB_LAUNCH_CHECK();
   bool handshake = true;  // first phase; the finishing phase follows when it stalls
   int phase_start = 0;
   for (int r = 0; r < rounds; ++r) {
@@ -392,19 +513,33 @@ __device__ __forceinline__ void contract_warp_body(const idx_t* xadj, const idx_
     for (int32_t i = lane; i < tsize; i += 32) tkey[i] = -1;
     __syncwarp();
     int32_t U = 0;
-    for (int mbr = 0; mbr < 2; ++mbr) {
-      const int32_t src = mbr == 0 ? mem0[c] : mem1[c];
-      if (src < 0) break;
-      const int32_t e = xadj[src + 1];
-      for (int32_t base = xadj[src]; base < e; base += 32) {
-        const int32_t j = base + lane;
-        int32_t cu = -1, w = 0;
-        bool valid = j < e;
-        if (valid) {
-          cu = cmap[adj[j]];
-          valid = cu != c;
-          w = HAS_W ? adjwgt[j] : 1;
-        }
+    // The two members' rows as one sequence (member 0's row first, each in
+    // CSR order): first appearances keep their order whatever the chunking.
+    // Four chunks are loaded at once so that their adjncy and cmap gathers
+    // overlap instead of forming one dependent chain per chunk.
+    const int32_t a0 = mem0[c], a1 = mem1[c];
+    const int32_t s0 = xadj[a0], len0 = xadj[a0 + 1] - s0;
+    const int32_t s1 = a1 >= 0 ? xadj[a1] : 0, len1 = a1 >= 0 ? xadj[a1 + 1] - s1 : 0;
+    const int32_t total = len0 + len1;
+    constexpr int kPre = 4;
+    for (int32_t base = 0; base < total; base += 32 * kPre) {
+      int32_t uu[kPre], ww[kPre];
+#pragma unroll
+      for (int q = 0; q < kPre; ++q) {
+        const int32_t idx = base + q * 32 + lane;
+        const int32_t j = idx < len0 ? s0 + idx : s1 + (idx - len0);
+        const bool in = idx < total;
+        uu[q] = in ? adj[j] : -1;
+        ww[q] = in ? (HAS_W ? adjwgt[j] : 1) : 0;
+      }
+#pragma unroll
+      for (int q = 0; q < kPre; ++q) uu[q] = uu[q] >= 0 ? cmap[uu[q]] : -1;
+#pragma unroll
+      for (int q = 0; q < kPre; ++q) {
+        if (base + q * 32 >= total) break;  // warp-uniform
+        const int32_t cu = uu[q];
+        const int32_t w = ww[q];
+        const bool valid = cu >= 0 && cu != c;
         const unsigned peers = __match_any_sync(0xffffffffu, valid ? cu : -(lane + 2));
         const bool leader = valid && (__ffs(peers) - 1) == lane;
         lanew[lane] = valid ? w : 0;
@@ -413,8 +548,8 @@ __device__ __forceinline__ void contract_warp_body(const idx_t* xadj, const idx_
         if (leader) {
           unsigned m = peers;
           while (m) {
-            const int b = __ffs(m) - 1;
-            gsum += lanew[b];
+            const int bb = __ffs(m) - 1;
+            gsum += lanew[bb];
             m &= m - 1;
           }
         }

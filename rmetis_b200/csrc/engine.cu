@@ -475,6 +475,7 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
     rp.over_thr = over_of(L);
     rp.small_weights = small[L];
     rp.fused_max_n = o.fused_max_n;
+    rp.fused_edge_factor = o.fused_edge_factor;
     rp.fm_fused_max_n = o.fm_fused_max_n;
     // A traced run replays bit for bit in the oracle: exact walks everywhere.
     rp.exact_max_n = trace ? INT32_MAX : o.exact_max_n;

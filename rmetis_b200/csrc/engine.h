@@ -38,6 +38,7 @@ struct KwayOptions {
   int exact_max_n = 16384;      // larger levels decide cut passes by parallel admission
   int contract_thread_max = 32; // coarse rows with a longer bound are merged by a warp (16 or 32)
   int gain_block = 256;         // threads per block of the gain-table kernel
+  int fused_edge_factor = 4;    // ... with at most this many entries per vertex of fused_max_n
   int fm_fused_max_n = 4096;    // FM levels up to this size refine in one launch
   int bisect_fm2 = 0;           // 1: a 2-way partition with rtype Fm refines with the 2-way FM of fm.rs
 };

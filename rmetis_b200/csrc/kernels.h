@@ -110,6 +110,11 @@ struct TailOut {
   int32_t coarse_vw[kTailMaxLevels];
 };
 
+// 1 (default): the matching rounds of a level run in one cooperative launch
+// (grid-wide barriers between phases); 0: one launch per phase. The same
+// matching either way.
+int& coop_matching();
+
 // Arguments of one graph's coarsening in a single block (coarsen_tail and
 // the batched form).
 struct TailArgs {
@@ -197,10 +202,13 @@ struct RefineParams {
   // Set when every part weight (|pw| <= total < 2^28) and every threshold
   // (|feas|, |over| < 2^29) is small: the walk may then keep 32-bit slacks.
   bool small_weights = false;
-  // Levels with at most this many vertices and 4 times as many adjacency
-  // entries (and k <= 256, ncon <= 2) run all their passes in one
+  // Levels with at most this many vertices and fused_edge_factor times as
+  // many adjacency entries (and k <= 256, ncon <= 2) run all their passes in one
   // single-block launch (k_refine_level); 0 = never.
   int32_t fused_max_n = 0;
+  // ... and at most this many adjacency entries per vertex of fused_max_n
+  // (the edge bound is fused_edge_factor * fused_max_n).
+  int32_t fused_edge_factor = 4;
   // FM levels with at most this many vertices (k <= 256, ncon <= 2, exact
   // walk) run all their passes and rounds in one single-block launch
   // (k_fm_level); 0 = never.

@@ -1391,7 +1391,8 @@ RefineStats greedy_refine(const DGraph& g, idx_t* part, const RefineParams& rp, 
   r.np = arena.alloc<int32_t>((size_t)g.n);
   // One block refines a level well while its edges stay few; a denser level of
   // the same size does better spread over the device.
-  const bool fused = rp.fused_max_n > 0 && g.n <= rp.fused_max_n && g.m <= 4LL * rp.fused_max_n && k <= 256 &&
+  const bool fused = rp.fused_max_n > 0 && g.n <= rp.fused_max_n &&
+                     g.m <= (int64_t)rp.fused_edge_factor * rp.fused_max_n && k <= 256 &&
                      g.ncon <= 2;
   int32_t* ghist = nullptr;
   if (nheavy > 0 && (fused || k > kGainHist))

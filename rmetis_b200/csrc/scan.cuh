@@ -119,6 +119,51 @@ __global__ void k_tile_scan(Load load, Store store, int64_t n, const T* tile_off
   }
 }
 
+// Phases 2 and 3 in one launch for inputs of at most kScanFusedTiles tiles:
+// each block sums the tile totals before it (a few thousand L2 reads) instead
+// of waiting for a separate scan of the tile sums; the last block writes the
+// grand total.
+constexpr int64_t kScanFusedTiles = 4096;
+
+template <typename T, typename Load, typename Store>
+__global__ void k_tile_scan_fused(Load load, Store store, int64_t n, const T* tile_sums, int64_t ntiles,
+                                  T* total_out) {
+  __shared__ T sw[32];
+  __shared__ T tile[kScanTile];
+  T before = 0;
+  for (int64_t i = threadIdx.x; i < (int64_t)blockIdx.x; i += blockDim.x) before += tile_sums[i];
+  T offset;
+  block_exclusive_scan<T>(before, sw, &offset);
+  const int64_t base = (int64_t)blockIdx.x * kScanTile;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const int64_t j = base + (int64_t)i * kScanThreads + threadIdx.x;
+    tile[i * kScanThreads + threadIdx.x] = (j < n) ? load(j) : T(0);
+  }
+  __syncthreads();
+  T vals[kScanItems];
+  T s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    vals[i] = tile[threadIdx.x * kScanItems + i];
+    s += vals[i];
+  }
+  T tile_total;
+  T run = block_exclusive_scan<T>(s, sw, &tile_total) + offset;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    tile[threadIdx.x * kScanItems + i] = run;
+    run += vals[i];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const int64_t j = base + (int64_t)i * kScanThreads + threadIdx.x;
+    if (j < n) store(j, tile[i * kScanThreads + threadIdx.x]);
+  }
+  if (threadIdx.x == 0 && total_out && (int64_t)blockIdx.x == ntiles - 1) *total_out = offset + tile_total;
+}
+
 // Small inputs: the whole scan in one block (tiles of 1024 x 8 items in
 // order, with a running carry), one launch instead of three.
 constexpr int kScanSmallThreads = 1024;
@@ -163,24 +208,47 @@ __global__ void __launch_bounds__(kScanSmallThreads) k_scan_small(Load load, Sto
   if (threadIdx.x == 0 && total_out) *total_out = carry;
 }
 
-// Exclusive scan of load(0..n-1) by one block (inside a fused kernel): each
-// thread takes a contiguous run of ceil(n / blockDim.x) items. Every thread of
-// the block must call it; sw holds 32 values of shared memory.
+// Exclusive scan of load(0..n-1) by one block (inside a fused kernel), in
+// tiles of blockDim.x * 4 items: warp w takes the w-th run of 128 items of a
+// tile, its lanes reading 32 consecutive items at a time (coalesced), and
+// each item is loaded once. Every thread of the block must call it; sw holds
+// 32 values of shared memory.
 template <typename T, typename Load, typename Store>
 __device__ void block_scan_n(Load load, Store store, int64_t n, T* total_out, T* sw) {
-  const int64_t per = (n + blockDim.x - 1) / blockDim.x;
-  const int64_t b = (int64_t)threadIdx.x * per;
-  const int64_t e = b + per < n ? b + per : n;
-  T s = 0;
-  for (int64_t i = b; i < e; ++i) s += load(i);
-  T tot;
-  T ex = block_exclusive_scan<T>(s, sw, &tot);
-  for (int64_t i = b; i < e; ++i) {
-    const T v = load(i);
-    store(i, ex);
-    ex += v;
+  constexpr int kIt = 4;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int64_t tile = (int64_t)blockDim.x * kIt;
+  T carry = 0;
+  for (int64_t base = 0; base < n; base += tile) {
+    const int64_t wbase = base + (int64_t)wid * 32 * kIt;
+    T v[kIt];
+    T s = 0;
+#pragma unroll
+    for (int i = 0; i < kIt; ++i) {
+      const int64_t idx = wbase + i * 32 + lane;
+      v[i] = idx < n ? load(idx) : T(0);
+      s += v[i];
+    }
+    s = warp_sum(s);
+    T tile_total;
+    // lane 0 of each warp stands for its run: the exclusive scan gives the run's offset
+    const T wex = block_exclusive_scan<T>(lane == 0 ? s : T(0), sw, &tile_total);
+    T off = carry + __shfl_sync(0xffffffffu, wex, 0);
+#pragma unroll
+    for (int i = 0; i < kIt; ++i) {
+      T x = v[i];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const T y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      const int64_t idx = wbase + i * 32 + lane;
+      if (idx < n) store(idx, off + x - v[i]);
+      off += __shfl_sync(0xffffffffu, x, 31);
+    }
+    carry += tile_total;
   }
-  if (threadIdx.x == 0 && total_out) *total_out = tot;
+  if (threadIdx.x == 0 && total_out) *total_out = carry;
 }
 
 template <typename T>
@@ -226,6 +294,13 @@ void exclusive_scan(Load load, Store store, int64_t n, T* total_dev, Arena& aren
     RMB_LAUNCH_CHECK();
   } else {
     RMB_CUDA(cudaMemsetAsync(sums, 0, sizeof(T), st));
+  }
+  if (n > 0 && ntiles <= kScanFusedTiles) {
+    k_tile_scan_fused<T, Load, Store><<<(unsigned)ntiles, kScanThreads, 0, st>>>(load, store, n, sums, ntiles,
+                                                                                 total_dev);
+    RMB_LAUNCH_CHECK();
+    arena.reset_to(mk);
+    return;
   }
   k_scan_tile_sums<T><<<1, 1024, 0, st>>>(sums, ntiles, total_dev);
   RMB_LAUNCH_CHECK();

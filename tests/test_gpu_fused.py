@@ -125,3 +125,40 @@ def test_fm_full_partitions_identical_across_paths(rmb):
             rmb.set_fm_fused_max(4096)
         assert multi.objval == fused.objval
         np.testing.assert_array_equal(multi.part, fused.part)
+
+
+@pytest.mark.parametrize("name", list(GRAPHS))
+@pytest.mark.parametrize("mode", [0, 1])
+def test_coop_matching_identical(rmb, name, mode):
+    """The matching rounds in one cooperative launch (grid-wide barriers,
+    progress checks on the device) and one launch per phase with host checks
+    give the same matching."""
+    from rmetis_b200 import functions as F
+    x, a, v, w = load(name)
+    g = rmb.Graph(len(x) - 1, 1, x, a, vwgt=v, adjwgt=w)
+    out = {}
+    try:
+        for on in (0, 1):
+            rmb.set_coop_matching(on)
+            out[on] = F.match(g, mode=mode, seed=77, rounds=24)
+    finally:
+        rmb.set_coop_matching(1)
+    np.testing.assert_array_equal(out[0], out[1])
+    m = out[1]
+    assert (m[m] == np.arange(len(m))).all()
+
+
+def test_coop_matching_full_partitions(rmb):
+    cases = [(G.grid3d(40, weights_seed=2), 64), (G.random_graph(30000, 9.0, seed=4), 16)]
+    for (x, a, v, w), k in cases:
+        g = rmb.Graph(len(x) - 1, 1, x, a, vwgt=v, adjwgt=w)
+        o = rmb.Options(rtype=rmb.RType.Greedy, seed=8)
+        try:
+            rmb.set_coop_matching(0)
+            plain = rmb.part_graph_kway(g, k, options=o)
+            rmb.set_coop_matching(1)
+            coop = rmb.part_graph_kway(g, k, options=o)
+        finally:
+            rmb.set_coop_matching(1)
+        assert plain.objval == coop.objval
+        np.testing.assert_array_equal(plain.part, coop.part)
