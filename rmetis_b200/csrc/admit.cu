@@ -144,15 +144,39 @@ __device__ void apply_body(Lanes L, const int32_t* __restrict__ nm_dev, const id
                            const int32_t* __restrict__ cut, idx_t* __restrict__ part,
                            const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
                            idx_t* __restrict__ touched) {
+  const unsigned FULL = 0xffffffffu;
   const int32_t nm = *nm_dev;
-  RMB_FOR(j, nm, L) {
-    const int32_t t = tgt[j];
-    if (t >= 0 && rank[j] < cut[t]) {
-      const int32_t v = movers[j];
-      part[v] = t;
-      if (touched) {
+  const int lane = threadIdx.x & 31;
+  // Warp-uniform trips (the lanes of a warp hold consecutive movers); the
+  // neighbours of a moved vertex with a long row are flagged by the whole
+  // warp, so a hub's row is not one thread's loop.
+  for (int64_t j0 = L.first - lane; j0 < nm; j0 += L.stride) {
+    const int64_t j = j0 + lane;
+    int32_t v = -1;
+    if (j < nm) {
+      const int32_t t = tgt[j];
+      if (t >= 0 && rank[j] < cut[t]) {
+        v = movers[j];
+        part[v] = t;
+      }
+    }
+    if (touched) {
+      // Short rows by their own thread, rows above kHeavyDegree by the warp.
+      bool long_row = false;
+      if (v >= 0) {
         touched[v] = 1;
-        for (int32_t e = xadj[v]; e < xadj[v + 1]; ++e) touched[adj[e]] = 1;
+        const int32_t s0 = xadj[v], e0 = xadj[v + 1];
+        long_row = e0 - s0 > kHeavyDegree;
+        if (!long_row)
+          for (int32_t x = s0; x < e0; ++x) touched[adj[x]] = 1;
+      }
+      unsigned mv = __ballot_sync(FULL, long_row);
+      while (mv) {
+        const int l = __ffs(mv) - 1;
+        mv &= mv - 1;
+        const int32_t u = __shfl_sync(FULL, v, l);
+        const int32_t e = xadj[u + 1];
+        for (int32_t x = xadj[u] + lane; x < e; x += 32) touched[adj[x]] = 1;
       }
     }
   }

@@ -183,11 +183,27 @@ __device__ void gain_heavy_body(int32_t gw, int32_t nw, int32_t* hist, const idx
     __syncwarp();
     uint32_t wf = 0;
     int bnd = 0;
-    for (int32_t j = s + lane; j < e; j += 32) {
-      const int32_t pu = part[adj[j]];
-      const uint32_t w = (uint32_t)(HAS_W ? adjwgt[j] : 1);
-      if (pu == pv) wf += w;
-      else { bnd = 1; atomicAdd(reinterpret_cast<unsigned*>(&hist[pu]), w); }
+    // Eight entries per lane at a time: their adjncy and part gathers are in
+    // flight together (a hub's row is otherwise one long dependent chain).
+    constexpr int kIlp = 8;
+    for (int32_t j0 = s; j0 < e; j0 += 32 * kIlp) {
+      int32_t uu[kIlp];
+      uint32_t ww[kIlp];
+#pragma unroll
+      for (int q = 0; q < kIlp; ++q) {
+        const int32_t j = j0 + q * 32 + lane;
+        uu[q] = j < e ? adj[j] : -1;
+        ww[q] = j < e ? (uint32_t)(HAS_W ? adjwgt[j] : 1) : 0u;
+      }
+#pragma unroll
+      for (int q = 0; q < kIlp; ++q) uu[q] = uu[q] >= 0 ? part[uu[q]] : -1;
+#pragma unroll
+      for (int q = 0; q < kIlp; ++q) {
+        const int32_t pu = uu[q];
+        if (pu < 0) continue;
+        if (pu == pv) wf += ww[q];
+        else { bnd = 1; atomicAdd(reinterpret_cast<unsigned*>(&hist[pu]), ww[q]); }
+      }
     }
     wf = warp_sum(wf);
     const bool boundary = __any_sync(FULL, bnd);
