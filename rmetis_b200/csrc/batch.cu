@@ -210,7 +210,8 @@ void Engine::partition_kway_batch(std::vector<BatchItem>& items, const float* ub
     plan[b].item = b;
     plan[b].k = items[b].k;
     // kway.rs:55-61, attempt 0
-    plan[b].seed64 = o.seed == 0 ? (((uint64_t)rd() << 32) ^ (uint64_t)rd()) : o.seed;
+    const uint64_t sd = items[b].seed >= 0 ? (uint64_t)items[b].seed : o.seed;
+    plan[b].seed64 = sd == 0 ? (((uint64_t)rd() << 32) ^ (uint64_t)rd()) : sd;
   }
   // Largest graphs first: blocks start in index order.
   std::vector<int32_t> order(B);

@@ -6,6 +6,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <exception>
+#include <condition_variable>
+#include <thread>
+#include <memory>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -937,6 +940,160 @@ int RMETIS_GPU_PartGraphKwayBatch(idx_t ngraphs, idx_t ncon, const int64_t* vtx_
 }
 
 namespace {
+
+// ---- continuous batching of small requests --------------------------------
+// A request of RMETIS_GPU_SubmitKway that the batched kernels can take goes to
+// the device's dispatcher instead of the worker pool: a thread that, whenever
+// it is idle, takes every request queued meanwhile and runs them as one batch
+// (Engine::partition_kway_batch on its own engine and stream), grouped by
+// options (all but the seed), ncon and ubvec. Requests that arrive while a
+// batch runs form the next one, so batches grow with the load. Large requests
+// keep running on the pool at the same time.
+struct BatchReq {
+  int32_t n = 0, nc = 1, np = 2;
+  int64_t ne = 0;
+  const idx_t* xadj = nullptr;
+  const idx_t* adjncy = nullptr;
+  const idx_t* vwgt = nullptr;
+  const idx_t* adjwgt = nullptr;
+  idx_t* objval = nullptr;
+  idx_t* part = nullptr;
+  KwayOptions o;
+  std::vector<real_t> ub;
+  std::promise<int> prom;
+  bool done = false;
+  void finish(int rc) {
+    if (!done) {
+      done = true;
+      prom.set_value(rc);
+    }
+  }
+};
+
+std::vector<long long> group_key(const BatchReq& r) {
+  const KwayOptions& o = r.o;
+  std::vector<long long> k = {r.nc, o.ctype, o.iptype, o.rtype, o.niter, o.ncuts, (long long)o.ufactor,
+                              o.grow_trials, o.match_rounds, o.summed_unit_weights, o.fused_max_n, o.tail_max_n,
+                              o.exact_max_n, o.contract_thread_max, o.gain_block, o.fused_edge_factor,
+                              o.fm_fused_max_n, (long long)r.ub.size()};
+  for (real_t u : r.ub) {
+    uint32_t bits;
+    std::memcpy(&bits, &u, sizeof(bits));
+    k.push_back(bits);
+  }
+  return k;
+}
+
+class Dispatcher {
+ public:
+  explicit Dispatcher(int dev) : dev_(dev) { th_ = std::thread([this] { run(); }); }
+  std::future<int> submit(std::unique_ptr<BatchReq> r) {
+    std::future<int> f = r->prom.get_future();
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      q_.push_back(std::move(r));
+    }
+    cv_.notify_one();
+    return f;
+  }
+
+ private:
+  void run() {
+    cudaSetDevice(dev_);
+    Engine E(true);
+    for (;;) {
+      std::vector<std::unique_ptr<BatchReq>> take;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return !q_.empty(); });
+        take.swap(q_);
+      }
+      std::map<std::vector<long long>, std::vector<BatchReq*>> groups;
+      for (auto& r : take) groups[group_key(*r)].push_back(r.get());
+      for (auto& kv : groups) run_group(E, kv.second);
+      for (auto& r : take) r->finish(METIS_ERROR);  // (every request is finished above)
+    }
+  }
+
+  static void run_group(Engine& E, std::vector<BatchReq*>& grp) {
+    Arena::Mark mk = E.arena().mark();
+    try {
+      std::vector<BatchItem> items(grp.size());
+      for (size_t i = 0; i < grp.size(); ++i) {
+        BatchReq& r = *grp[i];
+        BatchItem& it = items[i];
+        it.g.n = r.n;
+        it.g.m = r.ne;
+        it.g.ncon = r.nc;
+        it.g.xadj = upload(E, r.xadj, (size_t)r.n + 1);
+        it.g.adjncy = upload(E, r.adjncy, (size_t)r.ne);
+        it.g.vwgt = upload(E, r.vwgt, (size_t)r.n * r.nc);
+        it.g.adjwgt = upload(E, r.adjwgt, (size_t)r.ne);
+        it.k = r.np;
+        it.part_out = E.arena().alloc<idx_t>((size_t)r.n);
+        it.seed = (int64_t)r.o.seed;
+      }
+      const BatchReq& r0 = *grp[0];
+      bool batched = true;
+      try {
+        E.partition_kway_batch(items, r0.ub.empty() ? nullptr : r0.ub.data(), r0.o);
+      } catch (const Error& e) {
+        if (e.code != METIS_ERROR_MEMORY) throw;
+        batched = false;  // out of device memory: one request at a time
+      }
+      for (size_t i = 0; i < grp.size(); ++i) {
+        BatchReq& r = *grp[i];
+        BatchItem& it = items[i];
+        if (!batched || it.status == 0) {
+          try {
+            // (validated by the batch unless it never ran)
+            if (!batched && validate_device(it.g, E.arena(), E.stream(), E.host_scratch()) != 0)
+              throw Error(METIS_ERROR_INPUT, "graph failed validation");
+            int32_t obj = 0;
+            E.partition_kway(it.g, r.np, nullptr, r.ub.empty() ? nullptr : r.ub.data(), r.o, it.part_out, &obj,
+                             nullptr);
+            it.status = METIS_OK;
+            it.objval = obj;
+          } catch (const Error& e) {
+            it.status = e.code;
+          }
+        }
+        if (it.status == METIS_OK) download(E, r.part, it.part_out, (size_t)r.n);
+      }
+      RMB_CUDA(cudaStreamSynchronize(E.stream()));
+      for (size_t i = 0; i < grp.size(); ++i) {
+        if (items[i].status == METIS_OK && grp[i]->objval) *grp[i]->objval = items[i].objval;
+        grp[i]->finish(items[i].status);
+      }
+    } catch (const Error& e) {
+      cudaStreamSynchronize(E.stream());
+      for (BatchReq* r : grp) r->finish(e.code);
+    } catch (...) {
+      cudaStreamSynchronize(E.stream());
+      for (BatchReq* r : grp) r->finish(METIS_ERROR);
+    }
+    E.arena().reset_to(mk);
+  }
+
+  int dev_;
+  std::thread th_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::vector<std::unique_ptr<BatchReq>> q_;
+};
+
+Dispatcher& dispatcher_for_device(int dev) {
+  static std::mutex m;
+  static std::vector<Dispatcher*> ds;
+  std::lock_guard<std::mutex> lk(m);
+  if ((int)ds.size() <= dev) ds.resize(dev + 1, nullptr);
+  if (!ds[dev]) ds[dev] = new Dispatcher(dev);  // lives until process exit
+  return *ds[dev];
+}
+
+}  // namespace
+
+namespace {
 struct Tickets {
   std::mutex mu;
   int64_t next = 1;
@@ -966,6 +1123,26 @@ int64_t RMETIS_GPU_SubmitKway(const idx_t* nvtxs, const idx_t* ncon, const idx_t
     if (ubvec) ub.assign(ubvec, ubvec + nc);
     int dev = 0;
     RMB_CUDA(cudaGetDevice(&dev));
+    if (batch_mode() == 1 && !tpwgts && n <= batch_max_n() && batch_eligible(o, n, np, nc)) {
+      auto r = std::make_unique<BatchReq>();
+      r->n = n;
+      r->nc = nc;
+      r->np = np;
+      r->ne = ne;
+      r->xadj = xadj;
+      r->adjncy = adjncy;
+      r->vwgt = vwgt;
+      r->adjwgt = adjwgt;
+      r->objval = objval;
+      r->part = part;
+      r->o = o;
+      r->ub = ub;
+      std::shared_future<int> f = dispatcher_for_device(dev).submit(std::move(r)).share();
+      std::lock_guard<std::mutex> lk(tickets().mu);
+      const int64_t id = tickets().next++;
+      tickets().pending.emplace(id, f);
+      return id;
+    }
     WorkerPool& pool = pool_for_device(dev);
     std::shared_future<int> f =
         pool.submit(footprint_bytes(n, ne, np, nc), [=](Engine& W) {

@@ -67,6 +67,7 @@ struct BatchItem {
   DGraph g;
   int k = 2;
   idx_t* part_out = nullptr;
+  int64_t seed = -1;  // >= 0: this item's options seed instead of the shared one
   int32_t objval = 0;
   int status = 0;
 };

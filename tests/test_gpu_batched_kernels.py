@@ -150,3 +150,33 @@ def test_batched_invalid_graph_keeps_others(rmb, batch_mode):
         lo = 0 if gi == 0 else 1604
         assert obj[0 if gi == 0 else 2] == solo.objval
         np.testing.assert_array_equal(part[lo:lo + len(x) - 1], solo.part)
+
+
+def test_submitted_requests_batched_equal_sync_calls(rmb, batch_mode):
+    """Continuous batching: submitted requests that the batched kernels can take
+    are collected by the device's dispatcher while earlier batches run, grouped
+    by options, and partitioned together; each result equals the synchronous
+    call's. The requests mix seeds, ufactors (two groups), k buckets, a graph
+    above the batch size limit (the pool) and an invalid graph."""
+    rng = np.random.default_rng(21)
+    reqs = []
+    for i in range(30):
+        n = int(rng.integers(500, 12000))
+        x, a, w, _ = G.rgg2d(n, 700 + i, mean_degree=8.0)
+        v = rng.integers(1, 5, size=n).astype(np.int32) if i % 3 else None
+        g = graph_of(rmb, x, a, v, w)
+        reqs.append((g, int(rng.choice([4, 16, 40, 100])), greedy(rmb, 100 + i, ufactor=30 if i % 2 else 50)))
+    rmb.set_batch_mode(1, 8000)   # graphs above 8,000 vertices on the pool
+    try:
+        tickets = [rmb.submit_kway(g, k, options=o) for g, k, o in reqs]
+        bad = rmb.Graph(4, 1, np.array([0, 2, 4, 6, 8]), np.array([1, 3, 0, 2, 1, 3, 0, 0]), validate=False)
+        bad_t = rmb.submit_kway(bad, 2, options=greedy(rmb, 1))
+        results = [t.wait() for t in tickets]
+        with pytest.raises(rmb.InputError):
+            bad_t.wait()
+    finally:
+        rmb.set_batch_mode(1, 131072)
+    for (g, k, o), r in zip(reqs, results):
+        solo = rmb.part_graph_kway(g, k, options=o)
+        assert r.objval == solo.objval
+        np.testing.assert_array_equal(r.part, solo.part)
