@@ -297,7 +297,7 @@ static int coop_blocks() {
 }
 
 void match_parallel(const DGraph& g, int mode, uint64_t seed, int rounds, idx_t* match, const idx_t* heavy,
-                    int32_t nheavy, Arena& arena, cudaStream_t st, int32_t* h_scratch) {
+                    int32_t nheavy, Arena& arena, cudaStream_t st, int32_t* h_scratch, bool coop) {
   Arena::Mark mk = arena.mark();
   idx_t* prop = arena.alloc<idx_t>((size_t)g.n);
   int32_t* stamp = arena.alloc<int32_t>((size_t)g.n);
@@ -309,7 +309,7 @@ void match_parallel(const DGraph& g, int mode, uint64_t seed, int rounds, idx_t*
   const int blocks = grid_for(g.n, 256);
   const bool w = g.adjwgt != nullptr;
   const uint64_t vseed = mix64(seed ^ 0x7669736974ULL);
-  if (coop_matching()) {
+  if (coop && coop_matching()) {
     const int cb = w ? coop_blocks<true>() : coop_blocks<false>();
     if (cb > 0) {
       MatchCoop a;

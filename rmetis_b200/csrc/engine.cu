@@ -311,7 +311,11 @@ void Engine::run_attempt(const DGraph& g0, int k, const float* tpwgts, const std
       Arena::Mark mm = arena_.mark();
       idx_t* match = arena_.alloc<idx_t>((size_t)cur.n);
       const uint64_t lseed = mix64(seed64 * 0x100000001b3ULL + (uint64_t)lvl + 1);
-      match_parallel(cur, o.ctype == 0 ? 0 : 1, lseed, o.match_rounds, match, hl, nh, arena_, st, h_scratch_);
+      // A cooperative launch waits until all its blocks fit on the device at
+      // once, which stalls a worker whose jobs share the device with others:
+      // workers match with one launch per phase.
+      match_parallel(cur, o.ctype == 0 ? 0 : 1, lseed, o.match_rounds, match, hl, nh, arena_, st, h_scratch_,
+                     !is_worker_);
       if (trace) {
         std::vector<int32_t> hm(cur.n);
         RMB_CUDA(cudaMemcpyAsync(hm.data(), match, sizeof(int32_t) * cur.n, cudaMemcpyDeviceToHost, st));

@@ -69,9 +69,10 @@ void compact_flags(const idx_t* flag, int32_t n, idx_t* out, idx_t* count_dev, A
 // random_matching src/coarsen/rm.rs:13-43). mode 1 = heavy edge first
 // (SHEM), 0 = random (RM). match[v] is an involution, self = unmatched.
 // heavy/nheavy: precomputed list of vertices with degree > kHeavyDegree.
+// coop: the rounds may run in one cooperative launch (coop_matching()).
 void match_parallel(const DGraph& g, int mode, uint64_t seed, int rounds, idx_t* match,
                     const idx_t* heavy, int32_t nheavy, Arena& arena, cudaStream_t st,
-                    int32_t* h_scratch);
+                    int32_t* h_scratch, bool coop = true);
 
 struct CoarseResult {
   DGraph g;
