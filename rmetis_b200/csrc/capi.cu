@@ -267,7 +267,8 @@ HostGraph extract_sub(const HostGraph& g, const std::vector<idx_t>& part, idx_t 
 
 // multilevel_bisect (recursive.rs:133-187) on the GPU. A bisection without
 // edges has cut 0 whatever it does; it is split on the host in vertex order,
-// filling side 0 up to its target on constraint 0.
+// each vertex to the side it leaves least loaded relative to its targets on
+// all constraints.
 void bisect(Engine& E, const HostGraph& g, const std::vector<float>& tp2, const real_t* ubvec, const KwayOptions& o,
             uint64_t seed, std::vector<idx_t>& part) {
   part.assign((size_t)g.n, 0);
@@ -276,16 +277,26 @@ void bisect(Engine& E, const HostGraph& g, const std::vector<float>& tp2, const 
     return;
   }
   if (g.xadj[g.n] == 0) {
-    double tot = 0;
-    for (int32_t v = 0; v < g.n; ++v) tot += g.vw(v, 0);
-    const double t0 = (double)tp2[0] * tot;
-    double w0 = 0;
-    for (int32_t v = 0; v < g.n; ++v) {
-      if (w0 + g.vw(v, 0) <= t0) {
-        w0 += g.vw(v, 0);
-      } else {
-        part[v] = 1;
+    // Each vertex, in order, goes to the side whose largest relative load
+    // (weight / target over the constraints) stays lower with it (side 0 on
+    // ties), which keeps both sides near their targets on every constraint.
+    const int nc = g.ncon;
+    std::vector<double> tot(nc, 0.0), w[2] = {std::vector<double>(nc, 0.0), std::vector<double>(nc, 0.0)};
+    for (int32_t v = 0; v < g.n; ++v)
+      for (int c = 0; c < nc; ++c) tot[c] += g.vw(v, c);
+    auto load = [&](int side, int32_t v) {
+      double worst = 0.0;
+      for (int c = 0; c < nc; ++c) {
+        const double t = (double)tp2[(size_t)side * nc + c] * tot[c];
+        const double x = w[side][c] + g.vw(v, c);
+        worst = std::max(worst, t > 0 ? x / t : (x > 0 ? 1e300 : 0.0));
       }
+      return worst;
+    };
+    for (int32_t v = 0; v < g.n; ++v) {
+      const int side = load(0, v) <= load(1, v) ? 0 : 1;
+      part[v] = side;
+      for (int c = 0; c < nc; ++c) w[side][c] += g.vw(v, c);
     }
     return;
   }

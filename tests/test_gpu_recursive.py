@@ -102,3 +102,23 @@ def test_recursive_valid_deterministic_and_quality(rmb, oracle, rtype, capsys):
         print(f"\nrecursive {rtype}: GPU summed cut {gpu_sum}, oracle {ref_sum}, ratio {gpu_sum / ref_sum:.3f}")
     # Measured on a B200: greedy 17,451 vs 22,990 (0.76), fm 11,453 vs 18,203 (0.63).
     assert gpu_sum <= 1.05 * ref_sum, (gpu_sum, ref_sum)
+
+
+def test_recursive_edgeless_two_constraints_balanced(rmb):
+    """A graph without edges is split on the host; with two constraints every
+    part stays within 5% of its target on both (each vertex goes to the side
+    it leaves least loaded relative to its targets)."""
+    import rmetis_b200 as R
+    for seed in range(3):
+        rng = np.random.default_rng(seed)
+        n, k = 400, 4
+        x = np.zeros(n + 1, np.int32)
+        a = np.zeros(0, np.int32)
+        v = rng.integers(1, 9, size=2 * n).astype(np.int32)
+        g = R.Graph(n, 2, x, a, vwgt=v)
+        r = R.part_graph_recursive(g, k, options=R.Options(seed=1))
+        assert r.objval == 0
+        pw = np.zeros((k, 2))
+        np.add.at(pw, r.part, v.reshape(n, 2))
+        tgt = v.reshape(n, 2).sum(axis=0) / k
+        assert (pw <= 1.05 * tgt[None, :]).all(), pw / tgt
