@@ -15,8 +15,9 @@
 //   3. one read-back of every level table; the host derives each graph's
 //      thresholds, grow seeds and refinement jobs and uploads them at once
 //   4. every grow trial of every coarsest graph            (k_batch_grow)
-//   5. step s = 0, 1, ...: level L_g - s of every graph g that has it, with
-//      its projection, repair pass and exact cut passes     (k_batch_level)
+//   5. step s = 0, 1, ...: level Lmax - s of every graph that has it (the
+//      coarsest of a graph first), with its projection or best grow trial,
+//      repair pass and exact cut passes                     (k_batch_level)
 //      and the admission cut passes of its large levels     (k_batch_admit)
 //   6. the cut of every result                              (k_batch_cut)
 //
@@ -507,10 +508,17 @@ void Engine::partition_kway_batch(std::vector<BatchItem>& items, const float* ub
       int32_t b;
       int l;
     };
+    // Step s refines level index max_steps - 1 - s of every graph that has
+    // it: the graphs with the most levels start first and every graph ends
+    // with its input level in the last step. A step lasts as long as its
+    // largest level, and the largest levels of a step are then the same
+    // graph's (the largest graphs have the largest level at each index), so
+    // the steps add up to about that graph's own refinement time.
     std::vector<Entry> es;
+    const int l_step = max_steps - 1 - s;
     for (int32_t b : planned) {
       const int L = (int)plan[b].levels.size() - 1;
-      if (L - s >= 0) es.push_back({b, L - s});
+      if (l_step <= L) es.push_back({b, l_step});
     }
     auto make_job = [&](const Entry& e) {
       GraphPlan& P = plan[e.b];
