@@ -190,7 +190,7 @@ RMETIS_API int RMETIS_GPU_SetPoolTuning(int fused_max_n, int tail_max_n);
  * vtx_off[g]*ncon, its part at part[vtx_off[g]]. nparts[g] per graph; ncon,
  * ubvec and options are shared. The batch is uploaded once. With Greedy
  * refinement (options[METIS_OPTION_RTYPE] = 1), ncuts 1, a grown initial
- * partition, ncon <= 2 and nparts[g] <= 256, graphs of up to 131072
+ * partition, ncon <= 2 and nparts[g] <= 256, graphs of up to 262144
  * vertices (RMETIS_GPU_SetBatchMode) go through the pipeline together: each
  * step (validation, coarsening, grow trials, the refinement of one level per
  * graph, the cut) is one launch over them, one thread block per graph; the
@@ -226,7 +226,7 @@ RMETIS_API int RMETIS_GPU_SetFmFusedMax(int max_n);
 
 /* How RMETIS_GPU_PartGraphKwayBatch runs its graphs (no counterpart in the
  * reference; results are the same either way). mode 1 (default): eligible
- * graphs with at most max_n vertices (default 131072) go through the batched
+ * graphs with at most max_n vertices (default 262144) go through the batched
  * launches, while the others run on the worker pool at the same time (a
  * large graph's levels take one thread block each in the batched launches,
  * so it finishes sooner on the pool's grid-wide kernels); mode 0: every graph

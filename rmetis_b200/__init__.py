@@ -438,7 +438,7 @@ def set_fm_fused_max(max_n: int = -1):
 def set_batch_mode(mode: int = -1, max_n: int = -1):
     """How part_graph_kway_batch runs its graphs. mode 1 (default): eligible
     graphs (Greedy, ncuts 1, grown initial partitions, ncon <= 2,
-    nparts <= 256) of at most max_n vertices (default 131072) go through the
+    nparts <= 256) of at most max_n vertices (default 262144) go through the
     batched launches, one step of the pipeline for all of them at a time,
     while the others run on the worker pool at the same time; mode 0: every
     graph on the worker pool. -1 leaves a value unchanged. Results are the

@@ -60,7 +60,7 @@ int& batch_mode() {
 // Graphs of a batch with more vertices than this run on the worker pool,
 // alongside the batched launches of the others.
 int& batch_max_n() {
-  static int m = 131072;
+  static int m = 262144;
   return m;
 }
 Tuning& tuning() {

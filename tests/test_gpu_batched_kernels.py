@@ -33,7 +33,7 @@ def graph_of(rmb, x, a, v=None, w=None, ncon=1):
 @pytest.fixture
 def batch_mode(rmb):
     yield
-    rmb.set_batch_mode(1, 131072)
+    rmb.set_batch_mode(1, 262144)
 
 
 def _check(rmb, graphs, ks, opts):
@@ -46,7 +46,7 @@ def _check(rmb, graphs, ks, opts):
     pool = rmb.part_graph_kway_batch(graphs, ks, options=opts)
     rmb.set_batch_mode(1, 5000)
     mixed = rmb.part_graph_kway_batch(graphs, ks, options=opts)
-    rmb.set_batch_mode(1, 131072)
+    rmb.set_batch_mode(1, 262144)
     for i, (g, k, r, q, x) in enumerate(zip(graphs, ks, batch, pool, mixed)):
         solo = rmb.part_graph_kway(g, k, options=opts)
         for res in (r, q, x):
@@ -175,7 +175,7 @@ def test_submitted_requests_batched_equal_sync_calls(rmb, batch_mode):
         with pytest.raises(rmb.InputError):
             bad_t.wait()
     finally:
-        rmb.set_batch_mode(1, 131072)
+        rmb.set_batch_mode(1, 262144)
     for (g, k, o), r in zip(reqs, results):
         solo = rmb.part_graph_kway(g, k, options=o)
         assert r.objval == solo.objval
