@@ -2,6 +2,7 @@
 // extensions declared in include/rmetis.h.
 #include <future>
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
@@ -16,6 +17,7 @@
 #include "../../include/rmetis.h"
 #include "engine.h"
 #include "prof.h"
+#include "scan.cuh"
 
 using namespace rmb;
 
@@ -225,10 +227,12 @@ DGraph dgraph(HostCall& h, idx_t n, idx_t ncon, const idx_t* xadj, const idx_t* 
 }
 
 // ---- recursive bisection (src/partition/recursive.rs:12-187) --------------
-// The recursion, the target arithmetic (f32, as the reference's Real) and the
-// subgraph extraction run on the host; every bisection with more than two
-// vertices and at least one edge is a 2-way multilevel partition on the GPU
-// (coarsening, grow trials and refinement of the engine).
+// The recursion's bookkeeping and the target arithmetic (f32, as the
+// reference's Real) run on the host; the subgraphs stay on the device, every
+// bisection with more than two vertices and at least one edge is a 2-way
+// multilevel partition on the GPU (coarsening, grow trials and refinement of
+// the engine), and the sides are extracted by kernels (rb_levels_dev). Nested
+// dissection keeps host subgraphs (HostGraph, extract_sub).
 struct HostGraph {
   int32_t n = 0;
   int32_t ncon = 1;
@@ -360,81 +364,275 @@ void bisect_all(std::vector<BisectJob>& jobs, const real_t* ubvec, const KwayOpt
   if (rc != 1) throw Error(rc, "a bisection failed");
 }
 
-// rb_recurse (recursive.rs:61-131), one recursion level at a time: a node
-// with nparts parts is bisected with the summed f32 targets of its halves
-// (k1 = nparts / 2), both sides are extracted as subgraphs and become the next
-// level's nodes with their targets divided by constraint 0's sum; a node with
-// one part, or no more vertices than parts, is assigned directly. The
-// bisections of a level run concurrently (bisect_all). The reference draws
-// every bisection from one generator; here the bisection at position h of the
-// recursion tree (root 0, children 2h+1 and 2h+2) runs with seed + h (0 stays
-// 0: an entropy seed per bisection).
-struct RbNode {
-  HostGraph g;
-  std::vector<int32_t> orig;
+// rb_recurse (recursive.rs:61-131), one recursion level at a time (the
+// device form below, rb_levels_dev): a node with nparts parts is bisected with
+// the summed f32 targets of its halves (k1 = nparts / 2), both sides are
+// extracted as subgraphs and become the next level's nodes with their targets
+// divided by constraint 0's sum; a node with one part, or no more vertices
+// than parts, is assigned directly. The bisections of a level run
+// concurrently on the worker pool. The reference draws every bisection from
+// one generator; here the bisection at position h of the recursion tree (root
+// 0, children 2h+1 and 2h+2) runs with seed + h (0 stays 0: an entropy seed
+// per bisection).
+// ---- the recursion on the device -------------------------------------------
+// The subgraphs of every level stay on the device: a level's bisections run on
+// the worker pool reading their subgraph in place, and both sides of each are
+// extracted by kernels (Graph::extract_subgraph, src/graph/mod.rs:209-273:
+// the side's vertices in ascending old id, each row keeping its same-side
+// neighbours in CSR order, renumbered). Per level the host reads back only the
+// children's sizes.
+struct DevNode {
+  DGraph g;
+  idx_t* orig = nullptr;  // [n] original vertex ids
   int32_t nparts = 2, offset = 0;
   std::vector<float> tp;
   uint64_t heap = 0;
 };
 
-void rb_levels(RbNode root, const real_t* ubvec, const KwayOptions& o, std::vector<idx_t>& part) {
-  std::vector<RbNode> frontier;
+struct LoadSide0 {
+  const idx_t* side;
+  __device__ idx_t operator()(int64_t i) const { return side[i] == 0 ? 1 : 0; }
+};
+
+// kdeg of each vertex (its same-side neighbours) at its position in its side.
+__global__ void k_rb_kdeg(int32_t n, const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                          const idx_t* __restrict__ side, const idx_t* __restrict__ pos0, idx_t* __restrict__ kdeg0,
+                          idx_t* __restrict__ kdeg1) {
+  RMB_GRID_STRIDE(v, n) {
+    const idx_t s = side[v];
+    int32_t c = 0;
+    for (int32_t j = xadj[v]; j < xadj[v + 1]; ++j) c += side[adj[j]] == s ? 1 : 0;
+    if (s == 0) kdeg0[pos0[v]] = c;
+    else kdeg1[v - pos0[v]] = c;
+  }
+}
+
+struct RbSide {
+  idx_t* xadj;
+  idx_t* adj;
+  idx_t* adjw;
+  idx_t* vwgt;
+  idx_t* orig;
+};
+
+__global__ void k_rb_fill(int32_t n, int32_t ncon, const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
+                          const idx_t* __restrict__ adjw, const idx_t* __restrict__ vwgt,
+                          const idx_t* __restrict__ orig, const idx_t* __restrict__ side,
+                          const idx_t* __restrict__ pos0, RbSide s0, RbSide s1) {
+  RMB_GRID_STRIDE(v, n) {
+    const idx_t s = side[v];
+    const RbSide& o = s == 0 ? s0 : s1;
+    const int32_t i = s == 0 ? pos0[v] : (int32_t)v - pos0[v];
+    int32_t k = o.xadj[i];
+    for (int32_t j = xadj[v]; j < xadj[v + 1]; ++j) {
+      const int32_t u = adj[j];
+      if (side[u] != s) continue;
+      o.adj[k] = s == 0 ? pos0[u] : u - pos0[u];
+      if (adjw) o.adjw[k] = adjw[j];
+      ++k;
+    }
+    if (vwgt)
+      for (int c = 0; c < ncon; ++c) o.vwgt[(int64_t)i * ncon + c] = vwgt[(int64_t)v * ncon + c];
+    o.orig[i] = orig[v];
+  }
+}
+
+// part[orig[v]] = offset (mode 0) or offset + min(v, nparts - 1) (mode 1).
+__global__ void k_rb_assign(int32_t n, const idx_t* __restrict__ orig, int32_t offset, int32_t nparts, int mode,
+                            idx_t* __restrict__ part) {
+  RMB_GRID_STRIDE(v, n) part[orig[v]] = mode == 0 ? offset : offset + min((int32_t)v, nparts - 1);
+}
+
+__global__ void k_rb_iota(int32_t n, idx_t* __restrict__ a) {
+  RMB_GRID_STRIDE(v, n) a[v] = (idx_t)v;
+}
+
+// multilevel_bisect (recursive.rs:133-187) of a device-resident subgraph into
+// d_side: two vertices or fewer by position; a subgraph without edges on the
+// host (as bisect does); otherwise a 2-way partition on the GPU.
+void bisect_dev(Engine& E, const DGraph& g, const std::vector<float>& tp2, const real_t* ubvec, const KwayOptions& o,
+                uint64_t seed, idx_t* d_side) {
+  cudaStream_t st = E.stream();
+  if (g.n <= 2) {  // recursive.rs:141-144
+    k_rb_iota<<<1, 32, 0, st>>>(g.n, d_side);
+    RMB_LAUNCH_CHECK();
+    RMB_CUDA(cudaStreamSynchronize(st));
+    return;
+  }
+  if (g.m == 0) {
+    HostGraph h;
+    h.n = g.n;
+    h.ncon = g.ncon;
+    h.xadj.assign((size_t)g.n + 1, 0);
+    h.has_vw = g.vwgt != nullptr;
+    if (h.has_vw) {
+      h.vwgt.resize((size_t)g.n * g.ncon);
+      download(E, h.vwgt.data(), g.vwgt, h.vwgt.size());
+      RMB_CUDA(cudaStreamSynchronize(st));
+    }
+    std::vector<idx_t> side;
+    bisect(E, h, tp2, ubvec, o, seed, side);
+    RMB_CUDA(cudaMemcpyAsync(d_side, side.data(), sizeof(idx_t) * side.size(), cudaMemcpyHostToDevice, st));
+    RMB_CUDA(cudaStreamSynchronize(st));
+    return;
+  }
+  KwayOptions ob = o;
+  ob.seed = seed;
+  ob.ncuts = 1;
+  ob.parallel_attempts = 0;
+  ob.bisect_fm2 = 1;  // refine_2way (recursive.rs:184-186): the 2-way FM of fm.rs for rtype Fm
+  int32_t obj = 0;
+  E.partition_kway(g, 2, tp2.data(), ubvec, ob, d_side, &obj, nullptr);
+}
+
+// rb_recurse (recursive.rs:61-131) level by level on the device (targets,
+// seeds and direct assignments as described above). root.g and root.orig are
+// device arrays; d_part gets the parts.
+void rb_levels_dev(Engine& E, DevNode root, const real_t* ubvec, const KwayOptions& o, idx_t* d_part) {
+  cudaStream_t st = E.stream();
+  const int32_t n_in = root.g.n;
+  const int64_t m_in = root.g.m;
+  const int nc = root.g.ncon;
+  const bool has_w = root.g.adjwgt != nullptr, has_vw = root.g.vwgt != nullptr;
+  // Two regions, alternating by depth, hold the subgraphs of a level (the
+  // children of one level sum to at most the input's vertices and entries).
+  const size_t max_children = 2 * (size_t)std::max(root.nparts, 2) + 2;
+  const size_t region_bytes = sizeof(idx_t) * (2 * ((size_t)n_in + max_children) + 2 * (size_t)m_in * (has_w ? 2 : 1) +
+                                               2 * (size_t)n_in * (has_vw ? nc : 0) + 2 * (size_t)n_in) +
+                              max_children * 5 * 256 + 256;
+  char* region[2] = {E.arena().alloc<char>(region_bytes), E.arena().alloc<char>(region_bytes)};
+  std::vector<DevNode> frontier;
   frontier.push_back(std::move(root));
+  int depth = 0;
+  int dev = 0;
+  RMB_CUDA(cudaGetDevice(&dev));
+  WorkerPool& pool = pool_for_device(dev);
   while (!frontier.empty()) {
-    std::vector<RbNode*> split;
-    std::vector<BisectJob> jobs;
-    for (RbNode& nd : frontier) {
-      if (nd.nparts == 1) {
-        for (int32_t v : nd.orig) part[v] = nd.offset;
-        continue;
-      }
-      if (nd.g.n <= nd.nparts) {
-        for (int32_t v = 0; v < nd.g.n; ++v) part[nd.orig[v]] = nd.offset + std::min(v, nd.nparts - 1);
+    std::vector<DevNode*> split;
+    for (DevNode& nd : frontier) {
+      if (nd.nparts == 1 || nd.g.n <= nd.nparts) {
+        k_rb_assign<<<grid_for(nd.g.n, 256), 256, 0, st>>>(nd.g.n, nd.orig, nd.offset, nd.nparts,
+                                                           nd.nparts == 1 ? 0 : 1, d_part);
+        RMB_LAUNCH_CHECK();
         continue;
       }
       split.push_back(&nd);
     }
-    jobs.resize(split.size());
-    std::vector<std::vector<float>> lws(split.size()), rws(split.size());
-    for (size_t i = 0; i < split.size(); ++i) {
-      const RbNode& nd = *split[i];
-      const int32_t k1 = nd.nparts / 2, nc = nd.g.ncon;
-      std::vector<float>& lw = lws[i];
-      std::vector<float>& rw = rws[i];
-      lw.assign(nc, 0.0f);
-      rw.assign(nc, 0.0f);
+    if (split.empty()) break;
+    const size_t S = split.size();
+    Arena::Mark mk = E.arena().mark();
+    std::vector<std::vector<float>> tp2(S), lws(S), rws(S);
+    std::vector<idx_t*> d_side(S);
+    for (size_t i = 0; i < S; ++i) {
+      const DevNode& nd = *split[i];
+      const int32_t k1 = nd.nparts / 2;
+      lws[i].assign(nc, 0.0f);
+      rws[i].assign(nc, 0.0f);
       for (int c = 0; c < nc; ++c) {
-        for (int32_t t = c; t < k1 * nc; t += nc) lw[c] += nd.tp[t];
-        for (int32_t t = k1 * nc + c; t < nd.nparts * nc; t += nc) rw[c] += nd.tp[t];
+        for (int32_t t = c; t < k1 * nc; t += nc) lws[i][c] += nd.tp[t];
+        for (int32_t t = k1 * nc + c; t < nd.nparts * nc; t += nc) rws[i][c] += nd.tp[t];
       }
-      const float total = lw[0] + rw[0];
-      for (int c = 0; c < nc; ++c) jobs[i].tp2.push_back(lw[c] / total);
-      for (int c = 0; c < nc; ++c) jobs[i].tp2.push_back(rw[c] / total);
-      jobs[i].g = &nd.g;
-      jobs[i].seed = o.seed == 0 ? 0 : o.seed + nd.heap;
+      const float total = lws[i][0] + rws[i][0];
+      for (int c = 0; c < nc; ++c) tp2[i].push_back(lws[i][c] / total);
+      for (int c = 0; c < nc; ++c) tp2[i].push_back(rws[i][c] / total);
+      d_side[i] = E.arena().alloc<idx_t>((size_t)nd.g.n);
     }
-    bisect_all(jobs, ubvec, o);
-    std::vector<RbNode> next;
-    for (size_t i = 0; i < split.size(); ++i) {
-      const RbNode& nd = *split[i];
-      const int32_t k1 = nd.nparts / 2, k2 = nd.nparts - k1, nc = nd.g.ncon;
-      for (int side = 0; side < 2; ++side) {
-        RbNode ch;
-        std::vector<int32_t> n2o;
-        ch.g = extract_sub(nd.g, jobs[i].part, side, n2o);
-        ch.orig.resize(n2o.size());
-        for (size_t t = 0; t < n2o.size(); ++t) ch.orig[t] = nd.orig[n2o[t]];
-        ch.nparts = side == 0 ? k1 : k2;
-        ch.offset = side == 0 ? nd.offset : nd.offset + k1;
-        const float div = side == 0 ? lws[i][0] : rws[i][0];
-        for (int32_t t = side == 0 ? 0 : k1 * nc; t < (side == 0 ? k1 * nc : nd.nparts * nc); ++t)
+    RMB_CUDA(cudaStreamSynchronize(st));  // the level's subgraphs are complete before the workers read them
+    {
+      std::vector<std::future<int>> fut;
+      for (size_t i = 0; i < S; ++i) {
+        const DevNode* nd = split[i];
+        const std::vector<float>* t2 = &tp2[i];
+        idx_t* ds = d_side[i];
+        const uint64_t seed = o.seed == 0 ? 0 : o.seed + nd->heap;
+        fut.push_back(pool.submit(footprint_bytes(nd->g.n, nd->g.m, 2, nc), [nd, t2, ds, seed, ubvec, &o](Engine& W) {
+          bisect_dev(W, nd->g, *t2, ubvec, o, seed, ds);
+          return 1;
+        }));
+      }
+      int rc = 1;
+      for (auto& f : fut) {
+        const int r = f.get();
+        if (r != 1 && rc == 1) rc = r;
+      }
+      if (rc != 1) throw Error(rc, "a bisection failed");
+    }
+    // Side sizes: n0 per node (one read-back for the level).
+    idx_t* d_cnt = E.arena().alloc<idx_t>(S);
+    std::vector<idx_t*> pos0(S);
+    for (size_t i = 0; i < S; ++i) {
+      pos0[i] = E.arena().alloc<idx_t>((size_t)split[i]->g.n);
+      exclusive_scan<idx_t>(LoadSide0{d_side[i]}, StoreArr<idx_t>{pos0[i]}, split[i]->g.n, d_cnt + i, E.arena(), st);
+    }
+    std::vector<idx_t> n0(S);
+    download(E, n0.data(), d_cnt, S);
+    RMB_CUDA(cudaStreamSynchronize(st));
+    // Children's row offsets (in this depth's region) and entry counts.
+    char* reg = region[depth & 1];
+    size_t off = 0;
+    auto take = [&](size_t count) {
+      idx_t* p = reinterpret_cast<idx_t*>(reg + off);
+      off += (count * sizeof(idx_t) + 255) & ~(size_t)255;
+      if (off > region_bytes) throw Error(-4, "recursion region overflow");
+      return p;
+    };
+    std::vector<std::array<DevNode, 2>> kids(S);
+    for (size_t i = 0; i < S; ++i) {
+      const DevNode& nd = *split[i];
+      const int32_t ns[2] = {n0[i], nd.g.n - n0[i]};
+      idx_t* kdeg[2] = {E.arena().alloc<idx_t>((size_t)ns[0] + 1), E.arena().alloc<idx_t>((size_t)ns[1] + 1)};
+      k_rb_kdeg<<<grid_for(nd.g.n, 256), 256, 0, st>>>(nd.g.n, nd.g.xadj, nd.g.adjncy, d_side[i], pos0[i], kdeg[0],
+                                                       kdeg[1]);
+      RMB_LAUNCH_CHECK();
+      for (int sd = 0; sd < 2; ++sd) {
+        DevNode& ch = kids[i][sd];
+        ch.g.n = ns[sd];
+        ch.g.ncon = nc;
+        idx_t* cx = take((size_t)ns[sd] + 1);
+        exclusive_scan_arr<idx_t>(kdeg[sd], cx, ns[sd], cx + ns[sd], E.arena(), st);
+        ch.g.xadj = cx;
+      }
+    }
+    std::vector<idx_t> ms(2 * S);
+    for (size_t i = 0; i < S; ++i)
+      for (int sd = 0; sd < 2; ++sd)
+        download(E, &ms[2 * i + sd], kids[i][sd].g.xadj + kids[i][sd].g.n, 1);
+    RMB_CUDA(cudaStreamSynchronize(st));
+    std::vector<DevNode> next;
+    for (size_t i = 0; i < S; ++i) {
+      const DevNode& nd = *split[i];
+      const int32_t k1 = nd.nparts / 2, k2 = nd.nparts - k1;
+      RbSide so[2];
+      for (int sd = 0; sd < 2; ++sd) {
+        DevNode& ch = kids[i][sd];
+        ch.g.m = ms[2 * i + sd];
+        idx_t* ca = take((size_t)ch.g.m);
+        idx_t* cw = has_w ? take((size_t)ch.g.m) : nullptr;
+        idx_t* cv = has_vw ? take((size_t)ch.g.n * nc) : nullptr;
+        ch.orig = take((size_t)ch.g.n);
+        ch.g.adjncy = ca;
+        ch.g.adjwgt = cw;
+        ch.g.vwgt = cv;
+        so[sd] = RbSide{const_cast<idx_t*>(ch.g.xadj), ca, cw, cv, ch.orig};
+        ch.nparts = sd == 0 ? k1 : k2;
+        ch.offset = sd == 0 ? nd.offset : nd.offset + k1;
+        const float div = sd == 0 ? lws[i][0] : rws[i][0];
+        for (int32_t t = sd == 0 ? 0 : k1 * nc; t < (sd == 0 ? k1 * nc : nd.nparts * nc); ++t)
           ch.tp.push_back(nd.tp[t] / div);
-        ch.heap = 2 * nd.heap + 1 + (uint64_t)side;
-        next.push_back(std::move(ch));
+        ch.heap = 2 * nd.heap + 1 + (uint64_t)sd;
       }
+      k_rb_fill<<<grid_for(nd.g.n, 256), 256, 0, st>>>(nd.g.n, nc, nd.g.xadj, nd.g.adjncy, nd.g.adjwgt, nd.g.vwgt,
+                                                       nd.orig, d_side[i], pos0[i], so[0], so[1]);
+      RMB_LAUNCH_CHECK();
+      next.push_back(std::move(kids[i][0]));
+      next.push_back(std::move(kids[i][1]));
     }
+    RMB_CUDA(cudaStreamSynchronize(st));  // the children are written before the level's scratch is dropped
+    E.arena().reset_to(mk);
     frontier = std::move(next);
+    ++depth;
   }
+  RMB_CUDA(cudaStreamSynchronize(st));
 }
 
 int recursive_host(const idx_t* nvtxs, const idx_t* ncon, const idx_t* xadj, const idx_t* adjncy, const idx_t* vwgt,
@@ -451,46 +649,40 @@ int recursive_host(const idx_t* nvtxs, const idx_t* ncon, const idx_t* xadj, con
   apply_tuning(o);
   Engine& E = engine_for_current_device();
   std::lock_guard<std::mutex> lk(E.mu);
-  {
-    // validate_csr (src/graph/validate.rs:16-142) on the device, as Graph::new does.
-    Arena::Mark mk = E.arena().mark();
-    struct Rewind {
-      Engine& E;
-      Arena::Mark m;
-      ~Rewind() { E.arena().reset_to(m); }
-    } rw{E, mk};
-    DGraph g;
-    g.n = n;
-    g.m = ne;
-    g.ncon = nc;
-    g.xadj = upload(E, xadj, (size_t)n + 1);
-    g.adjncy = upload(E, adjncy, (size_t)ne);
-    g.vwgt = upload(E, vwgt, (size_t)n * nc);
-    g.adjwgt = upload(E, adjwgt, (size_t)ne);
-    if (validate_device(g, E.arena(), E.stream(), E.host_scratch()) != 0)
-      throw Error(METIS_ERROR_INPUT, "graph failed validation");
-  }
-  if (np > n) return METIS_ERROR_INPUT;  // recursive.rs:22-26
-  HostGraph g;
+  Arena::Mark mk = E.arena().mark();
+  struct Rewind {
+    Engine& E;
+    Arena::Mark m;
+    ~Rewind() { E.arena().reset_to(m); }
+  } rw{E, mk};
+  // The input on the device: validate_csr (src/graph/validate.rs:16-142) as
+  // Graph::new does, then the root of the recursion, read in place.
+  DGraph g;
   g.n = n;
+  g.m = ne;
   g.ncon = nc;
-  g.xadj.assign(xadj, xadj + n + 1);
-  g.adj.assign(adjncy, adjncy + ne);
-  g.has_vw = vwgt != nullptr;
-  g.has_w = adjwgt != nullptr;
-  if (vwgt) g.vwgt.assign(vwgt, vwgt + (size_t)n * nc);
-  if (adjwgt) g.adjw.assign(adjwgt, adjwgt + ne);
+  g.xadj = upload(E, xadj, (size_t)n + 1);
+  g.adjncy = upload(E, adjncy, (size_t)ne);
+  g.vwgt = upload(E, vwgt, (size_t)n * nc);
+  g.adjwgt = upload(E, adjwgt, (size_t)ne);
+  if (validate_device(g, E.arena(), E.stream(), E.host_scratch()) != 0)
+    throw Error(METIS_ERROR_INPUT, "graph failed validation");
+  if (np > n) return METIS_ERROR_INPUT;  // recursive.rs:22-26
   std::vector<float> tp;
   if (tpwgts) tp.assign(tpwgts, tpwgts + (size_t)np * nc);
   else tp.assign((size_t)np * nc, 1.0f / (float)np);  // recursive.rs:38-43
-  std::vector<idx_t> out((size_t)n, 0);
-  RbNode root;
-  root.g = std::move(g);
-  root.orig.resize(n);
-  for (int32_t v = 0; v < n; ++v) root.orig[v] = v;
+  DevNode root;
+  root.g = g;
+  root.orig = E.arena().alloc<idx_t>((size_t)n);
+  k_rb_iota<<<grid_for(n, 256), 256, 0, E.stream()>>>(n, root.orig);
+  RMB_LAUNCH_CHECK();
   root.nparts = np;
   root.tp = std::move(tp);
-  rb_levels(std::move(root), ubvec, o, out);
+  idx_t* d_part = E.arena().alloc<idx_t>((size_t)n);
+  rb_levels_dev(E, std::move(root), ubvec, o, d_part);
+  std::vector<idx_t> out((size_t)n, 0);
+  download(E, out.data(), d_part, (size_t)n);
+  RMB_CUDA(cudaStreamSynchronize(E.stream()));
   // edge_cut (src/graph/mod.rs:123-137): i32 sum over both directions, / 2.
   uint32_t cut = 0;
   for (int32_t v = 0; v < n; ++v)
