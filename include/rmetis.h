@@ -90,11 +90,13 @@ RMETIS_API int RMETIS_PartGraphKway(const idx_t *nvtxs, const idx_t *ncon, const
  * src/partition/recursive.rs:12-187). Same arguments, ownership and return
  * codes as RMETIS_PartGraphKway; the options are decoded the same way, and the
  * reference's Options::for_recursive() (iptype MetisRb, rtype Fm, ufactor 1)
- * is what its callers pass. The recursion, the f32 target arithmetic and the
- * subgraph extraction follow the reference on the host; each bisection is a
- * 2-way multilevel partition on the GPU (coarsening to 40 vertices, grow
- * trials, refinement), and the bisections of one recursion level run
- * concurrently on the device's worker pool. With rtype Fm every bisection is
+ * is what its callers pass. The recursion and the f32 target arithmetic
+ * follow the reference on the host; the subgraphs stay on the device (the
+ * input is uploaded once, both sides of every bisection are extracted there as
+ * extract_subgraph does), each bisection is a 2-way multilevel partition on
+ * the GPU (coarsening to 40 vertices, grow trials, refinement), and the
+ * bisections of one recursion level run concurrently on the device's worker
+ * pool. With rtype Fm every bisection is
  * refined by the reference's 2-way FM rule (src/refine/fm.rs: negative moves
  * and a rollback to the lowest cut) in parallel rounds (RMETIS_GPU_Fm2Refine).
  * Differences: the order of those moves, and the bisection at position h of the recursion tree (root 0,
