@@ -57,31 +57,46 @@ __device__ void gain_body(Lanes L, const idx_t* __restrict__ xadj, const idx_t* 
       rp[i] = -1;
       rw[i] = 0;
     }
-    for (int32_t j = s; j < e; ++j) {
-      const int32_t pu = part[adj[j]];
-      const uint32_t w = (uint32_t)(HAS_W ? adjwgt[j] : 1);
-      if (pu == pv) {
-        wf += w;
-      } else {
-        boundary = true;
-        bool found = false;
+    // Four entries at a time: their adjncy and part gathers are in flight
+    // together; they are then taken in row order.
+    for (int32_t j0 = s; j0 < e; j0 += 4) {
+      int32_t pq[4];
+      uint32_t wq[4];
 #pragma unroll
-        for (int i = 0; i < kRegParts; ++i)
-          if (rp[i] == pu) {
-            rw[i] += w;
-            found = true;
-          }
-        if (!found) {
-          if (cnt < kRegParts) {
+      for (int q = 0; q < 4; ++q) {
+        pq[q] = j0 + q < e ? adj[j0 + q] : -1;
+        wq[q] = j0 + q < e ? (uint32_t)(HAS_W ? adjwgt[j0 + q] : 1) : 0u;
+      }
 #pragma unroll
-            for (int i = 0; i < kRegParts; ++i)
-              if (i == cnt) {
-                rp[i] = pu;
-                rw[i] = w;
-              }
-            ++cnt;
-          } else {
-            spill = true;
+      for (int q = 0; q < 4; ++q) pq[q] = pq[q] >= 0 ? part[pq[q]] : -1;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (j0 + q >= e) break;
+        const int32_t pu = pq[q];
+        const uint32_t w = wq[q];
+        if (pu == pv) {
+          wf += w;
+        } else {
+          boundary = true;
+          bool found = false;
+#pragma unroll
+          for (int i = 0; i < kRegParts; ++i)
+            if (rp[i] == pu) {
+              rw[i] += w;
+              found = true;
+            }
+          if (!found) {
+            if (cnt < kRegParts) {
+#pragma unroll
+              for (int i = 0; i < kRegParts; ++i)
+                if (i == cnt) {
+                  rp[i] = pu;
+                  rw[i] = w;
+                }
+              ++cnt;
+            } else {
+              spill = true;
+            }
           }
         }
       }

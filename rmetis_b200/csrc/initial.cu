@@ -23,6 +23,10 @@ namespace rmb {
 // it fits, else in the trial's global scratch. A part's weight only changes
 // during its own turn, so the parts that may grow in a round are known at the
 // round's start.
+// Row chunks of 32 whose neighbour ids and labels are loaded together (a
+// hub's row is otherwise one long chain of dependent loads).
+constexpr int kGrowGroup = 8;
+
 template <bool HAS_VW>
 __device__ void grow_body(const idx_t* __restrict__ xadj, const idx_t* __restrict__ adj,
                           const idx_t* __restrict__ vwgt, int32_t n, int32_t ncon, int32_t k,
@@ -83,24 +87,24 @@ __device__ void grow_body(const idx_t* __restrict__ xadj, const idx_t* __restric
           const int32_t v = qh;
           qh = next[v];
           const int32_t e = __ldg(&xadj[v + 1]);
-          // The row is read 4 chunks of 32 at a time: neighbours and their
+          // The row is read kGrowGroup chunks of 32 at a time: neighbours and their
           // part labels are loaded together, then the chunks are claimed in
           // order. A claim earlier in the group may have taken a neighbour that
           // is listed again later in the row, so after one the later
           // candidates' labels are read again.
-          for (int32_t b0 = __ldg(&xadj[v]); b0 < e; b0 += 4 * 32) {
-            int32_t uu[4];
-            bool cc[4];
+          for (int32_t b0 = __ldg(&xadj[v]); b0 < e; b0 += kGrowGroup * 32) {
+            int32_t uu[kGrowGroup];
+            bool cc[kGrowGroup];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < kGrowGroup; ++q) {
               const int32_t j = b0 + q * 32 + lane;
               uu[q] = j < e ? __ldg(&adj[j]) : -1;
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) cc[q] = uu[q] >= 0 && part[uu[q]] == -1;
+            for (int q = 0; q < kGrowGroup; ++q) cc[q] = uu[q] >= 0 && part[uu[q]] == -1;
             bool claimed = false;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < kGrowGroup; ++q) {
               if (b0 + q * 32 >= e) break;
               const int32_t u = uu[q];
               bool cand = cc[q];
