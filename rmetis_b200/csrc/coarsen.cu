@@ -57,11 +57,22 @@ __device__ __forceinline__ void propose_body(const idx_t* xadj, const idx_t* adj
     if (e - s > kHeavyDegree) continue;
     EdgeKey best{INT32_MIN, 0u, -1};
     bool have = false;
-    for (int32_t j = s; j < e; ++j) {
-      const int32_t u = adj[j];
-      if (match[u] >= 0) continue;
-      EdgeKey k{MODE == 1 ? (HAS_W ? adjwgt[j] : 1) : 0, edge_hash(seed, (int32_t)v, u), u};
-      if (!have || k.better(best)) { best = k; have = true; }
+    // Four entries at a time: their adjncy and match gathers are in flight
+    // together; they are then taken in row order.
+    for (int32_t j0 = s; j0 < e; j0 += 4) {
+      int32_t uq[4], mq[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) uq[q] = j0 + q < e ? adj[j0 + q] : -1;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) mq[q] = uq[q] >= 0 ? match[uq[q]] : 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (j0 + q >= e) break;
+        const int32_t u = uq[q];
+        if (mq[q] >= 0) continue;
+        EdgeKey k{MODE == 1 ? (HAS_W ? adjwgt[j0 + q] : 1) : 0, edge_hash(seed, (int32_t)v, u), u};
+        if (!have || k.better(best)) { best = k; have = true; }
+      }
     }
     prop[v] = have ? best.u : -1;
   }
@@ -454,21 +465,30 @@ __device__ __forceinline__ void contract_thread_body(const idx_t* xadj, const id
       const int32_t src = mbr == 0 ? mem0[c] : mem1[c];
       if (src < 0) continue;
       const int32_t s = xadj[src], e = xadj[src + 1];
-      for (int32_t j = s; j < e; ++j) {
-        const int32_t cu = cmap[adj[j]];
-        if (cu == (int32_t)c) continue;
-        const int32_t w = HAS_W ? adjwgt[j] : 1;
-        bool found = false;
+      for (int32_t j0 = s; j0 < e; j0 += 4) {
+        int32_t cq[4];
 #pragma unroll
-        for (int i = 0; i < T; ++i) {
-          if (i < cnt && keys[i] == cu) { wts[i] += w; found = true; }
-        }
-        if (!found) {
+        for (int q = 0; q < 4; ++q) cq[q] = j0 + q < e ? adj[j0 + q] : -1;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) cq[q] = cq[q] >= 0 ? cmap[cq[q]] : -1;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (j0 + q >= e) break;
+          const int32_t cu = cq[q];
+          if (cu == (int32_t)c) continue;
+          const int32_t w = HAS_W ? adjwgt[j0 + q] : 1;
+          bool found = false;
 #pragma unroll
           for (int i = 0; i < T; ++i) {
-            if (i == cnt) { keys[i] = cu; wts[i] = w; }
+            if (i < cnt && keys[i] == cu) { wts[i] += w; found = true; }
           }
-          ++cnt;
+          if (!found) {
+#pragma unroll
+            for (int i = 0; i < T; ++i) {
+              if (i == cnt) { keys[i] = cu; wts[i] = w; }
+            }
+            ++cnt;
+          }
         }
       }
     }
