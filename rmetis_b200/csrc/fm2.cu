@@ -61,12 +61,21 @@ __global__ void k_fm2_gain(int32_t n, const idx_t* __restrict__ xadj, const idx_
     const int32_t pv = part[v];
     uint32_t wf = 0, wt = 0;
     bool bnd = false;
-    for (int32_t j = s; j < e; ++j) {
-      const uint32_t w = (uint32_t)(HAS_W ? adjwgt[j] : 1);
-      if (part[adj[j]] == pv) wf += w;
-      else {
-        wt += w;
-        bnd = true;
+    for (int32_t j0 = s; j0 < e; j0 += 4) {
+      int32_t pq[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) pq[q] = j0 + q < e ? adj[j0 + q] : -1;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) pq[q] = pq[q] >= 0 ? part[pq[q]] : -1;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (j0 + q >= e) break;
+        const uint32_t w = (uint32_t)(HAS_W ? adjwgt[j0 + q] : 1);
+        if (pq[q] == pv) wf += w;
+        else {
+          wt += w;
+          bnd = true;
+        }
       }
     }
     const bool cand = bnd && state[v] == kFree;

@@ -1606,13 +1606,23 @@ __device__ void fm_select_body(Lanes L, int32_t n, const idx_t* __restrict__ xad
       out = 1;
       const int32_t pv = part[v];
       const int32_t s = xadj[v], e = xadj[v + 1];
-      for (int32_t j = s; j < e; ++j) {
-        const int32_t u = adj[j];
-        if (u == (int32_t)v || part[u] == pv) continue;
-        const int32_t gu = fm_gain_of(u, xadj, mover, ncand, cand_g, state);
-        if (gu > gv || (gu == gv && u < (int32_t)v)) {
-          out = 0;
-          break;
+      // Four neighbours at a time: their ids and parts are gathered together,
+      // then compared in row order (the first better one ends the scan).
+      for (int32_t j0 = s; j0 < e && out; j0 += 4) {
+        int32_t uq[4], pq[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) uq[q] = j0 + q < e ? adj[j0 + q] : -1;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) pq[q] = uq[q] >= 0 ? part[uq[q]] : pv;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int32_t u = uq[q];
+          if (u < 0 || u == (int32_t)v || pq[q] == pv) continue;
+          const int32_t gu = fm_gain_of(u, xadj, mover, ncand, cand_g, state);
+          if (gu > gv || (gu == gv && u < (int32_t)v)) {
+            out = 0;
+            break;
+          }
         }
       }
     }
