@@ -26,6 +26,7 @@
 // largest graphs are started first (blocks in descending size), which keeps
 // the device busy while they finish.
 #include <algorithm>
+#include <climits>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -121,6 +122,55 @@ __global__ void k_batch_cut(const CutJob* __restrict__ jobs) {
   }
   acc = warp_sum(acc);
   if ((threadIdx.x & 31) == 0 && acc) atomicAdd(J.cut, acc);
+}
+
+// The thresholds of every level of a graph (Engine::thresholds with uniform
+// targets: t = total / k for every part, the same f64 expression) written on
+// the device: [level][feas, over, grow][k][ncon]. tot: [level][ncon], the i32
+// level totals.
+struct ThrJob {
+  long long* thr;
+  const int32_t* tot;
+  int32_t k, ncon, nlevels;
+};
+
+__device__ void threshold_values_dev(double t, double ub, long long* feas, long long* over, long long* grow) {
+  const double lim = 9.0e18;
+  const double x = t * ub;
+  if (isnan(x)) {
+    *feas = LLONG_MIN;
+    *over = LLONG_MAX;
+  } else if (x >= lim) {
+    *feas = LLONG_MAX;
+    *over = LLONG_MAX;
+  } else if (x <= -lim) {
+    *feas = LLONG_MIN;
+    *over = LLONG_MIN;
+  } else {
+    const long long f = (long long)floor(x);
+    *feas = f;
+    *over = f;
+  }
+  if (isnan(t) || t >= lim) *grow = LLONG_MAX;
+  else if (t <= -lim) *grow = LLONG_MIN;
+  else *grow = (long long)ceil(t);
+}
+
+struct UbVec {
+  double v[8];
+};
+
+__global__ void k_batch_thresholds(const ThrJob* __restrict__ jobs, UbVec ub) {
+  const ThrJob& J = jobs[blockIdx.x];
+  const int64_t K = (int64_t)J.k * J.ncon;
+  const double inv = 1.0 / (double)J.k;
+  for (int64_t idx = threadIdx.x; idx < (int64_t)J.nlevels * K; idx += blockDim.x) {
+    const int64_t l = idx / K, i = idx - l * K;
+    const int c = (int)(i % J.ncon);
+    const double t = inv * (double)J.tot[l * J.ncon + c];
+    long long* h = J.thr + 3 * K * l;
+    threshold_values_dev(t, ub.v[c], &h[i], &h[K + i], &h[2 * K + i]);
+  }
 }
 
 }  // namespace
@@ -336,25 +386,26 @@ void Engine::partition_kway_batch(std::vector<BatchItem>& items, const float* ub
     if (it.g.vwgt)
       for (int c = 0; c < ncon; ++c)
         total0[c] = (int32_t)(uint32_t)(unsigned long long)totals[(size_t)b * ncon + c];
-    std::vector<long long> thr(3 * K * (size_t)(L + 1));
+    // The thresholds are filled on the device (k_batch_thresholds); here one
+    // value per level and constraint decides the slack width (all parts have
+    // the same target).
+    std::vector<int32_t> ltot((size_t)(L + 1) * ncon);
     for (int l = 0; l <= L; ++l) {
       std::vector<long long> tot(ncon);
-      for (int c = 0; c < ncon; ++c)
+      for (int c = 0; c < ncon; ++c) {
         tot[c] = P.has_vw[l] ? total0[c] : (!it.g.vwgt && o.summed_unit_weights) ? it.g.n : P.levels[l].n;
-      long long* h = thr.data() + 3 * K * (size_t)l;
-      for (int p = 0; p < k; ++p)
-        for (int c = 0; c < ncon; ++c) {
-          const double tw = (1.0 / (double)k) * (double)(int32_t)tot[c];
-          const size_t i = (size_t)p * ncon + c;
-          threshold_values(tw, ub[c], &h[i], &h[K + i], &h[2 * K + i]);
-        }
-      P.small.push_back(weights_fit_int32(tot.data(), ncon, h, h + K, K));
+        ltot[(size_t)l * ncon + c] = (int32_t)tot[c];
+      }
+      std::vector<long long> f1(ncon), o1(ncon), g1(ncon);
+      for (int c = 0; c < ncon; ++c)
+        threshold_values((1.0 / (double)k) * (double)(int32_t)tot[c], ub[c], &f1[c], &o1[c], &g1[c]);
+      P.small.push_back(weights_fit_int32(tot.data(), ncon, f1.data(), o1.data(), (size_t)ncon));
       const DGraph& lg = P.levels[l];
       const bool fused = o.fused_max_n > 0 && lg.n <= o.fused_max_n &&
                          lg.m <= (int64_t)o.fused_edge_factor * o.fused_max_n;
       P.admit.push_back(!fused && lg.n > o.exact_max_n && admit_supported(k, ncon));
     }
-    o_thr[b] = s2.put(thr.data(), thr.size());
+    o_thr[b] = s2.put(ltot.data(), ltot.size());
     // Grow seeds of every trial (grow.rs:26-32, run_attempt's draws).
     const int32_t cn = P.levels[L].n;
     std::vector<int32_t> seeds((size_t)T * k);
@@ -401,6 +452,7 @@ void Engine::partition_kway_batch(std::vector<BatchItem>& items, const float* ub
     const int32_t n0 = it.g.n;
     const int64_t m0 = it.g.m;
     const int32_t cn = P.levels[L].n;
+    P.thr = c.take<long long>(3 * K * (size_t)(L + 1));
     P.trial_parts = c.take<idx_t>((size_t)T * cn);
     P.trial_cuts = c.take<long long>((size_t)T);
     const size_t gb = grow_scratch_bytes(cn, k, ncon);
@@ -458,6 +510,7 @@ void Engine::partition_kway_batch(std::vector<BatchItem>& items, const float* ub
   }
   // ---- 4: grow trials ----
   std::vector<GrowJob> gj;
+  std::vector<ThrJob> thr_jobs;
   std::vector<int32_t> block_job;
   size_t grow_dyn = 0;
   std::vector<int32_t> planned;  // planned graphs, largest first
@@ -479,7 +532,7 @@ void Engine::partition_kway_batch(std::vector<BatchItem>& items, const float* ub
     j.k = it.k;
     j.trials = T;
     j.seeds = reinterpret_cast<const idx_t*>(d_s2 + o_seed[b]);
-    j.grow_tgt = reinterpret_cast<const long long*>(d_s2 + o_thr[b]) + 3 * (size_t)it.k * ncon * L + 2 * (size_t)it.k * ncon;
+    j.grow_tgt = P.thr + 3 * (size_t)it.k * ncon * L + 2 * (size_t)it.k * ncon;
     j.parts = P.trial_parts;
     j.cuts = P.trial_cuts;
     j.use_smem = gb <= kGrowSmemCap ? 1 : 0;
@@ -489,7 +542,13 @@ void Engine::partition_kway_batch(std::vector<BatchItem>& items, const float* ub
     if (j.use_smem) grow_dyn = std::max(grow_dyn, gb);
     for (int tr = 0; tr < T; ++tr) block_job.push_back((int32_t)gj.size());
     gj.push_back(j);
-    P.thr = reinterpret_cast<long long*>(d_s2 + o_thr[b]);
+    ThrJob tj;
+    tj.thr = P.thr;
+    tj.tot = reinterpret_cast<const int32_t*>(d_s2 + o_thr[b]);
+    tj.k = it.k;
+    tj.ncon = ncon;
+    tj.nlevels = L + 1;
+    thr_jobs.push_back(tj);
   }
 
   // ---- 5: the refinement steps (coarsest levels first) ----
@@ -597,12 +656,17 @@ void Engine::partition_kway_batch(std::vector<BatchItem>& items, const float* ub
   const auto t_planned = clock::now();
   Staging s3;
   const size_t o_gj = s3.put(gj.data(), gj.size());
+  const size_t o_tj = s3.put(thr_jobs.data(), thr_jobs.size());
   const size_t o_bj = s3.put(block_job.data(), block_job.size());
   const size_t o_jobs = s3.put(jobs.data(), jobs.size());
   const size_t o_cj = s3.put(cj.data(), cj.size());
   char* d_s3 = s3.host.empty() ? nullptr : arena_.alloc<char>(s3.host.size());
   if (!planned.empty()) {
     RMB_CUDA(cudaMemcpyAsync(d_s3, s3.host.data(), s3.host.size(), cudaMemcpyHostToDevice, st));
+    UbVec ubv{};
+    for (int c = 0; c < ncon && c < 8; ++c) ubv.v[c] = ub[c];
+    k_batch_thresholds<<<(int)thr_jobs.size(), 256, 0, st>>>(reinterpret_cast<const ThrJob*>(d_s3 + o_tj), ubv);
+    RMB_LAUNCH_CHECK();
     nvtxRangePushA("batch grow");
     grow_trials_batch(reinterpret_cast<const GrowJob*>(d_s3 + o_gj), reinterpret_cast<const int32_t*>(d_s3 + o_bj),
                       (int)block_job.size(), grow_dyn, st);
