@@ -604,11 +604,18 @@ __device__ __forceinline__ void contract_warp_body(const idx_t* xadj, const idx_
 
 // Gather the merged rows into the final coarse CSR: a warp takes 32 coarse
 // vertices and strides over their contiguous scratch range. xs: 33 shared
-// ints of this warp. W runs over warps.
+// ints of this warp. W runs over warps. With VEC, each lane reads four
+// scratch entries per 16-byte load (int4, both scratch arrays 16-byte aligned,
+// checked here; the grid path allocates them with three entries of slack so
+// that the last group of a range stays inside its allocation) and locates
+// their rows with one binary search per group.
+template <bool VEC>
 __device__ __forceinline__ void compact_body(int32_t cn, const idx_t* ub_off, const idx_t* cdeg, const idx_t* cxadj,
                                              const idx_t* tmp_adj, const idx_t* tmp_w, idx_t* cadj, idx_t* cw,
                                              int32_t* xs, Lanes W) {
   const int lane = threadIdx.x & 31;
+  const bool vec =
+      VEC && ((reinterpret_cast<uintptr_t>(tmp_adj) | reinterpret_cast<uintptr_t>(tmp_w)) & 15) == 0;
   RMB_FOR(w, ceil_div(cn, 32), W) {
     const int32_t v0 = (int32_t)w * 32;
     const int32_t vend = min(v0 + 32, cn);
@@ -617,18 +624,46 @@ __device__ __forceinline__ void compact_body(int32_t cn, const idx_t* ub_off, co
     if (lane == 0) xs[cnt] = ub_off[vend];
     __syncwarp();
     const int32_t e0 = xs[0], e1 = xs[cnt];
-    for (int32_t p = e0 + lane; p < e1; p += 32) {
-      int lo = 0, hi = cnt;
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (xs[mid] <= p) lo = mid; else hi = mid;
+    if (vec) {
+      for (int32_t q = (e0 & ~3) + 4 * lane; q < e1; q += 128) {
+        const int4 a4 = *reinterpret_cast<const int4*>(tmp_adj + q);
+        const int4 w4 = *reinterpret_cast<const int4*>(tmp_w + q);
+        const int32_t av[4] = {a4.x, a4.y, a4.z, a4.w};
+        const int32_t wv[4] = {w4.x, w4.y, w4.z, w4.w};
+        const int32_t p0 = max(q, e0);
+        int lo = 0, hi = cnt;
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (xs[mid] <= p0) lo = mid; else hi = mid;
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int32_t p = q + t;
+          if (p < e0 || p >= e1) continue;
+          while (lo + 1 < cnt && xs[lo + 1] <= p) ++lo;
+          const int32_t c = v0 + lo;
+          const int32_t i = p - xs[lo];
+          if (i < cdeg[c]) {
+            const int32_t dst = cxadj[c] + i;
+            cadj[dst] = av[t];
+            cw[dst] = wv[t];
+          }
+        }
       }
-      const int32_t c = v0 + lo;
-      const int32_t i = p - xs[lo];
-      if (i < cdeg[c]) {
-        const int32_t dst = cxadj[c] + i;
-        cadj[dst] = tmp_adj[p];
-        cw[dst] = tmp_w[p];
+    } else {
+      for (int32_t p = e0 + lane; p < e1; p += 32) {
+        int lo = 0, hi = cnt;
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (xs[mid] <= p) lo = mid; else hi = mid;
+        }
+        const int32_t c = v0 + lo;
+        const int32_t i = p - xs[lo];
+        if (i < cdeg[c]) {
+          const int32_t dst = cxadj[c] + i;
+          cadj[dst] = tmp_adj[p];
+          cw[dst] = tmp_w[p];
+        }
       }
     }
     __syncwarp();
@@ -679,7 +714,7 @@ __global__ void k_contract_compact(int32_t cn, const idx_t* __restrict__ ub_off,
                                    const idx_t* __restrict__ tmp_w, idx_t* __restrict__ cadj,
                                    idx_t* __restrict__ cw) {
   __shared__ int32_t xs_all[8][33];
-  compact_body(cn, ub_off, cdeg, cxadj, tmp_adj, tmp_w, cadj, cw, xs_all[threadIdx.x >> 5], grid_warps());
+  compact_body<true>(cn, ub_off, cdeg, cxadj, tmp_adj, tmp_w, cadj, cw, xs_all[threadIdx.x >> 5], grid_warps());
 }
 
 struct LoadHeavy {
@@ -729,8 +764,11 @@ CoarseResult contract(const DGraph& g, const idx_t* match, int coarse_vwgt, Aren
   idx_t* ub_off = arena.alloc<idx_t>((size_t)cn + 1);
   idx_t* cdeg = arena.alloc<idx_t>((size_t)cn);
   idx_t* hlist = arena.alloc<idx_t>((size_t)cn);
-  idx_t* tmp_adj = arena.alloc<idx_t>((size_t)g.m + 1);
-  idx_t* tmp_w = arena.alloc<idx_t>((size_t)g.m + 1);
+  // Three entries of slack: the compaction reads its ranges in aligned
+  // groups of four, whose last one may reach up to three entries past the
+  // range's end (at most g.m).
+  idx_t* tmp_adj = arena.alloc<idx_t>((size_t)g.m + 4);
+  idx_t* tmp_w = arena.alloc<idx_t>((size_t)g.m + 4);
   k_build_cmap<<<grid_for(n, 256), 256, 0, st>>>(g.xadj, n, match, cidx, cmap, mem0, mem1, ub);
   RMB_LAUNCH_CHECK();
   exclusive_scan_arr<idx_t>(ub, ub_off, cn, ub_off + cn, arena, st);
@@ -964,7 +1002,7 @@ __device__ void tail_body(const TailArgs& a) {
       lo = lvl_lo;
       break;
     }
-    compact_body(cn, ub_off, cdeg, cxadj, tmp_adj, tmp_w, cadj, cw, xs_all[wib], W);
+    compact_body<false>(cn, ub_off, cdeg, cxadj, tmp_adj, tmp_w, cadj, cw, xs_all[wib], W);
     if (coarse_vw) coarse_vwgt_body(cn, cur.ncon, mem0, mem1, cur.vwgt, cvwgt, L);
     __syncthreads();
     // ---- the level is complete: record it and apply the stop rule ----
