@@ -354,7 +354,7 @@ def run_rmat_seeds(args):
     stream = torch.cuda.current_stream(dev)
     assert lib.RMETIS_GPU_SetStream(stream.cuda_stream) == 1
     call16, dpart16, obj16 = _device_call(lib, torch, dev, x, a, None, None, k, kway_options(seed, ncuts=ncuts))
-    warm = max(1, min(args.warmup, 2))
+    warm = args.warmup
     reps = max(1, min(args.steps, 3))
     rmb.set_tuning(parallel_attempts=1)
     for _ in range(warm):
@@ -490,7 +490,7 @@ def run_rgg_batch(args):
     n_tot = sum(g.nvtxs for g in graphs)
     m_tot = sum(len(g.adjncy) for g in graphs)
     o = rmb.Options(rtype=rmb.RType.Greedy, seed=1, ufactor=50)
-    warm = max(1, min(args.warmup, 2))
+    warm = args.warmup
     reps = max(1, min(args.steps, 3))
     # The batch as a caller of the C ABI holds it: concatenated CSR arrays in
     # pinned host memory, built once (outside the timed region).
