@@ -102,6 +102,28 @@ def test_contraction_bit_exact(rmb, oracle, name, source, thread_max):
         rmb.set_kernel_shapes(contract_thread_max=32)
 
 
+@pytest.mark.parametrize("source", ["shem", "gpu"])
+@pytest.mark.parametrize("thread_max", [16, 32])
+def test_contraction_isolated_vertices(rmb, oracle, source, thread_max):
+    """R-MAT keeps thousands of isolated vertices: runs of coarse vertices
+    whose merged rows are all empty (empty ranges in the compaction), short
+    rows beside hub rows, and ranges that start and end off a multiple of
+    four entries."""
+    from rmetis_b200 import functions as F
+    rmb.set_kernel_shapes(contract_thread_max=thread_max)
+    x, a = G.rmat(13, seed=21)
+    n = len(x) - 1
+    assert int((np.diff(x) == 0).sum()) > 1000
+    if source == "shem":
+        m = oracle.shem_matching(x, a, None, oracle.SmallRng(14))
+    else:
+        m = F.match(rmb.Graph(n, 1, x, a), mode=1, seed=15)
+    try:
+        _check_contraction(rmb, oracle, x, a, None, None, m)
+    finally:
+        rmb.set_kernel_shapes(contract_thread_max=32)
+
+
 def test_contraction_multiconstraint(rmb, oracle):
     x, a, _, w = G.random_graph(1500, 8.0, seed=9)
     n = len(x) - 1
